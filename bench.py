@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Train rays/s of the NeAT forward-projection training step on B200.
+
+A step = one fused neat_train_step over a batch of rays: camera rays,
+ray-octree intersection + stratified sampling, IGS + decoder + softplus, line
+integral, MSE, hand-written backward, Adam on grid and decoder.
+
+Default workload (N=1): the plain FP32 full-size configuration -- phantom of
+64 random ellipsoids + 200 void spheres, 360 projections of 512x512 with
+Poisson noise (I0 = 1e4), octree of max depth 4 refined by density variance
+to ~1500 active nodes, C=8 features on G=17 grids, decoder 8->64->64->1,
+32 samples per node segment, 2^18 rays per batch.  Synthetic data stands in
+for the reference's measured scans.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: the path is data parallel over rays with no exchange in this
+build (replicas only): every rank trains its own replica on its own batches,
+timing is the max over ranks, value = all rays processed / that time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "full": dict(desc="plain FP32 full size: 64 ellipsoids + 200 voids, 360 x 512^2 projections, Poisson I0=1e4, "
+                      "adaptive octree depth 4 (~1500 active), C=8, G=17, decoder 8-64-64-1, M=32, 2^18 rays/batch",
+                 n_ell=64, n_void=200, n_angles=360, w=512, h=512, photons=1e4, depth=4, active=1500, C=8, G=17,
+                 M=32, R=1 << 18, seed=2, cpu_rays=1 << 11),
+    "small": dict(desc="plain FP32 small: 8 ellipsoids, 32 x 128^2 projections, octree depth 2 (64 leaves), C=4, "
+                       "G=11, decoder 4-64-64-1, M=16, 4096 rays/batch",
+                  n_ell=8, n_void=0, n_angles=32, w=128, h=128, photons=None, depth=2, active=None, C=4, G=11, M=16,
+                  R=4096, seed=1, cpu_rays=4096),
+}
+METRIC = "train rays/s (fwd+bwd)"
+PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
+
+
+def hidden_flops(C, H=64):
+    return C * H + H * H + H  # multiply-adds of one decoder forward
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# workload
+# --------------------------------------------------------------------------
+def build_workload(cfg, device):
+    from neat_b200 import scene as SC
+    from neat_b200.api import CameraModel
+    from neat_b200.tree import HyperTreeBase
+    objs = SC.ellipsoid_phantom(cfg["n_ell"], cfg["n_void"], seed=cfg["seed"])
+    scene = SC.SyntheticScene(objs, cfg["n_angles"], cfg["w"], cfg["h"], device=device, photons=cfg["photons"],
+                              noise_seed=cfg["seed"])
+    tree = HyperTreeBase(3, cfg["depth"])
+    if cfg["active"]:
+        tree.RefineByVariance(scene.density, cfg["active"], samples_per_axis=4)
+    else:
+        tree.SetActive(cfg["depth"])
+    return scene, tree, CameraModel.from_scene(scene)
+
+
+def cpu_tree(cfg, objs):
+    from oracle import oracle as O
+    from neat_b200.tree import HyperTreeBase
+    tree = HyperTreeBase(3, cfg["depth"])
+    if cfg["active"]:
+        tree.RefineByVariance(lambda p: O.phantom_density(objs, p), cfg["active"], samples_per_axis=4)
+    else:
+        tree.SetActive(cfg["depth"])
+    return tree
+
+
+# --------------------------------------------------------------------------
+# CPU path (oracle port of the reference's CPU execution) -- baseline only
+# --------------------------------------------------------------------------
+def cpu_reference_rays_per_s(cfg, steps, warmup, budget_s=None):
+    """Times the CPU restatement of the step: C oracle rays + samples + IGS
+    (reference CPU semantics), libtorch-CPU decoder / softplus / index_add /
+    MSE / autograd / Adam, with all host threads.  Returns (rays/s, info)."""
+    from oracle import cpu_reference as CR
+    from neat_b200 import scene as SC
+    objs = SC.ellipsoid_phantom(cfg["n_ell"], cfg["n_void"], seed=cfg["seed"])
+    tree = cpu_tree(cfg, objs)
+    runner = CR.CpuReferenceStep(objs, tree, cfg)
+    R = cfg["cpu_rays"]
+    batches = [runner.batch(R) for _ in range(warmup + steps)]  # host data loading is not timed
+    for i in range(warmup):
+        runner.run(*batches[i], i + 1)
+    t0 = time.perf_counter()
+    done = 0
+    for i in range(steps):
+        runner.run(*batches[warmup + i], warmup + i + 1)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return R * done / dt, dict(cores=torch.get_num_threads(), rays=R, steps=done, seconds=dt,
+                               samples_per_ray=runner.last_samples / R)
+
+
+# --------------------------------------------------------------------------
+# main
+# --------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="neat", choices=["neat", "reference"])
+    ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference arm: rank 0 alone runs the CPU path
+        if rank != 0:
+            return
+        v, info = cpu_reference_rays_per_s(cfg, args.steps, args.warmup, budget_s=120.0)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": args.gpus,
+                "steps": info["steps"], "warmup": args.warmup, "ms_per_step": 1000.0 * info["seconds"] / info["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": cfg["desc"], "rays_per_step": info["rays"]},
+                "cpu_baseline": {"value": v, "unit": "rays/s", "cores": info["cores"], "kind": "port",
+                                 "sample": f"{info['rays']} rays/step of the same workload, {info['steps']} steps"},
+                "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device (the neat arm has no CPU fallback)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from neat_b200 import _lib
+    from neat_b200.csrc import build
+    from neat_b200.trainer import FusedTrainer
+    build.build()
+    scene, tree, cam = build_workload(cfg, dev)
+    R, K, W = cfg["R"], args.steps, args.warmup
+    tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"] + rank,
+                      device=dev)
+    tr.reserve(R)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1000 + rank)
+    batches = [scene.sample_batch(R, gen) for _ in range(W + K)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up (device-resident batches)
+    for i in range(W):
+        tr.step(*batches[i])
+    torch.cuda.synchronize()
+    tr.check_status()
+
+    # ---- timed: device-resident inputs (value)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(_lib.NEAT_STEP_PHASES)] for _ in range(K)]
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for i in range(K):
+        tr.step(*batches[W + i], phase_events=ev[i])
+    t_end.record()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    barrier()
+    ms = max_over_ranks(t_start.elapsed_time(t_end))
+    tr.check_status()
+    counters = tr.counters.cpu().tolist()
+    phase_ms = {p: 0.0 for p in PHASES}
+    for i in range(K):
+        for j, p in enumerate(PHASES):
+            phase_ms[p] += ev[i][j].elapsed_time(ev[i][j + 1])
+    phase_ms = {p: v / K for p, v in phase_ms.items()}
+    value = R * K * world / (ms / 1000.0)
+
+    # ---- timed: end to end through the public API with host buffers (e2e)
+    hb = []
+    for i in range(K):
+        uv, img, tgt = scene.sample_batch(R, gen)
+        hb.append((uv.cpu().pin_memory(), img.cpu().pin_memory(), tgt.cpu().pin_memory()))
+    d_uv = torch.empty((R, 2), device=dev)
+    d_img = torch.empty(R, dtype=torch.int32, device=dev)
+    d_tgt = torch.empty(R, device=dev)
+    loss_host = torch.empty(K, dtype=torch.float32).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(K):
+        uv, img, tgt = hb[i]
+        d_uv.copy_(uv, non_blocking=True)
+        d_img.copy_(img, non_blocking=True)
+        d_tgt.copy_(tgt, non_blocking=True)
+        loss = tr.step(d_uv, d_img, d_tgt)
+        loss_host[i:i + 1].copy_(loss, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    tr.check_status()
+    e2e = R * K * world / (e2e_ms / 1000.0)
+    h2d = R * (8 + 4 + 4)
+
+    # ---- roofline of the dominant kernel (backward tiles)
+    S = counters[1]
+    H = 64
+    flops_bwd = 4.0 * hidden_flops(cfg["C"], H) * S  # dX + dW products of the decoder backward
+    t_bwd = phase_ms["backward_tiles"] / 1000.0
+    peaks, peak_kind = measured_peaks()
+    achieved = flops_bwd / t_bwd / 1e12
+    peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+    sm_mhz = clock_info.get("sm_mhz") or 1965.0
+    simt_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0)
+        cpu_base = {"value": cv, "unit": "rays/s", "cores": ci["cores"], "kind": "port",
+                    "sample": f"{ci['rays']} rays/step of the same workload x {ci['steps']} steps "
+                              f"({ci['seconds']:.1f} s)"}
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": cfg["desc"], "rays_per_step": R, "samples_per_step": S, "segments_per_step":
+                   counters[0], "active_nodes": tree.NumActiveNodes(), "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2: grid + Adam state %.2f GB per replica" % (
+                       4 * 4 * tr.grid.numel() / 1e9)},
+        "phase_ms": phase_ms,
+        "roofline": {"kernel": "k_step_tiles<C=%d,backward>" % cfg["C"], "bound": "tensor", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                     "fp32_simt_peak_tflops": simt_peak,
+                     "frac_of_fp32_simt": achieved / simt_peak},
+        "e2e": {"value": e2e, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+        "gpu_launches": 20 * K,
+        "clocks": clock_info,
+        "cpu_baseline": cpu_base,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

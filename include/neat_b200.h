@@ -1,0 +1,254 @@
+/*
+ * neat_b200.h -- C ABI of the B200-native NeAT forward-projection step.
+ *
+ * All pointers are DEVICE pointers unless a comment says "host".  Buffers are
+ * owned by the caller; no entry point allocates device memory.  Every call is
+ * asynchronous on the given stream and returns a neat_status describing the
+ * launch; data-dependent failures (capacity overflow, too many hits on one
+ * ray, non-dyadic boxes) are reported through a device status word that the
+ * caller reads after its own synchronisation (neat_status_* codes, OR-ed).
+ *
+ * Index types follow the reference: node ids / ray ids / sample indices are
+ * int64 ("long" in the reference's torch::kLong tensors), coordinates f32,
+ * camera model f64.
+ */
+#ifndef NEAT_B200_H
+#define NEAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* neat_stream_t; /* == cudaStream_t */
+
+typedef enum
+{
+    NEAT_OK                = 0,
+    NEAT_ERR_BAD_INPUT     = 1,  /* invalid sizes / pointers (host check)                    */
+    NEAT_ERR_CAPACITY      = 2,  /* output or workspace capacity too small (device flag)     */
+    NEAT_ERR_TOO_MANY_HITS = 4,  /* > 256 ray-node intersections on one ray (device flag)    */
+    NEAT_ERR_NON_DYADIC    = 8,  /* node box not on the dyadic plane grid (device flag)      */
+    NEAT_ERR_CUDA          = 16, /* a CUDA launch failed                                      */
+    NEAT_ERR_UNSUPPORTED   = 32  /* configuration the kernels were not built for             */
+} neat_status;
+
+/* Maximum intersections one ray may have; the reference keeps 256 in shared
+ * memory (src/structure/HyperTree.cu:220) and overflows silently. */
+#define NEAT_MAX_HITS_PER_RAY 256
+
+/* Human-readable message for a status word. host */
+const char* neat_status_string(int status);
+
+/* Library version (host). */
+int neat_version(void);
+
+/* ----------------------------------------------------------------------- */
+/* Camera rays.                                                             */
+/* Replaces SceneBase::GetRays (src/data/SceneBase.cpp:171-193):             */
+/*   px = u*(w-1), py = v*(h-1)           (UVToPixel, CameraPose.h:20-36)    */
+/*   d_c = ((px-cx)/fx, (py-cy)/fy, 1)/|.|  in f64 (Unproject, CameraPose.cu:262-274) */
+/*   d = q (x) d_c  in f64                (RotatePointGPUk, CameraPose.cu:20-33) */
+/*   o = translation[image]; both cast to f32.                              */
+/* intrinsics: [num_cameras, 5] f64 (fx, fy, cx, cy, skew); camera_id may be */
+/* NULL (camera 0).  rotation: [num_images, 4] f64 (x, y, z, w);            */
+/* translation: [num_images, 3] f64.  origin/direction: [R, 3] f32.          */
+/* ----------------------------------------------------------------------- */
+int neat_make_rays(const float* uv, const int32_t* image_id, const int32_t* camera_id, int64_t num_rays, int w, int h,
+                   const double* intrinsics, const double* rotation, const double* translation, float* origin,
+                   float* direction, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Octree node table.                                                        */
+/* The reference keeps node_position_min/max [N,3] and active_node_ids [A]  */
+/* (src/structure/HyperTree.h:206-240).  neat_tree_prepare packs, for every */
+/* active node, its plane indices on the dyadic grid of depth max_depth and */
+/* its diagonal (HyperTree.cu:286) into a caller buffer of                  */
+/* neat_tree_table_bytes(A) bytes.  status: device int, OR-ed error flags.  */
+/* ----------------------------------------------------------------------- */
+size_t neat_tree_table_bytes(int num_active);
+int neat_tree_prepare(const float* node_min, const float* node_max, const int64_t* active_ids, int num_active,
+                      int max_depth, void* table, int* status, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Ray samples.                                                              */
+/* Replaces HyperTreeBaseImpl::CreateSamplesForRays (src/structure/HyperTree.h:157, */
+/* kernel ComputeRaySamples, src/structure/HyperTree.cu:206-438).  Outputs   */
+/* a SampleList (src/structure/HelperStructs.h:168-234) in canonical order:  */
+/* ray-major, segments of one ray ordered by (tmin, node_id).  jitter != 0   */
+/* draws the stratified offset a from Philox(seed; ray, index_in_ray, step), */
+/* else a = 0.5 (the evaluation setting).  out_count (device int64[2]) gets  */
+/* the sample count and the max samples of one ray; samples beyond capacity */
+/* are not written and NEAT_ERR_CAPACITY is raised in *status.              */
+/* workspace: neat_samples_workspace_bytes(num_rays) bytes.                 */
+/* ----------------------------------------------------------------------- */
+size_t neat_samples_workspace_bytes(int64_t num_rays);
+int neat_create_samples(const void* table, int num_active, int max_depth, const float* origin, const float* direction,
+                        int64_t num_rays, int max_samples_per_node, int jitter, uint64_t seed, uint32_t step,
+                        int64_t capacity, float* coords, float* ray_t, float* weight, int64_t* ray_index,
+                        int64_t* local_index_in_ray, int64_t* node_id, int64_t* out_count, int* status,
+                        void* workspace, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Local coordinates.                                                        */
+/* Replaces HyperTreeBaseImpl::ComputeLocalSamples (src/structure/HyperTree.cu:177-192): */
+/* local = (g - min[node]) / (max[node] - min[node]) * 2 - 1.                */
+/* ----------------------------------------------------------------------- */
+int neat_local_samples(const float* global, const int64_t* node_id, int64_t num_samples, const float* node_min,
+                       const float* node_max, float* local, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* IndirectGridSample3D.                                                     */
+/* Replaces IndirectGridSample3D(multi_grid, index, uv) and its autograd    */
+/* Function (src/modules/IndirectGridSample3D.h:18-30, .cu:432-892).        */
+/* grid: [N, C, Z, Y, X] f32 (reference layout), index: [S] int64 row,      */
+/* uv: [S, 3] f32 (x->X, y->Y, z->Z), out: [S, C].                          */
+/* Backward accumulates into grad_grid (same shape) and grad_uv [S,3]        */
+/* (may be NULL); both must be zeroed by the caller, as the reference's     */
+/* torch::zeros_like (IndirectGridSample3D.cu:848-849).                     */
+/* ----------------------------------------------------------------------- */
+int neat_igs_forward(const float* grid, int64_t N, int C, int Z, int Y, int X, const int64_t* index, const float* uv,
+                     int64_t num_samples, float* out, neat_stream_t stream);
+int neat_igs_backward(const float* grid, int64_t N, int C, int Z, int Y, int X, const int64_t* index, const float* uv,
+                      int64_t num_samples, const float* grad_out, float* grad_grid, float* grad_uv,
+                      neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Adam.                                                                     */
+/* Replaces torch::optim::Adam::step as used by NeuralGeometry::OptimizerStep */
+/* (src/geometry/geometry.h:66-88): bias-corrected, no weight decay, every  */
+/* element updated every step.  step is 1-based.  If zero_grad != 0 the     */
+/* gradient is cleared after it is read (optimizer->zero_grad()).           */
+/* ----------------------------------------------------------------------- */
+int neat_adam(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr, float beta1,
+              float beta2, float eps, int step, int zero_grad, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Decoder layout.                                                           */
+/* FCBlock(C, 1, hidden_layers=1, 64, "silu") (src/geometry/ImplicitNet.h:18-73) */
+/* + softplus(beta) (src/geometry/geometry.cpp:133-136).  The parameters are */
+/* packed in one f32 buffer of neat_decoder_params(C) floats:               */
+/*   W1 [64][C] | b1 [64] | W2 [64][64] | b2 [64] | W3 [64] | b3 [1]         */
+/* (torch nn.Linear weight layout: [out][in]).                              */
+/* ----------------------------------------------------------------------- */
+#define NEAT_HIDDEN 64
+int64_t neat_decoder_params(int C);
+
+/* ----------------------------------------------------------------------- */
+/* ComputeImage over an explicit SampleList.                                 */
+/* Replaces HierarchicalNeuralGeometry::ComputeImage (src/geometry/geometry.cpp:347-389) */
+/* for GeometryExEx::SampleVolumeIndirect (src/geometry/geometry_ex_ex.cpp:161-180): */
+/* local coords -> IGS -> decoder -> softplus -> * weight -> index_add by ray. */
+/* grid: [A, C, G, G, G] (reference layout), local_node_id: active row per  */
+/* sample (GlobalNodeIdToLocalActiveId).  image: [R] f32, zeroed by caller. */
+/* Backward: grad_image [R] -> grad_grid (same layout, zeroed by caller) and */
+/* grad_decoder (neat_decoder_params(C) floats, zeroed by caller).           */
+/* ----------------------------------------------------------------------- */
+int neat_compute_image_forward(const float* grid, int64_t num_rows, int C, int G, const float* decoder,
+                               float softplus_beta, const float* coords, const float* weight,
+                               const int64_t* ray_index, const int64_t* node_id, const int64_t* local_node_id,
+                               const float* node_min, const float* node_max, int64_t num_samples, float* image,
+                               neat_stream_t stream);
+int neat_compute_image_backward(const float* grid, int64_t num_rows, int C, int G, const float* decoder,
+                                float softplus_beta, const float* coords, const float* weight,
+                                const int64_t* ray_index, const int64_t* node_id, const int64_t* local_node_id,
+                                const float* node_min, const float* node_max, int64_t num_samples,
+                                const float* grad_image, float* grad_grid, float* grad_decoder, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Fused training step.                                                      */
+/* Replaces one iteration of Trainer::TrainStep (samples/reconstruct.cpp:362-403): */
+/*   GetRays -> CreateSamplesForRays(jitter) -> ComputeImage -> MSE loss ->   */
+/*   backward -> OptimizerStep (Adam on grid and decoder),                   */
+/* without materialising per-sample tensors: rays are cut into node          */
+/* segments, segments are bucketed by node, and node-major sample tiles run */
+/* the grid lookup, decoder and its backward in one kernel each way.         */
+/* The grid is kept channel-last [A, G, G, G, C] (neat_grid_to_channel_last). */
+/* ----------------------------------------------------------------------- */
+typedef struct
+{
+    /* octree */
+    const void* tree_table; /* from neat_tree_prepare */
+    int num_active;
+    int max_depth;
+    const float* node_min; /* [N,3] */
+    const float* node_max; /* [N,3] */
+    /* camera */
+    int w, h;
+    const double* intrinsics;  /* [1,5] */
+    const double* rotation;    /* [num_images,4] */
+    const double* translation; /* [num_images,3] */
+    /* model */
+    int C, G;
+    float softplus_beta;
+    int max_samples_per_node;
+    /* optimizer */
+    float lr_grid, lr_decoder, beta1, beta2, eps;
+    /* capacity of the per-step segment buffers */
+    int64_t seg_capacity;
+} neat_step_desc;
+
+typedef struct
+{
+    float* grid;       /* [A, G,G,G, C] channel-last */
+    float* grid_m;     /* Adam first moment, same shape */
+    float* grid_v;     /* Adam second moment */
+    float* grid_grad;  /* gradient scratch, same shape; zero on entry, left zero */
+    float* decoder;    /* neat_decoder_params(C) */
+    float* decoder_m;
+    float* decoder_v;
+    float* decoder_grad;
+} neat_step_state;
+
+typedef struct
+{
+    const float* uv;         /* [R,2] in [0,1] */
+    const int32_t* image_id; /* [R] */
+    const float* target;     /* [R] */
+    int64_t num_rays;
+} neat_step_batch;
+
+typedef struct
+{
+    float* loss;        /* device f32[1]: mean squared error of the batch */
+    int64_t* counters;  /* device int64[4]: segments, samples, max hits per ray, tiles */
+    int* status;        /* device int: OR-ed neat_status flags */
+    float* prediction;  /* optional [R] predicted projection (may be NULL) */
+    /* optional: NEAT_STEP_PHASES cudaEvent_t handles recorded on the step's
+     * stream at the phase boundaries: [0] start, [1] segment lists built,
+     * [2] forward tiles done, [3] loss done, [4] backward tiles done,
+     * [5] Adam done.  NULL disables. */
+    void* const* phase_events;
+} neat_step_out;
+
+#define NEAT_STEP_PHASES 6
+
+size_t neat_train_step_workspace_bytes(const neat_step_desc* desc, int64_t num_rays);
+int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, const neat_step_batch* batch,
+                    uint64_t seed, int step, const neat_step_out* out, void* workspace, size_t workspace_bytes,
+                    neat_stream_t stream);
+
+/* Grid layout conversion between the reference's [A, C, G,G,G] and the     */
+/* step's channel-last [A, G,G,G, C].                                        */
+int neat_grid_to_channel_last(const float* src, float* dst, int64_t A, int C, int G, neat_stream_t stream);
+int neat_grid_from_channel_last(const float* src, float* dst, int64_t A, int C, int G, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Synthetic scans (stand-in for the reference's measured projections).     */
+/* objects: [n, 17] f64 = centre(3), semi-axes(3), R(9, local = R^T (p-c)),  */
+/* density, kind (0 additive ellipsoid, 1 void).  Projection [n_img, h, w]   */
+/* f32 of line integrals through pixel centres; density volume [n^3] at     */
+/* voxel-corner positions -1 + 2 i/(n-1), x fastest.                         */
+/* ----------------------------------------------------------------------- */
+int neat_synth_project(const double* objects, int num_objects, int num_images, int w, int h,
+                       const double* intrinsics, const double* rotation, const double* translation, float* out,
+                       neat_stream_t stream);
+int neat_synth_density(const double* objects, int num_objects, const double* points, int64_t num_points,
+                       double* out, neat_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEAT_B200_H */

@@ -1,0 +1,69 @@
+"""Build libneat_b200.so (sm_100a) in-tree with nvcc.
+
+Usage: python -m neat_b200.csrc.build [--verbose-ptxas]
+
+Every .cu file is compiled separately for sm_100a (compute_100a PTX is not
+embedded), then linked into neat_b200/libneat_b200.so next to the package.
+neat_synth.cu is compiled with --fmad=false so the f64 projector rounds
+every operation as written.
+"""
+import concurrent.futures
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+OUT = os.path.join(PKG, "libneat_b200.so")
+BUILD = os.path.join(ROOT, "_build", "neat_b200")
+
+SOURCES = ["neat_rays.cu", "neat_step.cu", "neat_image.cu", "neat_igs.cu", "neat_api.cu", "neat_synth.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
+          "--expt-relaxed-constexpr"]
+PER_FILE = {"neat_synth.cu": ["--fmad=false"]}
+
+
+def _compile(src, verbose):
+    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+    cmd = [NVCC, *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", os.path.join(HERE, src), "-o", obj]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return src, obj, r.returncode, r.stdout + r.stderr
+
+
+def build(verbose=False):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = [os.path.join(HERE, s) for s in SOURCES]
+    deps = srcs + [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(ROOT, "include", "neat_b200.h"))
+    if os.path.exists(OUT) and not verbose:
+        newest = max(os.path.getmtime(p) for p in deps)
+        if os.path.getmtime(OUT) >= newest:
+            return OUT
+    objs, logs, failed = [], [], False
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        for src, obj, rc, log in ex.map(lambda s: _compile(s, verbose), SOURCES):
+            objs.append(obj)
+            if log.strip():
+                logs.append(f"--- {src}\n{log}")
+            if rc != 0:
+                failed = True
+    if logs and (failed or verbose):
+        sys.stderr.write("\n".join(logs) + "\n")
+    if failed:
+        raise RuntimeError("nvcc failed")
+    tmp = OUT + ".tmp"
+    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    os.replace(tmp, OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="--verbose-ptxas" in sys.argv))

@@ -1,0 +1,37 @@
+// neat_internal.h -- launchers shared between the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace neat
+{
+
+// Node-major segment record of the fused step (one ray crossing one node).
+struct __align__(16) SegRec
+{
+    int32_t ray;
+    int32_t local_base;  // index in ray of the segment's first sample
+    float tmin, tmax;
+    int32_t n;           // samples in the segment
+    int32_t rm;          // ray-major (canonical) segment index
+    int32_t row;         // active (local) node id = grid row
+    int32_t node;        // global node id
+};
+static_assert(sizeof(SegRec) == 32, "SegRec must be 32 bytes");
+
+// Pass 1 of the step: rays from (uv, image) and per-ray / per-node counts.
+cudaError_t launch_step_rays_count(const float* uv, const int32_t* image_id, int64_t R, int w, int h,
+                                   const double* intr, const double* rot, const double* trans, const void* table,
+                                   int A, int D, int M, float* origin, float* direction, int* ray_nseg,
+                                   int* node_nseg, int64_t* counters, int* status, cudaStream_t st);
+
+// Pass 2 of the step: canonical per-ray segment lists, bucketed by node.
+cudaError_t launch_step_rays_write(const float* origin, const float* direction, int64_t R, const void* table, int A,
+                                   int D, int M, const int* ray_seg_off, const int* node_seg_off, int* node_cursor,
+                                   SegRec* segs, int* seg_n, const int64_t* nseg_eff, int64_t cap, int* status,
+                                   cudaStream_t st);
+
+int sm_count();
+
+}  // namespace neat

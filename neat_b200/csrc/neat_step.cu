@@ -1,0 +1,564 @@
+// neat_step.cu -- one fused training step of the NeAT forward projector:
+// Trainer::TrainStep (samples/reconstruct.cpp:362-403) without per-sample
+// tensors in HBM.
+//
+// Data flow (all on one stream, no host synchronisation):
+//   1 rays+counts   warp/ray: f64 camera ray, slab test vs all active nodes
+//   2 scans         per-ray segment offsets, per-node bucket offsets
+//   3 segments      warp/ray: canonical (tmin,node) lists, bucketed by node
+//   4 scan          node-major sample offsets; tile -> first segment table
+//   5 forward       128-sample tiles in node-major order: jitter, position,
+//                   local coords, IGS, decoder, softplus, weight, per-segment
+//                   sums (a segment spans <= 2 tiles: two commutative adds)
+//   6 loss          per ray: sum of its segments in tmin order, MSE, dL/dpred
+//   7 backward      same tiles: recompute, decoder backward, grid scatter
+//   8 Adam          decoder (deterministic reduce of per-CTA partials), grid
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "neat_internal.h"
+#include "neat_scan.cuh"
+#include "neat_tiles.cuh"
+
+namespace neat
+{
+
+struct StepTileArgs
+{
+    const SegRec* segs;
+    const int* samp_off;
+    const int* tile_seg;
+    const int64_t* counters;
+    const float* origin;
+    const float* direction;
+    const float* node_min;
+    const float* node_max;
+    const float* grid;
+    float* grid_grad;
+    const float* decoder;
+    float* dec_part;
+    const float* dpred;
+    float* partial;
+    uint64_t seed;
+    uint32_t step;
+    int G;
+    float beta;
+};
+
+template <int C, bool BWD>
+__global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TileSmem<C, BWD>& sm = *reinterpret_cast<TileSmem<C, BWD>*>(smraw);
+    const int t          = threadIdx.x;
+    tile_load_decoder<C, BWD>(sm, a.decoder);
+    DecGradAcc<C> g;
+    g.zero();
+    const int nseg       = (int)a.counters[0];
+    const int64_t S      = a.counters[1];
+    const int64_t ntiles = (S + TT - 1) / TT;
+    __syncthreads();
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    {
+        const int64_t g0 = tile * TT;
+        const int seg_lo = a.tile_seg[tile];
+        // ---- slot -> segment: mark segment starts, inclusive max-scan ----
+        if (t < TT) sm.mark[t] = (t == 0) ? seg_lo : -1;
+        __syncthreads();
+        if (t <= TT)
+        {
+            const int seg = seg_lo + t;
+            if (seg < nseg)
+            {
+                const int64_t o = a.samp_off[seg];
+                if (o > g0 && o < g0 + TT) sm.mark[(int)(o - g0)] = seg;
+            }
+        }
+        __syncthreads();
+        if (t < TT)
+        {
+            int v = sm.mark[t];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if ((t & 31) >= o) v = max(v, y);
+            }
+            sm.slot_seg[t] = v;
+        }
+        __syncthreads();
+        if (t < TT)
+        {
+            int v = sm.slot_seg[t];
+            for (int w2 = 0; w2 < (t >> 5); ++w2) v = max(v, sm.slot_seg[w2 * 32 + 31]);
+            sm.mark[t] = v;  // final segment of slot t
+        }
+        __syncthreads();
+        // ---- per-slot sample setup + grid gather ----
+        bool valid = false;
+        float wgt = 0.0f, lu = 0.0f, lv = 0.0f, lw = 0.0f;
+        int ray = 0, rm = 0, row = 0;
+        if (t < TT)
+        {
+            const int64_t gs = g0 + t;
+            valid            = gs < S;
+            const int seg    = sm.mark[t];
+            const SegRec r   = a.segs[seg];
+            const int j      = valid ? (int)(gs - a.samp_off[seg]) : 0;
+            float ts, ws;
+            seg_sample(r.tmin, r.tmax, r.n, j, true, a.seed, a.step, r.ray, r.local_base, ts, ws);
+            const float* o  = a.origin + 3 * (int64_t)r.ray;
+            const float* d  = a.direction + 3 * (int64_t)r.ray;
+            const float* mn = a.node_min + 3 * (int64_t)r.node;
+            const float* mx = a.node_max + 3 * (int64_t)r.node;
+            lu              = local_coord(__fadd_rn(o[0], __fmul_rn(d[0], ts)), mn[0], mx[0]);
+            lv              = local_coord(__fadd_rn(o[1], __fmul_rn(d[1], ts)), mn[1], mx[1]);
+            lw              = local_coord(__fadd_rn(o[2], __fmul_rn(d[2], ts)), mn[2], mx[2]);
+            Corners k;
+            igs_corners(lu, lv, lw, a.G, a.G, a.G, k);
+            float x[C];
+            gather_cl<C>(a.grid, r.row, a.G, k, x);
+#pragma unroll
+            for (int c = 0; c < C; ++c) sm.XT[c * TT + t] = valid ? x[c] : 0.0f;
+            wgt = valid ? ws : 0.0f;
+            ray = r.ray;
+            rm  = r.rm;
+            row = r.row;
+        }
+        __syncthreads();
+        // ---- decoder forward ----
+        tile_layer1<C, BWD>(sm);
+        __syncthreads();
+        float z2[4][HPW];
+        tile_gemm_fwd<C, BWD>(sm, z2);
+        tile_ypart<C, BWD>(sm, z2);
+        __syncthreads();
+        if (t < TT)
+        {
+            const float y = tile_y(sm, t);
+            if (!BWD)
+            {
+                sm.val[t] = valid ? softplusf_(y, a.beta) * wgt : 0.0f;
+            }
+            else
+            {
+                const float dv = valid ? a.dpred[ray] : 0.0f;
+                const float dy = dv * wgt * softplus_grad(y, a.beta);
+                sm.val[t]      = dy;
+                g.db3 += dy;
+            }
+        }
+        __syncthreads();
+        if constexpr (!BWD)
+        {
+            // per-segment sums in sample order; a segment crossing the tile
+            // boundary gets exactly two commutative adds onto a zeroed slot.
+            if (t < TT && valid)
+            {
+                const int seg = sm.mark[t];
+                if (t == 0 || sm.mark[t - 1] != seg)
+                {
+                    float sum = 0.0f;
+                    for (int u = t; u < TT && sm.mark[u] == seg; ++u) sum += sm.val[u];
+                    atomicAdd(a.partial + rm, sum);
+                }
+            }
+            __syncthreads();
+        }
+        else
+        {
+            float dx[C];
+            tile_backward<C>(sm, z2, g, dx);
+            if (t < TT && valid)
+            {
+                Corners k;
+                igs_corners(lu, lv, lw, a.G, a.G, a.G, k);
+                scatter_cl<C>(a.grid_grad, row, a.G, k, dx);
+            }
+            __syncthreads();
+        }
+    }
+    if constexpr (BWD) dec_grad_flush<C>(g, a.dec_part + (int64_t)blockIdx.x * DecOff<C>::total, false, sm.ypart);
+}
+
+__global__ void k_clamp_segments(int64_t* counters, int64_t cap, int* status)
+{
+    if (counters[0] > cap)
+    {
+        raise_status(status, NEAT_ERR_CAPACITY);
+        counters[0] = 0;
+    }
+}
+
+__global__ void k_clamp_samples(int64_t* counters, int64_t sample_cap, int* status)
+{
+    if (counters[1] > sample_cap)
+    {
+        raise_status(status, NEAT_ERR_CAPACITY);
+        counters[1] = 0;
+    }
+    counters[3] = (counters[1] + TT - 1) / TT;
+}
+
+__global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, const int64_t* counters,
+                           int* __restrict__ tile_seg, int64_t tiles_cap)
+{
+    const int64_t i    = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nseg = counters[0];
+    if (i >= nseg || counters[1] == 0) return;
+    const int64_t o = samp_off[i], e = o + seg_n[i];
+    const int64_t t = (o + TT - 1) / TT;
+    if (t * TT < e && t < tiles_cap) tile_seg[t] = (int)i;
+}
+
+__global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const float* __restrict__ partial,
+                           const float* __restrict__ target, float* __restrict__ dpred, float* __restrict__ pred_out,
+                           float* __restrict__ loss_part, float invR, const int64_t* nseg_eff)
+{
+    __shared__ float red[256];
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float sq        = 0.0f;
+    if (r < R)
+    {
+        float pred = 0.0f;
+        if (*nseg_eff > 0)
+        {
+            const int b = ray_seg_off[r], e = ray_seg_off[r + 1];
+            for (int k = b; k < e; ++k) pred += partial[k];
+        }
+        const float diff = pred - target[r];
+        dpred[r]         = 2.0f * diff * invR;
+        sq               = diff * diff;
+        if (pred_out) pred_out[r] = pred;
+    }
+    red[threadIdx.x] = sq;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1)
+    {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss_part[blockIdx.x] = red[0];
+}
+
+__global__ void k_loss_final(const float* __restrict__ loss_part, int nb, float* loss, float invR)
+{
+    __shared__ float red[1024];
+    float s = 0.0f;
+    for (int i = threadIdx.x; i < nb; i += 1024) s += loss_part[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1)
+    {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *loss = red[0] * invR;
+}
+
+// torch::optim::Adam::step (libtorch 1.11): m = b1 m + (1-b1) g;
+// v = b2 v + (1-b2) g^2; p -= (lr/bc1) * m / (sqrt(v)/sqrt(bc2) + eps).
+__device__ __forceinline__ void adam_update(float& p, float gr, float& m, float& v, float b1, float b2, float eps,
+                                            float step_size, float sqrt_bc2)
+{
+    m                 = fmaf(1.0f - b1, gr, m * b1);
+    v                 = fmaf((1.0f - b2) * gr, gr, v * b2);
+    const float denom = sqrtf(v) / sqrt_bc2 + eps;
+    p                 = fmaf(-step_size, m / denom, p);
+}
+
+__global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, int P, float* __restrict__ grad,
+                                  float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float b1,
+                                  float b2, float eps, float step_size, float sqrt_bc2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    float gsum = 0.0f;
+    for (int b = 0; b < nparts; ++b) gsum += part[(int64_t)b * P + i];
+    grad[i] = gsum;
+    float pi = p[i], mi = m[i], vi = v[i];
+    adam_update(pi, gsum, mi, vi, b1, b2, eps, step_size, sqrt_bc2);
+    p[i] = pi;
+    m[i] = mi;
+    v[i] = vi;
+}
+
+__global__ void k_adam(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
+                       int64_t n, float b1, float b2, float eps, float step_size, float sqrt_bc2, int zero_grad)
+{
+    const int64_t n4     = n / 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride)
+    {
+        float4 pp = reinterpret_cast<float4*>(p)[i];
+        float4 gg = reinterpret_cast<float4*>(grad)[i];
+        float4 mm = reinterpret_cast<float4*>(m)[i];
+        float4 vv = reinterpret_cast<float4*>(v)[i];
+        adam_update(pp.x, gg.x, mm.x, vv.x, b1, b2, eps, step_size, sqrt_bc2);
+        adam_update(pp.y, gg.y, mm.y, vv.y, b1, b2, eps, step_size, sqrt_bc2);
+        adam_update(pp.z, gg.z, mm.z, vv.z, b1, b2, eps, step_size, sqrt_bc2);
+        adam_update(pp.w, gg.w, mm.w, vv.w, b1, b2, eps, step_size, sqrt_bc2);
+        reinterpret_cast<float4*>(p)[i] = pp;
+        reinterpret_cast<float4*>(m)[i] = mm;
+        reinterpret_cast<float4*>(v)[i] = vv;
+        if (zero_grad) reinterpret_cast<float4*>(grad)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        float pi = p[i], mi = m[i], vi = v[i];
+        adam_update(pi, grad[i], mi, vi, b1, b2, eps, step_size, sqrt_bc2);
+        p[i] = pi;
+        m[i] = mi;
+        v[i] = vi;
+        if (zero_grad) grad[i] = 0.0f;
+    }
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (n == 0)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <int C, bool BWD>
+static int tile_grid(size_t& smem)
+{
+    smem = sizeof(TileSmem<C, BWD>);
+    static int blocks = 0;
+    if (blocks == 0)
+    {
+        cudaFuncSetAttribute(k_step_tiles<C, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_tiles<C, BWD>, TN, smem);
+        if (per_sm < 1) per_sm = 1;
+        blocks = per_sm * sm_count();
+    }
+    return blocks;
+}
+
+static int tile_grid_any(int C, bool bwd, size_t& smem)
+{
+    switch (C)
+    {
+        case 4: return bwd ? tile_grid<4, true>(smem) : tile_grid<4, false>(smem);
+        case 8: return bwd ? tile_grid<8, true>(smem) : tile_grid<8, false>(smem);
+        case 16: return bwd ? tile_grid<16, true>(smem) : tile_grid<16, false>(smem);
+        default: return 0;
+    }
+}
+
+int64_t decoder_params(int C) { return (int64_t)HH * C + HH + (int64_t)HH * HH + HH + HH + 1; }
+
+// Workspace carve-out, shared by the size query and the step.
+struct StepLayout
+{
+    enum
+    {
+        ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, SEGS, SEG_N, SAMP_OFF,
+        TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, NUM
+    };
+    size_t off[NUM];
+    size_t total;
+    int64_t tiles_cap, sample_cap;
+    int loss_blocks, bwd_grid;
+};
+
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
+{
+    const int64_t cap = d->seg_capacity, A = d->num_active, M = d->max_samples_per_node;
+    L.sample_cap      = cap * (M + 1);
+    L.tiles_cap       = (L.sample_cap + TT - 1) / TT + 1;
+    L.loss_blocks     = (int)((R + 255) / 256);
+    size_t smem       = 0;
+    L.bwd_grid        = tile_grid_any(d->C, true, smem);
+    if (L.bwd_grid <= 0) return false;
+    const int64_t P        = decoder_params(d->C);
+    const int64_t scan_max = std::max(std::max(R, A), cap) + 1;
+    size_t sz[StepLayout::NUM] = {
+        (size_t)R * 3 * 4, (size_t)R * 3 * 4, (size_t)R * 4, (size_t)(R + 1) * 4, (size_t)A * 4, (size_t)A * 4,
+        (size_t)(A + 1) * 4, (size_t)cap * sizeof(SegRec), (size_t)cap * 4, (size_t)(cap + 1) * 4,
+        (size_t)L.tiles_cap * 4, (size_t)cap * 4, (size_t)R * 4, (size_t)L.loss_blocks * 4,
+        (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4};
+    size_t o = 0;
+    for (int i = 0; i < StepLayout::NUM; ++i)
+    {
+        L.off[i] = o;
+        o += align256(sz[i]);
+    }
+    L.total = o;
+    return true;
+}
+
+template <int C>
+static cudaError_t launch_tiles(bool bwd, const StepTileArgs& args, cudaStream_t st)
+{
+    size_t smem = 0;
+    if (!bwd)
+    {
+        const int grid = tile_grid<C, false>(smem);
+        k_step_tiles<C, false><<<grid, TN, smem, st>>>(args);
+    }
+    else
+    {
+        const int grid = tile_grid<C, true>(smem);
+        k_step_tiles<C, true><<<grid, TN, smem, st>>>(args);
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_tiles_any(int C, bool bwd, const StepTileArgs& args, cudaStream_t st)
+{
+    switch (C)
+    {
+        case 4: return launch_tiles<4>(bwd, args, st);
+        case 8: return launch_tiles<8>(bwd, args, st);
+        case 16: return launch_tiles<16>(bwd, args, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace neat
+
+using namespace neat;
+
+extern "C" int64_t neat_decoder_params(int C) { return decoder_params(C); }
+
+extern "C" size_t neat_train_step_workspace_bytes(const neat_step_desc* desc, int64_t num_rays)
+{
+    if (!desc || num_rays < 0) return 0;
+    StepLayout L;
+    if (!step_layout(desc, num_rays, L)) return 0;
+    return L.total;
+}
+
+extern "C" int neat_adam(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr, float beta1,
+                         float beta2, float eps, int step, int zero_grad, neat_stream_t stream)
+{
+    if (n < 0 || step < 1) return NEAT_ERR_BAD_INPUT;
+    if (n == 0) return NEAT_OK;
+    if (!param || !grad || !exp_avg || !exp_avg_sq) return NEAT_ERR_BAD_INPUT;
+    if (((uintptr_t)param | (uintptr_t)grad | (uintptr_t)exp_avg | (uintptr_t)exp_avg_sq) & 15)
+        return NEAT_ERR_BAD_INPUT;
+    const double bc1 = 1.0 - std::pow((double)beta1, step);
+    const double bc2 = 1.0 - std::pow((double)beta2, step);
+    const int grid   = std::min<int64_t>((n / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
+    k_adam<<<grid, 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, beta1, beta2, eps,
+                                                   (float)(lr / bc1), (float)std::sqrt(bc2), zero_grad);
+    return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
+}
+
+extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
+                               uint64_t seed, int step, const neat_step_out* out, void* workspace,
+                               size_t workspace_bytes, neat_stream_t stream)
+{
+    if (!d || !s || !b || !out || !out->loss || !out->counters || step < 1) return NEAT_ERR_BAD_INPUT;
+    if (d->C != 4 && d->C != 8 && d->C != 16) return NEAT_ERR_UNSUPPORTED;
+    const int64_t R = b->num_rays;
+    if (R < 1 || R > (1ll << 23) || d->num_active < 1 || d->max_depth < 1 || d->max_depth > kMaxDepth ||
+        d->G < 2 || d->max_samples_per_node < 1 || d->seg_capacity < 1 || d->w < 2 || d->h < 2)
+        return NEAT_ERR_BAD_INPUT;
+    if (d->seg_capacity * (int64_t)(d->max_samples_per_node + 1) >= (1ll << 31)) return NEAT_ERR_BAD_INPUT;
+    if (!d->tree_table || !d->node_min || !d->node_max || !d->intrinsics || !d->rotation || !d->translation ||
+        !s->grid || !s->grid_m || !s->grid_v || !s->grid_grad || !s->decoder || !s->decoder_m || !s->decoder_v ||
+        !s->decoder_grad || !b->uv || !b->image_id || !b->target || !workspace)
+        return NEAT_ERR_BAD_INPUT;
+    StepLayout L;
+    if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws        = (char*)workspace;
+    auto P_ = [&](int i) { return (void*)(ws + L.off[i]); };
+    float* origin     = (float*)P_(StepLayout::ORIGIN);
+    float* direction  = (float*)P_(StepLayout::DIRECTION);
+    int* ray_nseg     = (int*)P_(StepLayout::RAY_NSEG);
+    int* ray_seg_off  = (int*)P_(StepLayout::RAY_SEG_OFF);
+    int* node_nseg    = (int*)P_(StepLayout::NODE_NSEG);
+    int* node_cursor  = (int*)P_(StepLayout::NODE_CURSOR);
+    int* node_seg_off = (int*)P_(StepLayout::NODE_SEG_OFF);
+    SegRec* segs      = (SegRec*)P_(StepLayout::SEGS);
+    int* seg_n        = (int*)P_(StepLayout::SEG_N);
+    int* samp_off     = (int*)P_(StepLayout::SAMP_OFF);
+    int* tile_seg     = (int*)P_(StepLayout::TILE_SEG);
+    float* partial    = (float*)P_(StepLayout::PARTIAL);
+    float* dpred      = (float*)P_(StepLayout::DPRED);
+    float* loss_part  = (float*)P_(StepLayout::LOSS_PART);
+    float* dec_part   = (float*)P_(StepLayout::DEC_PART);
+    int* scratch      = (int*)P_(StepLayout::SCAN_SCRATCH);
+    int64_t* cnt      = out->counters;
+    const int A = d->num_active, D = d->max_depth, M = d->max_samples_per_node;
+    const int64_t cap = d->seg_capacity;
+
+    auto phase = [&](int i) {
+        if (out->phase_events && out->phase_events[i]) cudaEventRecord((cudaEvent_t)out->phase_events[i], st);
+    };
+    bool ok = true;
+    phase(0);
+    ok      = ok && cudaMemsetAsync(node_nseg, 0, (size_t)A * 4, st) == cudaSuccess;
+    ok      = ok && cudaMemsetAsync(node_cursor, 0, (size_t)A * 4, st) == cudaSuccess;
+    ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
+    ok      = ok && launch_step_rays_count(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation,
+                                           d->translation, d->tree_table, A, D, M, origin, direction, ray_nseg,
+                                           node_nseg, cnt, out->status, st) == cudaSuccess;
+    ok = ok && scan_exclusive<int>(ray_nseg, nullptr, R, ray_seg_off, scratch, cnt + 0, st) == cudaSuccess;
+    ok = ok && scan_exclusive<int>(node_nseg, nullptr, A, node_seg_off, scratch, nullptr, st) == cudaSuccess;
+    k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, out->status);
+    ok = ok && launch_step_rays_write(origin, direction, R, d->tree_table, A, D, M, ray_seg_off, node_seg_off,
+                                      node_cursor, segs, seg_n, cnt + 0, cap, out->status, st) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(partial, 0, (size_t)cap * 4, st) == cudaSuccess;
+    ok = ok && scan_exclusive<int>(seg_n, cnt + 0, cap, samp_off, scratch, cnt + 1, st) == cudaSuccess;
+    k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, out->status);
+    k_tile_seg<<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(samp_off, seg_n, cnt, tile_seg, L.tiles_cap);
+    phase(1);
+
+    StepTileArgs ta;
+    ta.segs      = segs;
+    ta.samp_off  = samp_off;
+    ta.tile_seg  = tile_seg;
+    ta.counters  = cnt;
+    ta.origin    = origin;
+    ta.direction = direction;
+    ta.node_min  = d->node_min;
+    ta.node_max  = d->node_max;
+    ta.grid      = s->grid;
+    ta.grid_grad = s->grid_grad;
+    ta.decoder   = s->decoder;
+    ta.dec_part  = dec_part;
+    ta.dpred     = dpred;
+    ta.partial   = partial;
+    ta.seed      = seed;
+    ta.step      = (uint32_t)step;
+    ta.G         = d->G;
+    ta.beta      = d->softplus_beta;
+    ok           = ok && launch_tiles_any(d->C, false, ta, st) == cudaSuccess;
+    phase(2);
+    const float invR = (float)(1.0 / (double)R);
+    k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, ray_seg_off, partial, b->target, dpred, out->prediction, loss_part,
+                                               invR, cnt + 0);
+    k_loss_final<<<1, 1024, 0, st>>>(loss_part, L.loss_blocks, out->loss, invR);
+    phase(3);
+    ok = ok && launch_tiles_any(d->C, true, ta, st) == cudaSuccess;
+    phase(4);
+
+    const double bc1g = 1.0 - std::pow((double)d->beta1, step);
+    const double bc2g = 1.0 - std::pow((double)d->beta2, step);
+    const int P       = (int)decoder_params(d->C);
+    k_dec_reduce_adam<<<(P + 255) / 256, 256, 0, st>>>(dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
+                                                        s->decoder_m, s->decoder_v, d->beta1, d->beta2, d->eps,
+                                                        (float)(d->lr_decoder / bc1g), (float)std::sqrt(bc2g));
+    const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;
+    const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
+    k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
+                                  (float)(d->lr_grid / bc1g), (float)std::sqrt(bc2g), 1);
+    phase(5);
+    ok = ok && cudaGetLastError() == cudaSuccess;
+    return ok ? NEAT_OK : NEAT_ERR_CUDA;
+}

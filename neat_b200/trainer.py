@@ -1,0 +1,128 @@
+"""Fused training step: one C-ABI call per Trainer::TrainStep iteration
+(samples/reconstruct.cpp:362-403: GetRays -> CreateSamplesForRays(jitter) ->
+ComputeImage -> MSE -> backward -> OptimizerStep).
+
+FusedTrainer owns the device state (grid in channel-last layout, decoder,
+Adam moments, gradient scratch, step workspace) and issues neat_train_step on
+the current stream.  Nothing is synchronised inside a step; the loss stays on
+the device until the caller reads it.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from .api import CameraModel, decoder_init, grid_init
+from .tree import HyperTreeBase
+
+
+class FusedTrainer:
+    def __init__(self, tree: HyperTreeBase, camera: CameraModel, num_features=4, grid_size=17,
+                 max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
+                 decoder=None, seg_capacity_per_ray=None, device="cuda"):
+        self.dev = torch.device(device)
+        self.tree, self.camera = tree, camera
+        self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
+        self.seed = int(seed)
+        A = tree.NumActiveNodes()
+        self.A = A
+        gen = torch.Generator().manual_seed(seed)
+        if grid is None:
+            grid = grid_init(A, self.C, self.G, gen)
+        if decoder is None:
+            decoder = decoder_init(self.C, gen)
+        lib = _lib.load()
+        self.lib = lib
+        grid = grid.to(self.dev, torch.float32).contiguous()
+        if tuple(grid.shape) != (A, self.C, self.G, self.G, self.G):
+            raise ValueError("grid must be [num_active, C, G, G, G]")
+        self.grid = torch.empty((A, self.G, self.G, self.G, self.C), dtype=torch.float32, device=self.dev)
+        _lib.check(lib.neat_grid_to_channel_last(grid.data_ptr(), self.grid.data_ptr(), A, self.C, self.G,
+                                                 self._stream()), "neat_grid_to_channel_last")
+        self.grid_m = torch.zeros_like(self.grid)
+        self.grid_v = torch.zeros_like(self.grid)
+        self.grid_grad = torch.zeros_like(self.grid)
+        self.decoder = decoder.to(self.dev, torch.float32).contiguous().clone()
+        if self.decoder.numel() != lib.neat_decoder_params(self.C):
+            raise ValueError("decoder has the wrong number of parameters")
+        self.decoder_m = torch.zeros_like(self.decoder)
+        self.decoder_v = torch.zeros_like(self.decoder)
+        self.decoder_grad = torch.zeros_like(self.decoder)
+        self.tables = tree.device_tables(self.dev)
+        # a line crosses at most 3 * 2^D - 2 cells of a 2^D grid
+        self.seg_per_ray = seg_capacity_per_ray or min(_lib.NEAT_MAX_HITS_PER_RAY, 3 * (1 << tree.max_depth))
+        self.loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
+        self.counters = torch.zeros(4, dtype=torch.int64, device=self.dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.desc = _lib.StepDesc(
+            tree_table=self.tables["table"].data_ptr(), num_active=A, max_depth=tree.max_depth,
+            node_min=self.tables["min"].data_ptr(), node_max=self.tables["max"].data_ptr(), w=camera.w, h=camera.h,
+            intrinsics=camera.intrinsics.data_ptr(), rotation=camera.rotation.data_ptr(),
+            translation=camera.translation.data_ptr(), C=self.C, G=self.G, softplus_beta=float(softplus_beta),
+            max_samples_per_node=self.M, lr_grid=float(lr_grid), lr_decoder=float(lr_decoder), beta1=0.9,
+            beta2=0.999, eps=1e-8, seg_capacity=0)
+        self.state = _lib.StepState(
+            grid=self.grid.data_ptr(), grid_m=self.grid_m.data_ptr(), grid_v=self.grid_v.data_ptr(),
+            grid_grad=self.grid_grad.data_ptr(), decoder=self.decoder.data_ptr(),
+            decoder_m=self.decoder_m.data_ptr(), decoder_v=self.decoder_v.data_ptr(),
+            decoder_grad=self.decoder_grad.data_ptr())
+        self.ws = None
+        self.ws_rays = 0
+        self.step_id = 0
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.dev).cuda_stream
+
+    def reserve(self, num_rays):
+        """Allocate the step workspace for batches of up to num_rays rays."""
+        if self.ws is not None and num_rays <= self.ws_rays:
+            return
+        self.desc.seg_capacity = int(num_rays) * self.seg_per_ray
+        nbytes = self.lib.neat_train_step_workspace_bytes(ctypes.byref(self.desc), int(num_rays))
+        if nbytes == 0:
+            raise _lib.NeatError(_lib.NEAT_ERR_UNSUPPORTED, "neat_train_step_workspace_bytes")
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        self.ws_rays = int(num_rays)
+
+    def step(self, uv, image_id, target, prediction=None, phase_events=None):
+        """One fused forward+backward+Adam step on a ray batch; returns the
+        device loss tensor (mean squared projection error of the batch).
+        phase_events: optional list of NEAT_STEP_PHASES torch.cuda.Event
+        (enable_timing) recorded at the step's phase boundaries."""
+        R = uv.shape[0]
+        self.reserve(R)
+        self.step_id += 1
+        batch = _lib.StepBatch(uv=uv.data_ptr(), image_id=image_id.data_ptr(), target=target.data_ptr(), num_rays=R)
+        ev = None
+        if phase_events is not None:
+            if len(phase_events) != _lib.NEAT_STEP_PHASES:
+                raise ValueError("phase_events needs NEAT_STEP_PHASES events")
+            self._ev_arr = (ctypes.c_void_p * _lib.NEAT_STEP_PHASES)(*[e.cuda_event for e in phase_events])
+            ev = ctypes.cast(self._ev_arr, ctypes.c_void_p)
+        out = _lib.StepOut(loss=self.loss.data_ptr(), counters=self.counters.data_ptr(),
+                           status=self.status.data_ptr(),
+                           prediction=prediction.data_ptr() if prediction is not None else None,
+                           phase_events=ev)
+        rc = self.lib.neat_train_step(ctypes.byref(self.desc), ctypes.byref(self.state), ctypes.byref(batch),
+                                      self.seed, self.step_id, ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
+                                      self._stream())
+        _lib.check(rc, "neat_train_step")
+        return self.loss
+
+    def check_status(self):
+        st = int(self.status.item())
+        if st:
+            self.status.zero_()
+            raise _lib.NeatError(st, "neat_train_step")
+
+    def grid_reference_layout(self):
+        out = torch.empty((self.A, self.C, self.G, self.G, self.G), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.neat_grid_from_channel_last(self.grid.data_ptr(), out.data_ptr(), self.A, self.C, self.G,
+                                                        self._stream()), "neat_grid_from_channel_last")
+        return out
+
+    def grad_reference_layout(self, t):
+        out = torch.empty((self.A, self.C, self.G, self.G, self.G), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.neat_grid_from_channel_last(t.data_ptr(), out.data_ptr(), self.A, self.C, self.G,
+                                                        self._stream()), "neat_grid_from_channel_last")
+        return out

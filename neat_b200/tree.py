@@ -1,0 +1,146 @@
+"""Octree node tables (HyperTreeBaseImpl, src/structure/HyperTree.h:98-243).
+
+Construction follows HyperTree.cpp:11-132: breadth-first node ids, root 0 is
+[-1,1]^3, child i of a node takes the upper half on axis k when bit k of i is
+set; every coordinate is produced by float32 midpoints, so all boxes lie on
+the dyadic plane grid of the tree depth.  SetActive/UpdateActive follow
+HyperTree.cpp:163-206: active ids ascending, node_active_prefix_sum[n] is the
+node's grid row or -1.
+
+The tables are built on the host (the reference builds them on the CPU too);
+device copies feed the CUDA kernels.
+"""
+import heapq
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class HyperTreeBase:
+    def __init__(self, d=3, max_depth=4):
+        if d != 3:
+            raise ValueError("only the 3-D tree is implemented (the reference dispatches D=3 only)")
+        if not 1 <= max_depth <= 7:
+            raise ValueError("max_depth must be in [1, 7]")
+        self.D = d
+        self.max_depth = max_depth
+        ns = 1 << d
+        n = sum(ns ** i for i in range(max_depth + 1))
+        pmin = np.empty((n, 3), np.float32)
+        pmax = np.empty((n, 3), np.float32)
+        depth = np.zeros(n, np.int32)
+        parent = np.full(n, -1, np.int32)
+        children = np.full((n, ns), -1, np.int32)
+        pmin[0] = -1.0
+        pmax[0] = 1.0
+        cur, layer_start, layer_count = 1, 0, 1
+        for dep in range(1, max_depth + 1):
+            nxt = cur
+            ids = np.arange(layer_start, layer_start + layer_count)
+            center = (pmin[ids] + pmax[ids]) * np.float32(0.5)
+            for j, nid in enumerate(ids):
+                for i in range(ns):
+                    bits = np.array([(i >> k) & 1 for k in range(3)], bool)
+                    pmin[cur] = np.where(bits, center[j], pmin[nid])
+                    pmax[cur] = np.where(bits, pmax[nid], center[j])
+                    children[nid, i] = cur
+                    depth[cur] = dep
+                    parent[cur] = nid
+                    cur += 1
+            layer_start, layer_count = nxt, layer_count * ns
+        self.node_position_min = pmin
+        self.node_position_max = pmax
+        self.node_depth = depth
+        self.node_parent = parent
+        self.node_children = children
+        self.node_active = np.zeros(n, np.int32)
+        self._dev = {}
+        self.SetActive(0)
+
+    # --- active set (HyperTree.cpp:163-206) ---
+    def NumNodes(self):
+        return self.node_position_min.shape[0]
+
+    def NumActiveNodes(self):
+        return int(self.active_node_ids.shape[0])
+
+    def SetActive(self, depth):
+        self.node_active = (self.node_depth == depth).astype(np.int32)
+        self.UpdateActive()
+
+    def SetActiveNodes(self, node_ids):
+        act = np.zeros(self.NumNodes(), np.int32)
+        act[np.asarray(node_ids, np.int64)] = 1
+        self.node_active = act
+        self.UpdateActive()
+
+    def UpdateActive(self):
+        ids = np.nonzero(self.node_active == 1)[0].astype(np.int64)
+        pre = np.full(self.NumNodes(), -1, np.int64)
+        pre[ids] = np.arange(ids.shape[0], dtype=np.int64)
+        self.active_node_ids = ids
+        self.node_active_prefix_sum = pre
+        self._dev = {}
+
+    def GlobalNodeIdToLocalActiveId(self, node_id):
+        if isinstance(node_id, torch.Tensor):
+            return self.device_tables(node_id.device)["prefix"].index_select(0, node_id.reshape(-1)).reshape(
+                node_id.shape)
+        return self.node_active_prefix_sum[np.asarray(node_id)]
+
+    # --- device tables ---
+    def device_tables(self, device="cuda"):
+        device = torch.device(device)
+        key = str(device)
+        if key not in self._dev:
+            t = {
+                "min": torch.from_numpy(self.node_position_min).to(device),
+                "max": torch.from_numpy(self.node_position_max).to(device),
+                "active": torch.from_numpy(self.active_node_ids).to(device),
+                "prefix": torch.from_numpy(self.node_active_prefix_sum).to(device),
+            }
+            if device.type == "cuda":
+                lib = _lib.load()
+                A = self.NumActiveNodes()
+                table = torch.empty(max(lib.neat_tree_table_bytes(A), 16), dtype=torch.uint8, device=device)
+                status = torch.zeros(1, dtype=torch.int32, device=device)
+                stream = torch.cuda.current_stream(device).cuda_stream
+                _lib.check(lib.neat_tree_prepare(t["min"].data_ptr(), t["max"].data_ptr(), t["active"].data_ptr(), A,
+                                                 self.max_depth, table.data_ptr(), status.data_ptr(), stream),
+                           "neat_tree_prepare")
+                st = int(status.item())
+                if st:
+                    raise _lib.NeatError(st, "neat_tree_prepare")
+                t["table"] = table
+            self._dev[key] = t
+        return self._dev[key]
+
+    # --- adaptive structure (stands in for the reference's MIP optimizer) ---
+    def RefineByVariance(self, density_fn, target_active, samples_per_axis=6, start_depth=1):
+        """Greedy refinement: start from all nodes of start_depth active, then
+        repeatedly split the active node whose sampled density variance is the
+        largest (ties: lower id) until target_active is reached or no active
+        node can split.  density_fn(points [N,3] f64) -> [N] f64."""
+        s = samples_per_axis
+        g = (np.arange(s, dtype=np.float64) + 0.5) / s
+        lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+        N = self.NumNodes()
+        lo = self.node_position_min.astype(np.float64)
+        hi = self.node_position_max.astype(np.float64)
+        pts = lo[:, None, :] + lattice[None, :, :] * (hi - lo)[:, None, :]
+        dens = np.asarray(density_fn(pts.reshape(-1, 3)), np.float64).reshape(N, -1)
+        var = dens.var(axis=1)
+        active = set(np.nonzero(self.node_depth == start_depth)[0].tolist())
+        heap = [(-var[i], i) for i in active if self.node_depth[i] < self.max_depth]
+        heapq.heapify(heap)
+        while len(active) + 7 <= target_active and heap:
+            _, nid = heapq.heappop(heap)
+            active.discard(nid)
+            for c in self.node_children[nid]:
+                active.add(int(c))
+                if self.node_depth[c] < self.max_depth:
+                    heapq.heappush(heap, (-var[c], int(c)))
+        self.SetActiveNodes(sorted(active))
+        return self

@@ -1,0 +1,310 @@
+"""Oracle for the NeAT forward-projection training step -- TEST INFRASTRUCTURE.
+
+Two layers:
+* ctypes wrappers of oracle/libneat_oracle.so (the C restatement in
+  neat_oracle.c: tree tables, rays, slab test, CreateSamplesForRays, IGS,
+  synthetic projector), built by oracle/Makefile;
+* step_f64: a float64 CPU restatement (torch f64 autograd) of
+  ComputeImage -> MSE -> backward -> Adam on the oracle's SampleList:
+    local coords       src/structure/HyperTree.cu:177-192
+    IGS (trilinear)    src/modules/IndirectGridSample3D.cu:27-191
+    FCBlock + softplus src/geometry/ImplicitNet.h:18-73, src/geometry/geometry.cpp:102-163
+    integral           src/geometry/geometry.cpp:393-424 (index_add_)
+    loss               samples/reconstruct.cpp:378-386 (mean of squares)
+    Adam               src/geometry/geometry.h:66-88 (torch::optim::Adam)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module.  The product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libneat_oracle.so")
+
+_f = ctypes.c_float
+_d = ctypes.c_double
+_i = ctypes.c_int
+_l = ctypes.c_long
+_p = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+
+_SIGS = {
+    "oracle_philox": (None, [_u64, _u32, _u32, _u32, _u32, _p]),
+    "oracle_uniform": (_f, [_u64, _u32, _u32, _u32, _u32]),
+    "oracle_tree_num_nodes": (_i, [_i]),
+    "oracle_tree_build": (None, [_i, _p, _p, _p, _p, _p]),
+    "oracle_make_rays": (None, [_i, _p, _p, _i, _i, _p, _p, _p, _p, _p]),
+    "oracle_intersect_box": (_i, [_p, _p, _p, _p, _p, _p]),
+    "oracle_node_diag": (_f, [_p, _p]),
+    "oracle_create_samples": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _i, _u64, _u32, _l, _p, _p, _p, _p, _p, _p, _p]),
+    "oracle_ray_segments": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _l, _p, _p, _p, _p, _p, _p, _p]),
+    "oracle_local_samples": (None, [_l, _p, _p, _p, _p, _p]),
+    "oracle_igs_forward": (None, [_p, _l, _i, _i, _i, _i, _p, _p, _l, _p]),
+    "oracle_igs_backward": (None, [_p, _l, _i, _i, _i, _i, _p, _p, _l, _p, _p, _p]),
+    "oracle_phantom_line": (_d, [_p, _i, _p, _p]),
+    "oracle_phantom_density": (_d, [_p, _i, _p]),
+    "oracle_project": (None, [_p, _i, _i, _i, _i, _p, _p, _p, _p]),
+    "oracle_project_pixels": (None, [_p, _i, _l, _p, _p, _p, _p, _p, _p, _p]),
+    "oracle_phantom_density_batch": (None, [_p, _i, _l, _p, _p]),
+}
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        for k, (r, a) in _SIGS.items():
+            fn = getattr(L, k)
+            fn.restype = r
+            fn.argtypes = a
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# --------------------------------------------------------------------------
+# wrappers
+# --------------------------------------------------------------------------
+def uniform(seed, c0, c1, c2, c3):
+    return lib().oracle_uniform(seed, c0, c1, c2, c3)
+
+
+def philox(seed, c0, c1, c2, c3):
+    out = np.zeros(4, np.uint32)
+    lib().oracle_philox(seed, c0, c1, c2, c3, _ptr(out))
+    return out
+
+
+def tree_build(max_depth):
+    N = lib().oracle_tree_num_nodes(max_depth)
+    pmin = np.zeros((N, 3), np.float32)
+    pmax = np.zeros((N, 3), np.float32)
+    depth = np.zeros(N, np.int32)
+    parent = np.zeros(N, np.int32)
+    children = np.zeros((N, 8), np.int32)
+    lib().oracle_tree_build(max_depth, _ptr(pmin), _ptr(pmax), _ptr(depth), _ptr(parent), _ptr(children))
+    return dict(min=pmin, max=pmax, depth=depth, parent=parent, children=children)
+
+
+def make_rays(uv, image_id, w, h, intr, rot, trans):
+    uv = _c(uv, np.float32)
+    image_id = _c(image_id, np.int32)
+    R = uv.shape[0]
+    o = np.zeros((R, 3), np.float32)
+    d = np.zeros((R, 3), np.float32)
+    lib().oracle_make_rays(R, _ptr(uv), _ptr(image_id), w, h, _ptr(_c(intr, np.float64)), _ptr(_c(rot, np.float64)),
+                           _ptr(_c(trans, np.float64)), _ptr(o), _ptr(d))
+    return o, d
+
+
+def intersect_box(pmin, pmax, o, d):
+    pmin, pmax, o, d = (_c(x, np.float32) for x in (pmin, pmax, o, d))
+    t0 = np.zeros(1, np.float32)
+    t1 = np.zeros(1, np.float32)
+    hit = lib().oracle_intersect_box(_ptr(pmin), _ptr(pmax), _ptr(o), _ptr(d), _ptr(t0), _ptr(t1))
+    return bool(hit), float(t0[0]), float(t1[0])
+
+
+def create_samples(o, d, active_ids, pmin, pmax, M, jitter, seed=0, step=1, cap=None):
+    o, d = _c(o, np.float32), _c(d, np.float32)
+    act = _c(active_ids, np.int64)
+    pmin, pmax = _c(pmin, np.float32), _c(pmax, np.float32)
+    R = o.shape[0]
+    if cap is None:
+        cap = max(16, int(R * M * 3 * (1 << 5)))
+    out = dict(coords=np.zeros((cap, 3), np.float32), ray_t=np.zeros(cap, np.float32),
+               weight=np.zeros(cap, np.float32), ray_index=np.zeros(cap, np.int64),
+               local_index=np.zeros(cap, np.int64), node_id=np.zeros(cap, np.int64))
+    mx = np.zeros(1, np.int32)
+    S = lib().oracle_create_samples(R, _ptr(o), _ptr(d), act.shape[0], _ptr(act), _ptr(pmin), _ptr(pmax), M,
+                                    int(jitter), seed, step, cap, _ptr(out["coords"]), _ptr(out["ray_t"]),
+                                    _ptr(out["weight"]), _ptr(out["ray_index"]), _ptr(out["local_index"]),
+                                    _ptr(out["node_id"]), _ptr(mx))
+    if S < 0:
+        raise RuntimeError(f"oracle_create_samples failed ({S})")
+    res = {k: v[:S].copy() for k, v in out.items()}
+    res["max_per_ray"] = int(mx[0])
+    return res
+
+
+def ray_segments(o, d, active_ids, pmin, pmax, M, cap=None):
+    o, d = _c(o, np.float32), _c(d, np.float32)
+    act = _c(active_ids, np.int64)
+    pmin, pmax = _c(pmin, np.float32), _c(pmax, np.float32)
+    R = o.shape[0]
+    cap = cap or R * 256
+    seg = {k: np.zeros(cap, t) for k, t in (("ray", np.int32), ("node", np.int32), ("local", np.int32),
+                                            ("tmin", np.float32), ("tmax", np.float32), ("n", np.int32))}
+    nseg = np.zeros(R, np.int32)
+    ns = lib().oracle_ray_segments(R, _ptr(o), _ptr(d), act.shape[0], _ptr(act), _ptr(pmin), _ptr(pmax), M, cap,
+                                   _ptr(seg["ray"]), _ptr(seg["node"]), _ptr(seg["local"]), _ptr(seg["tmin"]),
+                                   _ptr(seg["tmax"]), _ptr(seg["n"]), _ptr(nseg))
+    if ns < 0:
+        raise RuntimeError(f"oracle_ray_segments failed ({ns})")
+    res = {k: v[:ns].copy() for k, v in seg.items()}
+    res["ray_nseg"] = nseg
+    return res
+
+
+def local_samples(g, node_id, pmin, pmax):
+    g = _c(g, np.float32)
+    nid = _c(node_id, np.int64)
+    out = np.zeros_like(g)
+    lib().oracle_local_samples(g.shape[0], _ptr(g), _ptr(nid), _ptr(_c(pmin, np.float32)), _ptr(_c(pmax, np.float32)),
+                               _ptr(out))
+    return out
+
+
+def igs_forward(grid, index, uv):
+    grid = _c(grid, np.float32)
+    N, C, Z, Y, X = grid.shape
+    index = _c(index, np.int64)
+    uv = _c(uv, np.float32)
+    out = np.zeros((index.shape[0], C), np.float32)
+    lib().oracle_igs_forward(_ptr(grid), N, C, Z, Y, X, _ptr(index), _ptr(uv), index.shape[0], _ptr(out))
+    return out
+
+
+def igs_backward(grid, index, uv, grad_out):
+    grid = _c(grid, np.float32)
+    N, C, Z, Y, X = grid.shape
+    index = _c(index, np.int64)
+    uv = _c(uv, np.float32)
+    go = _c(grad_out, np.float32)
+    gg = np.zeros_like(grid)
+    gu = np.zeros_like(uv)
+    lib().oracle_igs_backward(_ptr(grid), N, C, Z, Y, X, _ptr(index), _ptr(uv), index.shape[0], _ptr(go), _ptr(gg),
+                              _ptr(gu))
+    return gg, gu
+
+
+def project(objects, n_img, w, h, intr, rot, trans):
+    obj = _c(objects, np.float64)
+    out = np.zeros((n_img, h, w), np.float32)
+    lib().oracle_project(_ptr(obj), obj.shape[0], n_img, w, h, _ptr(_c(intr, np.float64)), _ptr(_c(rot, np.float64)),
+                         _ptr(_c(trans, np.float64)), _ptr(out))
+    return out
+
+
+def phantom_line(objects, o, d):
+    obj = _c(objects, np.float64)
+    return lib().oracle_phantom_line(_ptr(obj), obj.shape[0], _ptr(_c(o, np.float64)), _ptr(_c(d, np.float64)))
+
+
+def phantom_density(objects, points):
+    obj = _c(objects, np.float64)
+    pts = _c(points, np.float64).reshape(-1, 3)
+    out = np.zeros(pts.shape[0], np.float64)
+    lib().oracle_phantom_density_batch(_ptr(obj), obj.shape[0], pts.shape[0], _ptr(pts), _ptr(out))
+    return out
+
+
+def project_pixels(objects, img, px, py, intr, rot, trans):
+    obj = _c(objects, np.float64)
+    img, px, py = _c(img, np.int32), _c(px, np.int32), _c(py, np.int32)
+    out = np.zeros(img.shape[0], np.float32)
+    lib().oracle_project_pixels(_ptr(obj), obj.shape[0], img.shape[0], _ptr(img), _ptr(px), _ptr(py),
+                                _ptr(_c(intr, np.float64)), _ptr(_c(rot, np.float64)), _ptr(_c(trans, np.float64)),
+                                _ptr(out))
+    return out
+
+
+# --------------------------------------------------------------------------
+# float64 step
+# --------------------------------------------------------------------------
+def _trilinear_f64(torch, grid, row, uvw):
+    """IGS in f64 with autograd: grid [N,C,G,G,G] (z,y,x), uvw [S,3] (x,y,z)."""
+    N, C, Z, Y, X = grid.shape
+    dims = torch.tensor([X - 1, Y - 1, Z - 1], dtype=torch.float64)
+    p = (uvw + 1) / 2 * dims
+    p0 = torch.floor(p)
+    f = p - p0
+    i0 = p0.long()
+    out = 0
+    for q in range(8):
+        bx, by, bz = q & 1, (q >> 1) & 1, (q >> 2) & 1
+        wx = f[:, 0] if bx else 1 - f[:, 0]
+        wy = f[:, 1] if by else 1 - f[:, 1]
+        wz = f[:, 2] if bz else 1 - f[:, 2]
+        ix = (i0[:, 0] + bx).clamp(0, X - 1)
+        iy = (i0[:, 1] + by).clamp(0, Y - 1)
+        iz = (i0[:, 2] + bz).clamp(0, Z - 1)
+        v = grid[row, :, iz, iy, ix]  # [S, C]
+        out = out + v * (wx * wy * wz)[:, None]
+    return out
+
+
+def decoder_f64(torch, x, dec, C, beta):
+    H = 64
+    W1, b1, W2, b2, W3, b3 = torch.split(dec, [H * C, H, H * H, H, H, 1])
+    h1 = torch.nn.functional.silu(x @ W1.reshape(H, C).T + b1)
+    h2 = torch.nn.functional.silu(h1 @ W2.reshape(H, H).T + b2)
+    y = h2 @ W3.reshape(1, H).T + b3
+    return torch.nn.functional.softplus(y, beta=beta, threshold=20.0)[:, 0]
+
+
+def image_f64(samples, grid, dec, node_min, node_max, prefix, R, beta=2.0):
+    """Forward projection in f64 with autograd graph; returns (pred [R], ctx)."""
+    import torch
+    g = torch.from_numpy(samples["coords"]).double()
+    nid = torch.from_numpy(samples["node_id"])
+    mn = torch.from_numpy(node_min).double()[nid]
+    mx = torch.from_numpy(node_max).double()[nid]
+    local = (g - mn) / (mx - mn) * 2 - 1
+    row = torch.from_numpy(prefix[samples["node_id"]])
+    C = grid.shape[1]
+    feat = _trilinear_f64(torch, grid, row, local)
+    dens = decoder_f64(torch, feat, dec, C, beta)
+    val = dens * torch.from_numpy(samples["weight"]).double()
+    pred = torch.zeros(R, dtype=torch.float64).index_add(0, torch.from_numpy(samples["ray_index"]), val)
+    return pred
+
+
+def adam_f64(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):
+    m = b1 * m + (1 - b1) * g
+    v = b2 * v + (1 - b2) * g * g
+    bc1 = 1 - b1 ** step
+    bc2 = 1 - b2 ** step
+    p = p - (lr / bc1) * m / (np.sqrt(v) / np.sqrt(bc2) + eps)
+    return p, m, v
+
+
+def step_f64(samples, grid_ref, dec, target, node_min, node_max, prefix, beta=2.0, lr_grid=1e-2, lr_decoder=5e-5,
+             step=1, state=None):
+    """One training step in f64.  grid_ref [A,C,G,G,G], dec packed.  Returns
+    dict(loss, pred, grad_grid, grad_dec, grid, dec, state)."""
+    import torch
+    R = target.shape[0]
+    grid = torch.from_numpy(np.asarray(grid_ref, np.float64)).requires_grad_(True)
+    d = torch.from_numpy(np.asarray(dec, np.float64)).requires_grad_(True)
+    pred = image_f64(samples, grid, d, node_min, node_max, prefix, R, beta)
+    loss = ((pred - torch.from_numpy(np.asarray(target, np.float64))) ** 2).mean()
+    loss.backward()
+    gg = grid.grad.numpy()
+    gd = d.grad.numpy()
+    if state is None:
+        state = dict(gm=np.zeros_like(gg), gv=np.zeros_like(gg), dm=np.zeros_like(gd), dv=np.zeros_like(gd))
+    new_grid, gm, gv = adam_f64(grid.detach().numpy(), gg, state["gm"], state["gv"], lr_grid, step)
+    new_dec, dm, dv = adam_f64(d.detach().numpy(), gd, state["dm"], state["dv"], lr_decoder, step)
+    return dict(loss=float(loss.detach()), pred=pred.detach().numpy(), grad_grid=gg, grad_dec=gd, grid=new_grid, dec=new_dec,
+                state=dict(gm=gm, gv=gv, dm=dm, dv=dv))

@@ -1,0 +1,264 @@
+"""GPU parity: every CUDA entry point against the oracle on the same inputs.
+
+Bars: bit-exact for rays, hit lists, sample counts, sample positions/weights,
+node indexing (the decisions are integer/ordering work) and for the IGS
+forward and grad_uv (same fma order); FP32 tolerances stated per test for
+everything that sums in a different order than the f64 oracle:
+  projection / loss:  1e-5 relative (north-star FP32 bar)
+  gradients:          1e-5 relative in the 2-norm (||g - g64|| / ||g64||);
+                      elementwise checks would flag cancellation noise.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from tests.cases import cfg1_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, dt=None):
+    t = torch.as_tensor(np.ascontiguousarray(a))
+    if dt is not None:
+        t = t.to(dt)
+    return t.cuda()
+
+
+def _rel2(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+@pytest.fixture(scope="module")
+def case(oracle):
+    return cfg1_case(R=4096, oracle=oracle)
+
+
+@pytest.fixture(scope="module")
+def adaptive_case(oracle):
+    # depth-4 tree refined by density variance (mixed node sizes)
+    return cfg1_case(R=2048, seed=3, depth=4, G=9, M=16, oracle=oracle, adaptive=400)
+
+
+def _camera(c):
+    from neat_b200.api import CameraModel
+    return CameraModel(c.w, c.h, c.intr, c.rot, c.trans)
+
+
+# ---------------------------------------------------------------- rays
+def test_make_rays_bit_exact(neat, oracle, case):
+    from neat_b200.api import GetRays
+    rays = GetRays(_camera(case), _dev(case.uv), _dev(case.img))
+    o, d = oracle.make_rays(case.uv, case.img, case.w, case.h, case.intr, case.rot, case.trans)
+    np.testing.assert_array_equal(rays.origin.cpu().numpy(), o)
+    np.testing.assert_array_equal(rays.direction.cpu().numpy(), d)
+
+
+# ---------------------------------------------------------------- samples
+@pytest.mark.parametrize("which", ["cfg1", "adaptive"])
+@pytest.mark.parametrize("jitter", [False, True])
+def test_create_samples_bit_exact(neat, oracle, case, adaptive_case, which, jitter):
+    from neat_b200.api import CreateSamplesForRays, GetRays
+    c = case if which == "cfg1" else adaptive_case
+    rays = GetRays(_camera(c), _dev(c.uv), _dev(c.img))
+    s = CreateSamplesForRays(c.tree, rays, c.M, jitter, seed=11, step=3)
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    ref = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, jitter,
+                                seed=11, step=3)
+    assert s.size() == ref["ray_t"].shape[0] > 0
+    np.testing.assert_array_equal(s.ray_index.cpu().numpy(), ref["ray_index"])
+    np.testing.assert_array_equal(s.node_id.cpu().numpy(), ref["node_id"])
+    np.testing.assert_array_equal(s.local_index_in_ray.cpu().numpy(), ref["local_index"])
+    np.testing.assert_array_equal(s.ray_t.cpu().numpy(), ref["ray_t"])
+    np.testing.assert_array_equal(s.weight.cpu().numpy(), ref["weight"])
+    np.testing.assert_array_equal(s.global_coordinate.cpu().numpy(), ref["coords"])
+    assert s.max_samples_per_ray == ref["max_per_ray"]
+
+
+def test_create_samples_edge_cases(neat, oracle, case):
+    from neat_b200.api import CreateSamplesForRays, RayList
+    T = case.tree
+    # rays that miss the volume, an axis-parallel ray on a node face, a ray
+    # starting inside the volume, an empty batch
+    o = np.array([[5, 5, 5], [-3, 0.0, 0.0], [0.1, 0.2, 0.3], [-3, 0.5, -0.5]], np.float32)
+    d = np.array([[1, 0, 0], [1, 0, 0], [0, 0, 1], [1, 0, 0]], np.float32)
+    s = CreateSamplesForRays(T, RayList(_dev(o), _dev(d)), case.M, False)
+    ref = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, case.M, False)
+    np.testing.assert_array_equal(s.ray_t.cpu().numpy(), ref["ray_t"])
+    np.testing.assert_array_equal(s.node_id.cpu().numpy(), ref["node_id"])
+    assert not np.any(s.ray_index.cpu().numpy() == 0)  # the first ray misses
+    empty = CreateSamplesForRays(T, RayList(_dev(np.zeros((0, 3), np.float32)), _dev(np.zeros((0, 3), np.float32))),
+                                 case.M, True)
+    assert empty.size() == 0
+
+
+def test_create_samples_capacity_status(neat, case):
+    from neat_b200 import _lib
+    from neat_b200.api import GetRays
+    rays = GetRays(_camera(case), _dev(case.uv), _dev(case.img))
+    t = case.tree.device_tables("cuda")
+    R = rays.size()
+    ws = torch.empty(neat.neat_samples_workspace_bytes(R), dtype=torch.uint8, device="cuda")
+    cap = 10
+    bufs = [torch.empty((cap, 3), device="cuda"), torch.empty(cap, device="cuda"), torch.empty(cap, device="cuda")] + \
+           [torch.empty(cap, dtype=torch.int64, device="cuda") for _ in range(3)]
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = neat.neat_create_samples(t["table"].data_ptr(), case.A, case.tree.max_depth, rays.origin.data_ptr(),
+                                  rays.direction.data_ptr(), R, case.M, 0, 0, 1, cap, *[b.data_ptr() for b in bufs],
+                                  cnt.data_ptr(), st.data_ptr(), ws.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(st.item()) & _lib.NEAT_ERR_CAPACITY
+    assert int(cnt[0]) > cap
+
+
+def test_non_dyadic_tree_rejected(neat):
+    from neat_b200 import _lib
+    from neat_b200.tree import HyperTreeBase
+    T = HyperTreeBase(3, 2)
+    T.SetActive(2)
+    T.node_position_max = T.node_position_max.copy()
+    T.node_position_max[T.active_node_ids[0], 0] += np.float32(0.01)
+    with pytest.raises(_lib.NeatError) as e:
+        T.device_tables("cuda")
+    assert e.value.status & _lib.NEAT_ERR_NON_DYADIC
+
+
+def test_bad_input_is_reported(neat):
+    from neat_b200 import _lib
+    assert neat.neat_make_rays(None, None, None, 5, 1, 1, None, None, None, None, None, None) == \
+        _lib.NEAT_ERR_BAD_INPUT
+    assert neat.neat_igs_forward(None, 1, 1, 1, 1, 1, None, None, 3, None, None) == _lib.NEAT_ERR_BAD_INPUT
+
+
+# ---------------------------------------------------------------- IGS
+def test_igs_forward_backward(neat, oracle):
+    from neat_b200.api import IndirectGridSample3D
+    rng = np.random.default_rng(4)
+    grid = rng.uniform(-1, 1, (7, 5, 11, 9, 13)).astype(np.float32)
+    S = 20000
+    idx = rng.integers(0, 7, S)
+    uv = rng.uniform(-1.05, 1.05, (S, 3)).astype(np.float32)
+    uv[:6] = [[-1, -1, -1], [1, 1, 1], [1, -1, 1], [0, 0, 0], [-1, 1, -1], [1, 1, -1]]
+    go = rng.normal(size=(S, 5)).astype(np.float32)
+    g = _dev(grid).requires_grad_(True)
+    p = _dev(uv).requires_grad_(True)
+    out = IndirectGridSample3D(g, _dev(idx), p)
+    np.testing.assert_array_equal(out.detach().cpu().numpy(), oracle.igs_forward(grid, idx, uv))
+    out.backward(_dev(go))
+    gg, gu = oracle.igs_backward(grid, idx, uv, go)
+    np.testing.assert_array_equal(p.grad.cpu().numpy(), gu)
+    assert _rel2(g.grad.cpu().numpy(), gg) < 1e-6
+    # empty batch
+    e = IndirectGridSample3D(g.detach(), _dev(np.zeros(0, np.int64)), _dev(np.zeros((0, 3), np.float32)))
+    assert e.shape == (0, 5)
+
+
+# ---------------------------------------------------------------- ComputeImage
+def test_compute_image_forward_backward(neat, oracle, case):
+    from neat_b200.api import CreateSamplesForRays, GeometryExEx, GetRays
+    c = case
+    rays = GetRays(_camera(c), _dev(c.uv), _dev(c.img))
+    s = CreateSamplesForRays(c.tree, rays, c.M, True, seed=5, step=1)
+    geom = GeometryExEx(c.tree, c.C, c.G)
+    with torch.no_grad():
+        geom.grid_data.copy_(_dev(c.grid))
+        geom.decoder.copy_(_dev(c.dec))
+    img = geom.ComputeImage(s, 1, c.R)
+    loss = ((img[0] - _dev(c.target)) ** 2).mean()
+    loss.backward()
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True, seed=5,
+                                  step=1)
+    ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                          T.node_active_prefix_sum)
+    pred = img[0].detach().cpu().numpy()
+    assert _rel2(pred, ref["pred"]) < 1e-5
+    assert abs(float(loss) - ref["loss"]) < 1e-5 * ref["loss"]
+    assert _rel2(geom.grid_data.grad.cpu().numpy(), ref["grad_grid"]) < 1e-5
+    assert _rel2(geom.decoder.grad.cpu().numpy(), ref["grad_dec"]) < 1e-5
+
+
+# ---------------------------------------------------------------- fused step
+def _trainer(c):
+    from neat_b200.trainer import FusedTrainer
+    return FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
+                        grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec))
+
+
+@pytest.mark.parametrize("which", ["cfg1", "adaptive"])
+def test_fused_step_matches_f64(neat, oracle, case, adaptive_case, which):
+    c = case if which == "cfg1" else adaptive_case
+    tr = _trainer(c)
+    pred = torch.zeros(c.R, device="cuda")
+    loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
+    torch.cuda.synchronize()
+    tr.check_status()
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                                  seed=99, step=1)
+    seg = oracle.ray_segments(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M)
+    cnt = tr.counters.cpu().numpy()
+    assert cnt[0] == seg["n"].shape[0]          # segments (bit-exact hit lists)
+    assert cnt[1] == ref_s["ray_t"].shape[0]    # samples
+    assert cnt[2] == seg["ray_nseg"].max()
+    ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                          T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
+    assert _rel2(pred.cpu().numpy(), ref["pred"]) < 1e-5
+    assert abs(float(loss.item()) - ref["loss"]) <= 1e-5 * ref["loss"]
+    # gradients: decoder grad is kept; grid grad recovered from m = (1-b1) g
+    assert _rel2(tr.decoder_grad.cpu().numpy(), ref["grad_dec"]) < 1e-5
+    gg = tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1
+    assert _rel2(gg, ref["grad_grid"]) < 1e-5
+    # parameters after Adam
+    assert _rel2(tr.grid_reference_layout().cpu().numpy(), ref["grid"]) < 1e-6
+    assert _rel2(tr.decoder.cpu().numpy(), ref["dec"]) < 1e-6
+    assert float(tr.grid_grad.abs().max()) == 0.0  # zero_grad after the step
+
+
+def test_fused_step_trajectory(neat, oracle, case):
+    """Five steps on the same batch: the loss follows the f64 trajectory."""
+    c = case
+    tr = _trainer(c)
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    grid, dec, state = c.grid.astype(np.float64), c.dec.astype(np.float64), None
+    for k in range(1, 6):
+        loss = float(tr.step(_dev(c.uv), _dev(c.img), _dev(c.target)).item())
+        ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                                      seed=99, step=k)
+        r = oracle.step_f64(ref_s, grid, dec, c.target, T.node_position_min, T.node_position_max,
+                            T.node_active_prefix_sum, step=k, state=state)
+        grid, dec, state = r["grid"], r["dec"], r["state"]
+        assert abs(loss - r["loss"]) <= 1e-4 * r["loss"], (k, loss, r["loss"])
+    tr.check_status()
+
+
+def test_fused_step_capacity_overflow_is_reported(neat, case):
+    from neat_b200 import _lib
+    from neat_b200.trainer import FusedTrainer
+    c = case
+    tr = FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, seed=1, seg_capacity_per_ray=1)
+    tr.step(_dev(c.uv), _dev(c.img), _dev(c.target))
+    torch.cuda.synchronize()
+    with pytest.raises(_lib.NeatError) as e:
+        tr.check_status()
+    assert e.value.status & _lib.NEAT_ERR_CAPACITY
+
+
+# ---------------------------------------------------------------- synthetic scans
+def test_projector_matches_oracle(neat, oracle):
+    from neat_b200 import scene as SC
+    objs = SC.ellipsoid_phantom(6, 20, seed=9)
+    sc = SC.SyntheticScene(objs, 4, 48, 40)
+    ref = oracle.project(objs, 4, 48, 40, sc.intrinsics, sc.rotation, sc.translation)
+    np.testing.assert_allclose(sc.projection.cpu().numpy(), ref, rtol=0, atol=1e-6)
+    pts = np.random.default_rng(0).uniform(-1, 1, (500, 3))
+    np.testing.assert_array_equal(sc.density(pts), oracle.phantom_density(objs, pts))

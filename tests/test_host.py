@@ -1,0 +1,132 @@
+"""Host-side tests (no GPU): the C ABI library loads and exports every entry
+point include/neat_b200.h declares; host octree bookkeeping equals the
+oracle's; synthetic geometry conventions; the multi-rank timing helpers of
+bench.py over gloo."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_functions():
+    src = open(os.path.join(ROOT, "include", "neat_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(neat_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    from neat_b200.csrc import build
+    path = build.build()
+    lib = ctypes.CDLL(path)
+    names = _header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    from neat_b200 import _lib
+    assert sorted(_lib.exported_symbols()) == names
+
+
+def test_library_host_calls_without_gpu():
+    from neat_b200 import _lib
+    lib = _lib.load()
+    assert lib.neat_version() >= 1
+    assert lib.neat_decoder_params(8) == 64 * 8 + 64 + 64 * 64 + 64 + 64 + 1
+    assert lib.neat_tree_table_bytes(100) == 1600
+    assert b"capacity" in lib.neat_status_string(_lib.NEAT_ERR_CAPACITY)
+    # argument validation happens on the host before any launch
+    assert lib.neat_make_rays(None, None, None, -1, 16, 16, None, None, None, None, None, None) == \
+        _lib.NEAT_ERR_BAD_INPUT
+    assert lib.neat_tree_prepare(None, None, None, 4, 9, None, None, None) == _lib.NEAT_ERR_BAD_INPUT
+
+
+def test_no_cpu_fallback_when_library_missing(monkeypatch):
+    from neat_b200 import _lib
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", "/nonexistent/libneat_b200.so")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _lib.load()
+
+
+@pytest.mark.parametrize("depth", [1, 2, 4])
+def test_tree_tables_match_oracle(oracle, depth):
+    from neat_b200.tree import HyperTreeBase
+    T = HyperTreeBase(3, depth)
+    t = oracle.tree_build(depth)
+    np.testing.assert_array_equal(T.node_position_min, t["min"])
+    np.testing.assert_array_equal(T.node_position_max, t["max"])
+    np.testing.assert_array_equal(T.node_children, t["children"])
+    np.testing.assert_array_equal(T.node_parent, t["parent"])
+    T.SetActive(depth)
+    assert T.NumActiveNodes() == 8 ** depth
+    assert np.all(np.diff(T.active_node_ids) > 0)
+    pre = T.node_active_prefix_sum
+    assert np.all(pre[T.active_node_ids] == np.arange(8 ** depth))
+    assert np.all(pre[T.node_depth != depth] == -1)
+
+
+def test_refine_by_variance_partitions_the_cube(oracle):
+    from neat_b200 import scene as SC
+    from neat_b200.tree import HyperTreeBase
+    objs = SC.ellipsoid_phantom(8, 10, seed=3)
+    T = HyperTreeBase(3, 4)
+    T.RefineByVariance(lambda p: oracle.phantom_density(objs, p), 300, samples_per_axis=3)
+    A = T.NumActiveNodes()
+    assert 290 <= A <= 300
+    # active leaves tile [-1,1]^3 exactly: volumes sum to 8, no active ancestor of an active node
+    vol = np.prod(T.node_position_max[T.active_node_ids] - T.node_position_min[T.active_node_ids], axis=1)
+    assert abs(vol.sum() - 8.0) < 1e-9
+    act = set(T.active_node_ids.tolist())
+    for n in T.active_node_ids:
+        p = T.node_parent[n]
+        while p >= 0:
+            assert p not in act
+            p = T.node_parent[p]
+    # refinement follows the density: finest nodes where the phantom varies
+    assert T.node_depth[T.active_node_ids].max() == 4
+
+
+def test_cone_beam_geometry():
+    from neat_b200 import scene as SC
+    intr, rot, trans = SC.cone_beam_geometry(8, 64, 48)
+    assert intr.shape == (1, 5) and intr[0, 2] == 31.5 and intr[0, 3] == 23.5
+    # the cube's bounding sphere (radius sqrt 3) spans the detector width
+    assert abs(64 / intr[0, 0] / 2 - np.tan(np.arcsin(np.sqrt(3) / 3))) < 1e-12
+    for q, t in zip(rot, trans):
+        assert abs(np.linalg.norm(q) - 1) < 1e-12
+        assert abs(np.linalg.norm(t) - 3) < 1e-12 and t[2] == 0
+
+
+def _gloo_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    t = torch.tensor([10.0 + rank], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    q.put((rank, float(t.item())))
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo():
+    """bench.py takes the max of the per-rank device times over ranks; the
+    replicas-only multi-GPU path has no other collective."""
+    import multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_gloo_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+    res = sorted(q.get(timeout=5) for _ in range(2))
+    assert res == [(0, 11.0), (1, 11.0)]

@@ -1,0 +1,250 @@
+"""Pins of the CPU oracle (no GPU): known-answer tests and independent
+restatements.  The reference ships no tests or golden vectors; the pins are
+(a) the equivalence the reference documents between IndirectGridSample3D and
+grid_sample(border, align_corners) (src/modules/IndirectGridSample3D.cu:30-40),
+(b) published Philox4x32-10 known answers, (c) hand-derived slab-test and
+sampling cases, (d) committed golden fixtures (tests/golden)."""
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from tests.cases import cfg1_case
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+# --------------------------------------------------------------------------
+# Philox (Random123 kat_vectors, philox4x32_10)
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("seed,ctr,expect", [
+    (0, (0, 0, 0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+    (0xffffffffffffffff, (0xffffffff,) * 4, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+    (0x299f31d0a4093822, (0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344),
+     (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1)),
+])
+def test_philox_known_answers(oracle, seed, ctr, expect):
+    assert tuple(int(v) for v in oracle.philox(seed, *ctr)) == expect
+
+
+def test_uniform_range(oracle):
+    u = np.array([oracle.uniform(3, i, 7, 1, 0x4a495454) for i in range(2000)])
+    assert u.min() >= 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 0.03
+
+
+# --------------------------------------------------------------------------
+# IndirectGridSample3D
+# --------------------------------------------------------------------------
+def _grid_sample_ref(grid, idx, uv):
+    g = torch.from_numpy(grid)[torch.from_numpy(idx)]
+    p = torch.from_numpy(uv)[:, None, None, None, :]
+    return torch.nn.functional.grid_sample(g, p, mode="bilinear", padding_mode="border", align_corners=True)
+
+
+def test_igs_forward_equals_grid_sample(oracle):
+    rng = np.random.default_rng(0)
+    grid = rng.uniform(-1, 1, (6, 4, 11, 9, 7)).astype(np.float32)
+    S = 3000
+    idx = rng.integers(0, 6, S)
+    uv = rng.uniform(-1, 1, (S, 3)).astype(np.float32)
+    uv[:10] = np.array([[-1, -1, -1], [1, 1, 1], [1, -1, 1], [-1, 1, -1], [0, 0, 0], [1, 0, -1], [-1, 0, 1],
+                        [0.5, -0.5, 1], [1, 1, -1], [-1, -1, 1]], np.float32)
+    out = oracle.igs_forward(grid, idx, uv)
+    ref = _grid_sample_ref(grid, idx, uv)[:, :, 0, 0, 0].numpy()
+    np.testing.assert_allclose(out, ref, rtol=0, atol=4e-7)
+
+
+def test_igs_backward_equals_grid_sample_autograd(oracle):
+    rng = np.random.default_rng(1)
+    grid = rng.uniform(-1, 1, (3, 2, 5, 6, 7)).astype(np.float32)
+    S = 400
+    idx = rng.integers(0, 3, S)
+    uv = rng.uniform(-0.999, 0.999, (S, 3)).astype(np.float32)
+    go = rng.normal(size=(S, 2)).astype(np.float32)
+    gg, gu = oracle.igs_backward(grid, idx, uv, go)
+    g = torch.from_numpy(grid).double().requires_grad_(True)
+    p = torch.from_numpy(uv).double().requires_grad_(True)
+    out = torch.nn.functional.grid_sample(g[torch.from_numpy(idx)], p[:, None, None, None, :], mode="bilinear",
+                                          padding_mode="border", align_corners=True)[:, :, 0, 0, 0]
+    (out * torch.from_numpy(go).double()).sum().backward()
+    np.testing.assert_allclose(gg, g.grad.numpy(), rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(gu, p.grad.numpy(), rtol=1e-4, atol=1e-5)
+
+
+def test_igs_out_of_range_is_index_clamped(oracle):
+    """Weights come from unclamped corners, indices are clamped (the
+    reference's border-by-clamp): at uv = 1.5 on a 3-wide axis the x corners
+    are 3 and 4, both clamped to 2, weights (-0.5, 1.5) sum to 1 -> value of
+    the border cell."""
+    grid = np.arange(27, dtype=np.float32).reshape(1, 1, 3, 3, 3)
+    out = oracle.igs_forward(grid, np.array([0]), np.array([[1.5, -1, -1]], np.float32))
+    assert out[0, 0] == pytest.approx(2.0)
+
+
+# --------------------------------------------------------------------------
+# IntersectBoxRayPrecise known answers
+# --------------------------------------------------------------------------
+UNIT = (np.array([-1, -1, -1], np.float32), np.array([1, 1, 1], np.float32))
+
+
+def test_slab_axis_ray(oracle):
+    hit, t0, t1 = oracle.intersect_box(*UNIT, [-3, 0.25, 0.5], [1, 0, 0])
+    assert hit and t0 == 2.0 and t1 == 4.0
+
+
+def test_slab_parallel_outside_and_on_max_face(oracle):
+    assert not oracle.intersect_box(*UNIT, [-3, 1.5, 0], [1, 0, 0])[0]
+    # o == max on a parallel axis is outside (o >= max)
+    assert not oracle.intersect_box(*UNIT, [-3, 1.0, 0], [1, 0, 0])[0]
+    # o == min on a parallel axis is inside
+    assert oracle.intersect_box(*UNIT, [-3, -1.0, 0], [1, 0, 0])[0]
+
+
+def test_slab_behind_origin_and_inside(oracle):
+    assert not oracle.intersect_box(*UNIT, [3, 0, 0], [1, 0, 0])[0]
+    hit, t0, t1 = oracle.intersect_box(*UNIT, [0, 0, 0], [1, 0, 0])
+    assert hit and t0 == -1.0 and t1 == 1.0
+
+
+def test_slab_corner_graze(oracle):
+    d = np.array([1, 1, 0], np.float32) / np.float32(math.sqrt(2))
+    hit, t0, t1 = oracle.intersect_box(np.array([0, 0, 0], np.float32), np.array([1, 1, 1], np.float32),
+                                       [-1, 0, 0.5], d)
+    # passes exactly through the edge x=0, y=1: tmin == tmax
+    assert hit and t0 == t1
+
+
+def test_sample_count_rule(oracle):
+    """n = iCeil(((tmax - tmin) / diag) * M) and the 1e-5 skip
+    (src/structure/HyperTree.cu:274-291)."""
+    pmin = np.array([[0, 0, 0]], np.float32)
+    pmax = np.array([[0.5, 0.5, 0.5]], np.float32)
+    diag = np.float32(math.sqrt(0.75))
+    o = np.array([[-1, 0.25, 0.25]], np.float32)
+    d = np.array([[1, 0, 0]], np.float32)
+    s = oracle.create_samples(o, d, np.array([0]), pmin, pmax, 16, False)
+    n = len(s["ray_t"])
+    assert n == math.ceil(float(np.float32(np.float32(0.5) / diag) * np.float32(16)))
+    # a 5e-6 sliver is skipped
+    o2 = np.array([[-1, 0.25, 0.4999975]], np.float32)
+    d2 = np.array([[0, 0, 1]], np.float32)
+    s2 = oracle.create_samples(np.array([[0.25, 0.25, -1]], np.float32), d2, np.array([0]),
+                               np.array([[0, 0, 0]], np.float32), np.array([[0.5, 0.5, 0.000005]], np.float32), 16,
+                               False)
+    assert len(s2["ray_t"]) == 0
+
+
+# --------------------------------------------------------------------------
+# Octree / rays / samples
+# --------------------------------------------------------------------------
+def test_tree_numbering(oracle):
+    t = oracle.tree_build(1)
+    assert t["min"].shape == (9, 3)
+    for i in range(8):
+        bits = [(i >> k) & 1 for k in range(3)]
+        np.testing.assert_array_equal(t["min"][1 + i], [0.0 if b else -1.0 for b in bits])
+        np.testing.assert_array_equal(t["max"][1 + i], [1.0 if b else 0.0 for b in bits])
+        assert t["parent"][1 + i] == 0 and t["children"][0, i] == 1 + i
+    t4 = oracle.tree_build(4)
+    assert t4["min"].shape[0] == 1 + 8 + 64 + 512 + 4096
+    assert (t4["depth"] == 4).sum() == 4096
+
+
+def test_center_ray_passes_origin(oracle):
+    c = cfg1_case(R=4)
+    w = h = 129
+    from neat_b200 import scene as SC
+    intr, rot, trans = SC.cone_beam_geometry(8, w, h)
+    uv = np.array([[0.5, 0.5]] * 8, np.float32)
+    o, d = oracle.make_rays(uv, np.arange(8), w, h, intr, rot, trans)
+    for k in range(8):
+        # closest approach of the central ray to the volume centre
+        oo, dd = o[k].astype(np.float64), d[k].astype(np.float64)
+        closest = oo - np.dot(oo, dd) * dd
+        assert np.linalg.norm(closest) < 1e-6
+        assert abs(np.linalg.norm(oo) - 3.0) < 1e-6
+
+
+def test_samples_canonical_and_weights(oracle):
+    c = cfg1_case(R=512, oracle=oracle)
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True, seed=3)
+    seg = oracle.ray_segments(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M)
+    assert s["ray_t"].shape[0] == seg["n"].sum()
+    # per ray: ray-major, local index contiguous, t increasing across segments
+    ri = s["ray_index"]
+    assert np.all(np.diff(ri) >= 0)
+    for r in np.unique(ri)[:64]:
+        m = ri == r
+        np.testing.assert_array_equal(s["local_index"][m], np.arange(m.sum()))
+        assert np.all(np.diff(s["ray_t"][m]) >= -1e-6)
+    # weights of a segment sum to its length
+    off = 0
+    for k in range(min(len(seg["n"]), 500)):
+        n = seg["n"][k]
+        wsum = s["weight"][off:off + n].astype(np.float64).sum()
+        assert abs(wsum - (seg["tmax"][k] - seg["tmin"][k])) < 1e-5
+        off += n
+    # jitter a=0.5 gives midpoints
+    s0 = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, False)
+    seg_t0 = seg["tmin"][0]
+    step = np.float32(np.float32(seg["tmax"][0] - seg["tmin"][0]) / np.float32(seg["n"][0]))
+    assert s0["ray_t"][0] == np.float32(np.float32(seg_t0 * np.float32(0.5)) +
+                                        np.float32(np.float32(seg_t0 + step) * np.float32(0.5)))
+
+
+def test_projector_matches_numeric_integral(oracle):
+    from neat_b200 import scene as SC
+    objs = SC.ellipsoid_phantom(4, 3, seed=5)
+    objs[-1, 0:3] = objs[0, 0:3]  # put a void inside an ellipsoid
+    rng = np.random.default_rng(2)
+    for _ in range(5):
+        o = np.array([0.1, -3.0, 0.05]) + rng.uniform(-0.2, 0.2, 3)
+        d = np.array([0.0, 1.0, 0.0]) + rng.uniform(-0.1, 0.1, 3)
+        d /= np.linalg.norm(d)
+        t = np.linspace(1.0, 5.0, 40001)
+        dens = oracle.phantom_density(objs, o[None, :] + t[:, None] * d[None, :])
+        num = np.trapezoid(dens, t)
+        ana = oracle.phantom_line(objs, o, d)
+        assert abs(num - ana) < 2e-3 * max(1.0, ana)
+
+
+def test_step_f64_gradient_matches_finite_differences(oracle):
+    c = cfg1_case(R=64, oracle=oracle, n_angles=4, w=32, h=32)
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True, seed=1)
+    base = oracle.step_f64(s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                           T.node_active_prefix_sum)
+    rng = np.random.default_rng(0)
+    flat_idx = np.nonzero(np.abs(base["grad_grid"].reshape(-1)) > 1e-6)[0]
+    for i in rng.choice(flat_idx, 5, replace=False):
+        for arr, gname in ((c.grid, "grad_grid"),):
+            e = 1e-6
+            gp = arr.astype(np.float64).copy().reshape(-1)
+            gm = gp.copy()
+            gp[i] += e
+            gm[i] -= e
+            lp = oracle.step_f64(s, gp.reshape(arr.shape), c.dec, c.target, T.node_position_min, T.node_position_max,
+                                 T.node_active_prefix_sum)["loss"]
+            lm = oracle.step_f64(s, gm.reshape(arr.shape), c.dec, c.target, T.node_position_min, T.node_position_max,
+                                 T.node_active_prefix_sum)["loss"]
+            fd = (lp - lm) / (2 * e)
+            assert abs(fd - base[gname].reshape(-1)[i]) < 1e-6 * max(1.0, abs(fd)) + 1e-9
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "igs_reference_cpu.npz")),
+                    reason="golden fixture not generated")
+def test_igs_golden_from_reference_cpu(oracle):
+    """IGS forward/backward against the reference's own CPU implementation
+    (generated by tests/golden/make_golden.py from oracle/_ref)."""
+    z = np.load(os.path.join(GOLDEN, "igs_reference_cpu.npz"))
+    out = oracle.igs_forward(z["grid"], z["index"], z["uv"])
+    np.testing.assert_allclose(out, z["out"], rtol=0, atol=2e-7)
+    gg, gu = oracle.igs_backward(z["grid"], z["index"], z["uv"], z["grad_out"])
+    np.testing.assert_allclose(gg, z["grad_grid"], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(gu, z["grad_uv"], rtol=1e-5, atol=1e-6)

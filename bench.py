@@ -247,6 +247,9 @@ def main():
 
     # ---- timed: device-resident inputs (value)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(_lib.NEAT_STEP_PHASES)] for _ in range(K)]
+    for row in ev:  # torch creates the CUDA event on first record; the step records it again
+        for e in row:
+            e.record()
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()

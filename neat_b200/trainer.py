@@ -97,7 +97,10 @@ class FusedTrainer:
         if phase_events is not None:
             if len(phase_events) != _lib.NEAT_STEP_PHASES:
                 raise ValueError("phase_events needs NEAT_STEP_PHASES events")
-            self._ev_arr = (ctypes.c_void_p * _lib.NEAT_STEP_PHASES)(*[e.cuda_event for e in phase_events])
+            handles = [e.cuda_event for e in phase_events]
+            if not all(handles):
+                raise ValueError("phase_events must be created (record them once) before use")
+            self._ev_arr = (ctypes.c_void_p * _lib.NEAT_STEP_PHASES)(*handles)
             ev = ctypes.cast(self._ev_arr, ctypes.c_void_p)
         out = _lib.StepOut(loss=self.loss.data_ptr(), counters=self.counters.data_ptr(),
                            status=self.status.data_ptr(),

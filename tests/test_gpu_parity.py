@@ -180,7 +180,7 @@ def test_compute_image_forward_backward(neat, oracle, case):
                           T.node_active_prefix_sum)
     pred = img[0].detach().cpu().numpy()
     assert _rel2(pred, ref["pred"]) < 1e-5
-    assert abs(float(loss) - ref["loss"]) < 1e-5 * ref["loss"]
+    assert abs(float(loss.detach()) - ref["loss"]) < 1e-5 * ref["loss"]
     assert _rel2(geom.grid_data.grad.cpu().numpy(), ref["grad_grid"]) < 1e-5
     assert _rel2(geom.decoder.grad.cpu().numpy(), ref["grad_dec"]) < 1e-5
 

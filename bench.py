@@ -181,10 +181,13 @@ def main():
     ap.add_argument("--impl", default="neat", choices=["neat", "reference"])
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rays", type=int, default=0, help="override rays per batch (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    cfg = WORKLOADS[args.workload]
+    cfg = dict(WORKLOADS[args.workload])
+    if args.rays:
+        cfg["R"] = args.rays
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -91,6 +91,28 @@ int neat_create_samples(const void* table, int num_active, int max_depth, const 
                         int64_t* local_index_in_ray, int64_t* node_id, int64_t* out_count, int* status,
                         void* workspace, neat_stream_t stream);
 
+/* Same as neat_create_samples, but the caller passes no workspace: the call
+ * allocates nothing.  No counterpart in the reference (its sampler always
+ * allocates its outputs and a counter with torch).  It exists for callers that
+ * cannot allocate device memory while they run -- a host framework that has
+ * reserved the GPU's memory for its own pool, or a loop that must not take the
+ * implicit device synchronisation a cudaMalloc costs -- and for bindings that
+ * can only hand over input and output arrays.  Its per-ray counts and offsets
+ * live in one file-scope device array of the library, sized for at most
+ * NEAT_NOALLOC_MAX_RAYS rays (about 3 MB, held on every GPU that loads the
+ * library until the process exits); larger batches are rejected with
+ * NEAT_ERR_CAPACITY before anything is launched.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress); make it before
+ * any stream capture.  Every call on a device shares the one array, so calls
+ * whose work overlaps on the GPU (different streams or threads without
+ * ordering) race and must be serialised by the caller. */
+#define NEAT_NOALLOC_MAX_RAYS (1 << 18)
+int neat_create_samples_noalloc(const void* table, int num_active, int max_depth, const float* origin,
+                                const float* direction, int64_t num_rays, int max_samples_per_node, int jitter,
+                                uint64_t seed, uint32_t step, int64_t capacity, float* coords, float* ray_t,
+                                float* weight, int64_t* ray_index, int64_t* local_index_in_ray, int64_t* node_id,
+                                int64_t* out_count, int* status, neat_stream_t stream);
+
 /* ----------------------------------------------------------------------- */
 /* Local coordinates.                                                        */
 /* Replaces HyperTreeBaseImpl::ComputeLocalSamples (src/structure/HyperTree.cu:177-192): */

@@ -18,6 +18,7 @@ NEAT_ERR_CUDA = 16
 NEAT_ERR_UNSUPPORTED = 32
 NEAT_MAX_HITS_PER_RAY = 256
 NEAT_HIDDEN = 64
+NEAT_NOALLOC_MAX_RAYS = 1 << 18
 
 c_void_p = ctypes.c_void_p
 c_int = ctypes.c_int
@@ -69,6 +70,9 @@ _SIGS = {
     "neat_create_samples": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_int64, c_int, c_int, c_uint64,
                                     c_uint32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p, c_void_p, c_void_p, c_void_p]),
+    "neat_create_samples_noalloc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_int64, c_int, c_int,
+                                            c_uint64, c_uint32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_local_samples": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_igs_forward": (c_int, [c_void_p, c_int64, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_int64,
                                  c_void_p, c_void_p]),

@@ -456,3 +456,90 @@ extern "C" int neat_create_samples(const void* table, int num_active, int max_de
                                                      node_id, status);
     return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// Sampling without a caller workspace.
+//
+// Some callers cannot allocate device memory while they run (a host framework
+// that owns the GPU's memory pool, a latency-bound loop that cannot afford the
+// device-wide synchronisation of cudaMalloc, a binding that only passes input
+// and output arrays).  For them the per-ray counts, offsets and scan partials
+// of the sampler live in this file-scope array, sized for
+// NEAT_NOALLOC_MAX_RAYS rays.  Every GPU that loads the library keeps it until
+// the process exits.  All calls on a device share it: the kernels overwrite
+// every entry they read before reading it, so nothing needs clearing between
+// calls, but calls that overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace neat
+{
+constexpr int64_t kNoAllocRays = NEAT_NOALLOC_MAX_RAYS;
+constexpr size_t kNoAllocNsampBytes = ((size_t)kNoAllocRays * 4 + 255) / 256 * 256;
+constexpr size_t kNoAllocOffBytes   = ((size_t)(kNoAllocRays + 1) * 8 + 255) / 256 * 256;
+constexpr size_t kNoAllocScanBytes  = ((size_t)((kNoAllocRays + SCAN_TILE - 1) / SCAN_TILE + 1) * 8 + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes      = kNoAllocNsampBytes + kNoAllocOffBytes + kNoAllocScanBytes;
+}  // namespace neat
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[neat::kNoAllocBytes];
+
+namespace
+{
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the host-side name is only a stand-in, never a device pointer).
+int noalloc_scratch(char** out)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NEAT_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return NEAT_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev])
+    {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return NEAT_ERR_CUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = (char*)g_noalloc_ptr[dev];
+    return NEAT_OK;
+}
+}  // namespace
+
+extern "C" int neat_create_samples_noalloc(const void* table, int num_active, int max_depth, const float* origin,
+                                           const float* direction, int64_t num_rays, int max_samples_per_node,
+                                           int jitter, uint64_t seed, uint32_t step, int64_t capacity, float* coords,
+                                           float* ray_t, float* weight, int64_t* ray_index,
+                                           int64_t* local_index_in_ray, int64_t* node_id, int64_t* out_count,
+                                           int* status, neat_stream_t stream)
+{
+    if (num_rays < 0 || num_active < 0 || max_depth < 1 || max_depth > kMaxDepth || max_samples_per_node < 1 ||
+        capacity < 0 || !out_count)
+        return NEAT_ERR_BAD_INPUT;
+    if (num_rays > kNoAllocRays) return NEAT_ERR_CAPACITY;  // beyond the static scratch: nothing launched
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(out_count, 0, 2 * sizeof(int64_t), st) != cudaSuccess) return NEAT_ERR_CUDA;
+    if (num_rays == 0) return NEAT_OK;
+    if (!table && num_active > 0) return NEAT_ERR_BAD_INPUT;
+    if (!origin || !direction) return NEAT_ERR_BAD_INPUT;
+    if (capacity > 0 && (!coords || !ray_t || !weight || !ray_index || !local_index_in_ray || !node_id))
+        return NEAT_ERR_BAD_INPUT;
+    char* ws = nullptr;
+    const int e = noalloc_scratch(&ws);
+    if (e != NEAT_OK) return e;
+    int* ray_nsamp    = (int*)ws;
+    int64_t* samp_off = (int64_t*)(ws + kNoAllocNsampBytes);
+    int64_t* scratch  = (int64_t*)(ws + kNoAllocNsampBytes + kNoAllocOffBytes);
+    const unsigned grid = (unsigned)((num_rays + RAY_WARPS - 1) / RAY_WARPS);
+    k_samples_count<<<grid, 32 * RAY_WARPS, 0, st>>>(origin, direction, num_rays, (const NodeEntry*)table, num_active,
+                                                     max_depth, max_samples_per_node, ray_nsamp, out_count, status);
+    if (scan_exclusive<int64_t>(ray_nsamp, nullptr, num_rays, samp_off, scratch, out_count, st) != cudaSuccess)
+        return NEAT_ERR_CUDA;
+    k_samples_write<<<grid, 32 * RAY_WARPS, 0, st>>>(origin, direction, num_rays, (const NodeEntry*)table, num_active,
+                                                     max_depth, max_samples_per_node, jitter, seed, step, samp_off,
+                                                     capacity, coords, ray_t, weight, ray_index, local_index_in_ray,
+                                                     node_id, status);
+    return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
+}

@@ -44,6 +44,9 @@ WORKLOADS = {
                   R=4096, seed=1, cpu_rays=4096),
 }
 METRIC = "train rays/s (fwd+bwd)"
+DECODER_DESC = {"simt": "FP32 FFMA (CUDA cores)",
+                "bf16x3": "tcgen05, FP32-accurate: operands split in 3 BF16 pieces, 6 products, FP32 accumulation",
+                "bf16": "tcgen05, BF16 operands, FP32 accumulation (precision variant)"}
 PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 
 
@@ -182,6 +185,8 @@ def main():
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rays", type=int, default=0, help="override rays per batch (profiling runs only)")
+    ap.add_argument("--decoder", default="bf16x3", choices=["simt", "bf16x3", "bf16"],
+                    help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -224,8 +229,10 @@ def main():
     build.build()
     scene, tree, cam = build_workload(cfg, dev)
     R, K, W = cfg["R"], args.steps, args.warmup
+    path = {"simt": _lib.NEAT_DECODER_SIMT_FP32, "bf16x3": _lib.NEAT_DECODER_TC_BF16X3,
+            "bf16": _lib.NEAT_DECODER_TC_BF16}[args.decoder]
     tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"] + rank,
-                      device=dev)
+                      decoder_path=path, device=dev)
     tr.reserve(R)
     gen = torch.Generator(device=dev)
     gen.manual_seed(1000 + rank)
@@ -328,9 +335,10 @@ def main():
         return
     line = {
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16" if args.decoder == "bf16" else "f32",
         "data": "synthetic",
-        "config": {"workload": cfg["desc"], "rays_per_step": R, "samples_per_step": S, "segments_per_step":
+        "config": {"workload": cfg["desc"], "decoder": DECODER_DESC[args.decoder], "rays_per_step": R, "samples_per_step": S, "segments_per_step":
                    counters[0], "active_nodes": tree.NumActiveNodes(), "parallelism": f"replicas x{world}",
                    "l2": "working set > L2: grid + Adam state %.2f GB per replica" % (
                        4 * 4 * tr.grid.numel() / 1e9)},

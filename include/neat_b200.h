@@ -32,7 +32,8 @@ typedef enum
     NEAT_ERR_TOO_MANY_HITS = 4,  /* > 256 ray-node intersections on one ray (device flag)    */
     NEAT_ERR_NON_DYADIC    = 8,  /* node box not on the dyadic plane grid (device flag)      */
     NEAT_ERR_CUDA          = 16, /* a CUDA launch failed                                      */
-    NEAT_ERR_UNSUPPORTED   = 32  /* configuration the kernels were not built for             */
+    NEAT_ERR_UNSUPPORTED   = 32, /* configuration the kernels were not built for             */
+    NEAT_ERR_TIMEOUT       = 64  /* a bounded wait inside a kernel gave up (device flag)     */
 } neat_status;
 
 /* Maximum intersections one ray may have; the reference keeps 256 in shared
@@ -210,7 +211,21 @@ typedef struct
     float lr_grid, lr_decoder, beta1, beta2, eps;
     /* capacity of the per-step segment buffers */
     int64_t seg_capacity;
+    /* decoder GEMMs: NEAT_DECODER_* */
+    int decoder_path;
 } neat_step_desc;
+
+/* Decoder paths of the fused step.
+ *   SIMT_FP32:  FP32 FFMA on CUDA cores.
+ *   TC_BF16X3:  tcgen05 tensor cores, every operand split into three BF16
+ *               pieces (24 significant bits), the six cross products of piece
+ *               order <= 2 accumulated in FP32 (FP32-level accuracy, checked
+ *               at 1e-5 against the f64 oracle).
+ *   TC_BF16:    tcgen05 tensor cores on BF16 operands, FP32 accumulation
+ *               (the precision variant; error stated against f64). */
+#define NEAT_DECODER_SIMT_FP32 0
+#define NEAT_DECODER_TC_BF16X3 1
+#define NEAT_DECODER_TC_BF16 2
 
 typedef struct
 {

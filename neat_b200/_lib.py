@@ -16,6 +16,10 @@ NEAT_ERR_TOO_MANY_HITS = 4
 NEAT_ERR_NON_DYADIC = 8
 NEAT_ERR_CUDA = 16
 NEAT_ERR_UNSUPPORTED = 32
+NEAT_ERR_TIMEOUT = 64
+NEAT_DECODER_SIMT_FP32 = 0
+NEAT_DECODER_TC_BF16X3 = 1
+NEAT_DECODER_TC_BF16 = 2
 NEAT_MAX_HITS_PER_RAY = 256
 NEAT_HIDDEN = 64
 NEAT_NOALLOC_MAX_RAYS = 1 << 18
@@ -37,7 +41,7 @@ class StepDesc(ctypes.Structure):
         ("intrinsics", c_void_p), ("rotation", c_void_p), ("translation", c_void_p),
         ("C", c_int), ("G", c_int), ("softplus_beta", c_float), ("max_samples_per_node", c_int),
         ("lr_grid", c_float), ("lr_decoder", c_float), ("beta1", c_float), ("beta2", c_float), ("eps", c_float),
-        ("seg_capacity", c_int64),
+        ("seg_capacity", c_int64), ("decoder_path", c_int),
     ]
 
 

@@ -52,6 +52,7 @@ extern "C" const char* neat_status_string(int status)
     if (status & NEAT_ERR_TOO_MANY_HITS) return "more than 256 ray-node intersections on one ray";
     if (status & NEAT_ERR_CAPACITY) return "output or workspace capacity exceeded";
     if (status & NEAT_ERR_NON_DYADIC) return "node box not on the dyadic plane grid of max_depth";
+    if (status & NEAT_ERR_TIMEOUT) return "a bounded wait inside a kernel gave up";
     return "unknown status";
 }
 

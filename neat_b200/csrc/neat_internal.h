@@ -34,4 +34,33 @@ cudaError_t launch_step_rays_write(const float* origin, const float* direction, 
 
 int sm_count();
 
+// Arguments of the node-major sample-tile kernels of the fused step.
+struct StepTileArgs
+{
+    const SegRec* segs;
+    const int* samp_off;
+    const int* tile_seg;
+    const int64_t* counters;
+    const float* origin;
+    const float* direction;
+    const float* node_min;
+    const float* node_max;
+    const float* grid;
+    float* grid_grad;
+    const float* decoder;
+    float* dec_part;
+    const float* dpred;
+    float* partial;
+    int* status;
+    uint64_t seed;
+    uint32_t step;
+    int G;
+    float beta;
+};
+using StepTcArgs = StepTileArgs;
+
+// tcgen05 tile kernels (neat_tc.cu); prec 0 = BF16 operands, 1 = three-piece BF16 split.
+int tc_backward_grid(int C, int prec);
+cudaError_t launch_tiles_tc(int C, int prec, bool bwd, const StepTileArgs& args, cudaStream_t st);
+
 }  // namespace neat

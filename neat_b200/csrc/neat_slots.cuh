@@ -1,0 +1,90 @@
+// neat_slots.cuh -- map the 128 slots of a node-major sample tile to their
+// segments and build each slot's sample (jittered position, weight, local
+// coordinates, trilinear corners).  Shared by the SIMT and tcgen05 tile
+// kernels of the fused step.
+#pragma once
+
+#include "neat_common.cuh"
+#include "neat_internal.h"
+
+namespace neat
+{
+
+constexpr int SLOTS = 128;  // samples per tile
+
+// mark/slot_seg: shared int[128] each.  On return mark[s] is the node-major
+// segment of slot s (tile samples g0 .. g0+127; slots past S map to the last
+// segment).  All threads of the block must call it.
+__device__ __forceinline__ void tile_slot_segments(int64_t g0, int seg_lo, int nseg, const int* __restrict__ samp_off,
+                                                   int* mark, int* slot_seg)
+{
+    const int t = threadIdx.x;
+    for (int i = t; i < SLOTS; i += blockDim.x) mark[i] = (i == 0) ? seg_lo : -1;
+    __syncthreads();
+    for (int i = t; i <= SLOTS; i += blockDim.x)
+    {
+        const int seg = seg_lo + i;
+        if (seg < nseg)
+        {
+            const int64_t o = samp_off[seg];
+            if (o > g0 && o < g0 + SLOTS) mark[(int)(o - g0)] = seg;
+        }
+    }
+    __syncthreads();
+    if (t < SLOTS)
+    {
+        int v = mark[t];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if ((t & 31) >= o) v = max(v, y);
+        }
+        slot_seg[t] = v;
+    }
+    __syncthreads();
+    if (t < SLOTS)
+    {
+        int v = slot_seg[t];
+        for (int w2 = 0; w2 < (t >> 5); ++w2) v = max(v, slot_seg[w2 * 32 + 31]);
+        mark[t] = v;
+    }
+    __syncthreads();
+}
+
+struct SlotSample
+{
+    bool valid;
+    float weight;
+    float lu, lv, lw;  // local coordinates in [-1,1]
+    int ray, rm, row;
+};
+
+// Sample of slot s of segment seg: stratified jitter, o + d t, local coords.
+__device__ __forceinline__ SlotSample slot_sample(const SegRec* __restrict__ segs, const int* __restrict__ samp_off,
+                                                  int seg, int64_t gs, int64_t S, const float* __restrict__ origin,
+                                                  const float* __restrict__ direction,
+                                                  const float* __restrict__ node_min,
+                                                  const float* __restrict__ node_max, uint64_t seed, uint32_t step)
+{
+    SlotSample q;
+    q.valid        = gs < S;
+    const SegRec r = segs[seg];
+    const int j    = q.valid ? (int)(gs - samp_off[seg]) : 0;
+    float ts, ws;
+    seg_sample(r.tmin, r.tmax, r.n, j, true, seed, step, r.ray, r.local_base, ts, ws);
+    const float* o  = origin + 3 * (int64_t)r.ray;
+    const float* d  = direction + 3 * (int64_t)r.ray;
+    const float* mn = node_min + 3 * (int64_t)r.node;
+    const float* mx = node_max + 3 * (int64_t)r.node;
+    q.lu            = local_coord(__fadd_rn(o[0], __fmul_rn(d[0], ts)), mn[0], mx[0]);
+    q.lv            = local_coord(__fadd_rn(o[1], __fmul_rn(d[1], ts)), mn[1], mx[1]);
+    q.lw            = local_coord(__fadd_rn(o[2], __fmul_rn(d[2], ts)), mn[2], mx[2]);
+    q.weight        = q.valid ? ws : 0.0f;
+    q.ray           = r.ray;
+    q.rm            = r.rm;
+    q.row           = r.row;
+    return q;
+}
+
+}  // namespace neat

@@ -24,27 +24,6 @@
 namespace neat
 {
 
-struct StepTileArgs
-{
-    const SegRec* segs;
-    const int* samp_off;
-    const int* tile_seg;
-    const int64_t* counters;
-    const float* origin;
-    const float* direction;
-    const float* node_min;
-    const float* node_max;
-    const float* grid;
-    float* grid_grad;
-    const float* decoder;
-    float* dec_part;
-    const float* dpred;
-    float* partial;
-    uint64_t seed;
-    uint32_t step;
-    int G;
-    float beta;
-};
 
 template <int C, bool BWD>
 __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
@@ -380,7 +359,9 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
     L.tiles_cap       = (L.sample_cap + TT - 1) / TT + 1;
     L.loss_blocks     = (int)((R + 255) / 256);
     size_t smem       = 0;
-    L.bwd_grid        = tile_grid_any(d->C, true, smem);
+    L.bwd_grid        = d->decoder_path == NEAT_DECODER_SIMT_FP32
+                            ? tile_grid_any(d->C, true, smem)
+                            : tc_backward_grid(d->C, d->decoder_path == NEAT_DECODER_TC_BF16 ? 0 : 1);
     if (L.bwd_grid <= 0) return false;
     const int64_t P        = decoder_params(d->C);
     const int64_t scan_max = std::max(std::max(R, A), cap) + 1;
@@ -463,6 +444,9 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
 {
     if (!d || !s || !b || !out || !out->loss || !out->counters || step < 1) return NEAT_ERR_BAD_INPUT;
     if (d->C != 4 && d->C != 8 && d->C != 16) return NEAT_ERR_UNSUPPORTED;
+    if (d->decoder_path != NEAT_DECODER_SIMT_FP32 && d->decoder_path != NEAT_DECODER_TC_BF16X3 &&
+        d->decoder_path != NEAT_DECODER_TC_BF16)
+        return NEAT_ERR_UNSUPPORTED;
     const int64_t R = b->num_rays;
     if (R < 1 || R > (1ll << 23) || d->num_active < 1 || d->max_depth < 1 || d->max_depth > kMaxDepth ||
         d->G < 2 || d->max_samples_per_node < 1 || d->seg_capacity < 1 || d->w < 2 || d->h < 2)
@@ -534,18 +518,24 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ta.dec_part  = dec_part;
     ta.dpred     = dpred;
     ta.partial   = partial;
+    ta.status    = out->status;
     ta.seed      = seed;
     ta.step      = (uint32_t)step;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;
-    ok           = ok && launch_tiles_any(d->C, false, ta, st) == cudaSuccess;
+    const int prec = d->decoder_path == NEAT_DECODER_TC_BF16 ? 0 : 1;
+    auto tiles     = [&](bool bwd) {
+        return d->decoder_path == NEAT_DECODER_SIMT_FP32 ? launch_tiles_any(d->C, bwd, ta, st)
+                                                         : launch_tiles_tc(d->C, prec, bwd, ta, st);
+    };
+    ok = ok && tiles(false) == cudaSuccess;
     phase(2);
     const float invR = (float)(1.0 / (double)R);
     k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, ray_seg_off, partial, b->target, dpred, out->prediction, loss_part,
                                                invR, cnt + 0);
     k_loss_final<<<1, 1024, 0, st>>>(loss_part, L.loss_blocks, out->loss, invR);
     phase(3);
-    ok = ok && launch_tiles_any(d->C, true, ta, st) == cudaSuccess;
+    ok = ok && tiles(true) == cudaSuccess;
     phase(4);
 
     const double bc1g = 1.0 - std::pow((double)d->beta1, step);

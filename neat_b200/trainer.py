@@ -19,7 +19,7 @@ from .tree import HyperTreeBase
 class FusedTrainer:
     def __init__(self, tree: HyperTreeBase, camera: CameraModel, num_features=4, grid_size=17,
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
-                 decoder=None, seg_capacity_per_ray=None, device="cuda"):
+                 decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda"):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -60,7 +60,7 @@ class FusedTrainer:
             intrinsics=camera.intrinsics.data_ptr(), rotation=camera.rotation.data_ptr(),
             translation=camera.translation.data_ptr(), C=self.C, G=self.G, softplus_beta=float(softplus_beta),
             max_samples_per_node=self.M, lr_grid=float(lr_grid), lr_decoder=float(lr_decoder), beta1=0.9,
-            beta2=0.999, eps=1e-8, seg_capacity=0)
+            beta2=0.999, eps=1e-8, seg_capacity=0, decoder_path=int(decoder_path))
         self.state = _lib.StepState(
             grid=self.grid.data_ptr(), grid_m=self.grid_m.data_ptr(), grid_v=self.grid_v.data_ptr(),
             grid_grad=self.grid_grad.data_ptr(), decoder=self.decoder.data_ptr(),

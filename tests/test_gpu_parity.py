@@ -43,6 +43,12 @@ def adaptive_case(oracle):
     return cfg1_case(R=2048, seed=3, depth=4, G=9, M=16, oracle=oracle, adaptive=400)
 
 
+@pytest.fixture(scope="module")
+def c8_case(oracle):
+    # C=8, G=17 grids (the full-size model) on a depth-3 refined tree
+    return cfg1_case(R=2048, seed=5, depth=3, C=8, G=17, M=32, oracle=oracle, adaptive=200)
+
+
 def _camera(c):
     from neat_b200.api import CameraModel
     return CameraModel(c.w, c.h, c.intr, c.rot, c.trans)
@@ -186,16 +192,26 @@ def test_compute_image_forward_backward(neat, oracle, case):
 
 
 # ---------------------------------------------------------------- fused step
-def _trainer(c):
+# decoder paths and their tolerances against the f64 oracle:
+#   simt / bf16x3: the FP32 bar (1e-5 relative); Adam-updated parameters 1e-6
+#   bf16: BF16 operands with FP32 accumulation -- stated bound 1e-2 on the
+#   projection, 5e-2 on gradients (2-norm relative)
+PATHS = {"simt": (0, 1e-5, 1e-5, 1e-6), "bf16x3": (1, 1e-5, 1e-5, 1e-6), "bf16": (2, 1e-2, 5e-2, 5e-3)}
+
+
+def _trainer(c, path="bf16x3"):
     from neat_b200.trainer import FusedTrainer
     return FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
-                        grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec))
+                        grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec),
+                        decoder_path=PATHS[path][0])
 
 
-@pytest.mark.parametrize("which", ["cfg1", "adaptive"])
-def test_fused_step_matches_f64(neat, oracle, case, adaptive_case, which):
-    c = case if which == "cfg1" else adaptive_case
-    tr = _trainer(c)
+@pytest.mark.parametrize("path", list(PATHS))
+@pytest.mark.parametrize("which", ["cfg1", "adaptive", "c8"])
+def test_fused_step_matches_f64(neat, oracle, case, adaptive_case, c8_case, which, path):
+    c = {"cfg1": case, "adaptive": adaptive_case, "c8": c8_case}[which]
+    _, tol_p, tol_g, tol_w = PATHS[path]
+    tr = _trainer(c, path)
     pred = torch.zeros(c.R, device="cuda")
     loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
     torch.cuda.synchronize()
@@ -211,22 +227,26 @@ def test_fused_step_matches_f64(neat, oracle, case, adaptive_case, which):
     assert cnt[2] == seg["ray_nseg"].max()
     ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
                           T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
-    assert _rel2(pred.cpu().numpy(), ref["pred"]) < 1e-5
-    assert abs(float(loss.item()) - ref["loss"]) <= 1e-5 * ref["loss"]
+    err = dict(pred=_rel2(pred.cpu().numpy(), ref["pred"]), loss=abs(float(loss.item()) - ref["loss"]) / ref["loss"],
+               dec=_rel2(tr.decoder_grad.cpu().numpy(), ref["grad_dec"]),
+               grid=_rel2(tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1,
+                          ref["grad_grid"]),
+               pgrid=_rel2(tr.grid_reference_layout().cpu().numpy(), ref["grid"]),
+               pdec=_rel2(tr.decoder.cpu().numpy(), ref["dec"]))
+    print(which, path, {k: f"{v:.2e}" for k, v in err.items()})
+    assert err["pred"] < tol_p and err["loss"] <= tol_p
     # gradients: decoder grad is kept; grid grad recovered from m = (1-b1) g
-    assert _rel2(tr.decoder_grad.cpu().numpy(), ref["grad_dec"]) < 1e-5
-    gg = tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1
-    assert _rel2(gg, ref["grad_grid"]) < 1e-5
+    assert err["dec"] < tol_g and err["grid"] < tol_g
     # parameters after Adam
-    assert _rel2(tr.grid_reference_layout().cpu().numpy(), ref["grid"]) < 1e-6
-    assert _rel2(tr.decoder.cpu().numpy(), ref["dec"]) < 1e-6
+    assert err["pgrid"] < tol_w and err["pdec"] < tol_w
     assert float(tr.grid_grad.abs().max()) == 0.0  # zero_grad after the step
 
 
-def test_fused_step_trajectory(neat, oracle, case):
+@pytest.mark.parametrize("path", ["simt", "bf16x3"])
+def test_fused_step_trajectory(neat, oracle, case, path):
     """Five steps on the same batch: the loss follows the f64 trajectory."""
     c = case
-    tr = _trainer(c)
+    tr = _trainer(c, path)
     o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
     T = c.tree
     grid, dec, state = c.grid.astype(np.float64), c.dec.astype(np.float64), None

@@ -124,9 +124,7 @@ static cudaError_t launch_image(const ImageTileArgs& a, cudaStream_t st)
     if (grid == 0)
     {
         cudaFuncSetAttribute(k_image_tiles<C, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_image_tiles<C, BWD>, TN, smem);
-        grid = (per_sm < 1 ? 1 : per_sm) * sm_count();
+        grid = resident_ctas((const void*)k_image_tiles<C, BWD>, TN, smem, 0) * sm_count();
     }
     const int64_t ntiles = (a.S + TT - 1) / TT;
     const int g          = (int)std::min<int64_t>(grid, std::max<int64_t>(ntiles, 1));

@@ -34,6 +34,10 @@ cudaError_t launch_step_rays_write(const float* origin, const float* direction, 
 
 int sm_count();
 
+// CTAs per SM a kernel can keep resident, from its registers, static and
+// dynamic shared memory and the device limits (cap: extra limit, e.g. TMEM).
+int resident_ctas(const void* kernel, int threads, size_t dyn_smem, int cap);
+
 // Arguments of the node-major sample-tile kernels of the fused step.
 struct StepTileArgs
 {

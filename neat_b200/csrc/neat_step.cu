@@ -307,6 +307,30 @@ int sm_count()
     return n;
 }
 
+int resident_ctas(const void* kernel, int threads, size_t dyn_smem, int cap)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 1;
+    int regs_sm = 0, smem_sm = 0, max_thr = 0, max_blocks = 0, reserved = 0;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&max_thr, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    cudaDeviceGetAttribute(&max_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    // registers are allocated per warp in units of 256
+    const int warps     = (threads + 31) / 32;
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+    int n               = max_blocks > 0 ? max_blocks : 32;
+    if (regs_warp > 0) n = std::min(n, regs_sm / (regs_warp * warps));
+    const size_t smem_blk = fa.sharedSizeBytes + dyn_smem + (size_t)reserved;
+    if (smem_blk > 0) n = std::min<int>(n, (int)(smem_sm / smem_blk));
+    n = std::min(n, max_thr / (warps * 32));
+    if (cap > 0) n = std::min(n, cap);
+    return std::max(n, 1);
+}
+
 template <int C, bool BWD>
 static int tile_grid(size_t& smem)
 {
@@ -315,10 +339,7 @@ static int tile_grid(size_t& smem)
     if (blocks == 0)
     {
         cudaFuncSetAttribute(k_step_tiles<C, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_tiles<C, BWD>, TN, smem);
-        if (per_sm < 1) per_sm = 1;
-        blocks = per_sm * sm_count();
+        blocks = resident_ctas((const void*)k_step_tiles<C, BWD>, TN, smem, 0) * sm_count();
     }
     return blocks;
 }

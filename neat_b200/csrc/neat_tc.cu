@@ -602,10 +602,9 @@ static int tc_grid(size_t& smem)
     if (blocks == 0)
     {
         cudaFuncSetAttribute(k_step_tiles_tc<C, PREC, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_tiles_tc<C, PREC, BWD>, 128, smem);
-        per_sm = std::max(1, std::min(per_sm, (int)(512 / K::TMEM_COLS)));
-        blocks = per_sm * sm_count();
+        // TMEM: 512 columns per SM shared by the resident CTAs
+        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, 128, smem, (int)(512 / K::TMEM_COLS)) *
+                 sm_count();
     }
     return blocks;
 }

@@ -66,7 +66,7 @@ struct TileSmem
     float dZ2S[BWD ? TT * LDS : 4]; // [s][h]
 };
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float sigmoidf_(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float siluf_(float z) { return z * sigmoidf_(z); }
 __device__ __forceinline__ float silu_grad(float z)
 {

@@ -64,12 +64,14 @@ int neat_make_rays(const float* uv, const int32_t* image_id, const int32_t* came
 /* ----------------------------------------------------------------------- */
 /* Octree node table.                                                        */
 /* The reference keeps node_position_min/max [N,3] and active_node_ids [A]  */
-/* (src/structure/HyperTree.h:206-240).  neat_tree_prepare packs, for every */
-/* active node, its plane indices on the dyadic grid of depth max_depth and */
-/* its diagonal (HyperTree.cu:286) into a caller buffer of                  */
-/* neat_tree_table_bytes(A) bytes.  status: device int, OR-ed error flags.  */
+/* (src/structure/HyperTree.h:206-240) for the complete breadth-first tree  */
+/* of max_depth (HyperTree.cpp:11-132).  neat_tree_prepare packs, for every */
+/* node, its plane indices on the dyadic grid of depth max_depth, its        */
+/* diagonal (HyperTree.cu:286), its grid row when active and whether an      */
+/* active node lies below it, into a caller buffer of                        */
+/* neat_tree_table_bytes(max_depth) bytes.  status: device int, OR-ed flags. */
 /* ----------------------------------------------------------------------- */
-size_t neat_tree_table_bytes(int num_active);
+size_t neat_tree_table_bytes(int max_depth);
 int neat_tree_prepare(const float* node_min, const float* node_max, const int64_t* active_ids, int num_active,
                       int max_depth, void* table, int* status, neat_stream_t stream);
 

@@ -49,16 +49,26 @@ __device__ __forceinline__ void raise_status(int* status, int flag)
 }
 
 // ---------------------------------------------------------------------------
-// Node table entry (one per active node): plane indices of the node's faces on
-// the dyadic grid of depth D (plane k at -1 + k * 2^(1-D)) and its diagonal.
+// Node table entry, one per node of the complete octree (breadth-first ids:
+// children of n are 8n+1 .. 8n+8): plane indices of the node's faces on the
+// dyadic grid of depth D (plane k at -1 + k * 2^(1-D)), its diagonal, its
+// grid row when active, and whether an active node lies below it.
 // ---------------------------------------------------------------------------
 struct __align__(16) NodeEntry
 {
-    int32_t node_id;
-    uint8_t k[6];  // x0, x1, y0, y1, z0, z1
-    uint8_t pad[2];
+    int32_t local;   // active (local) id = grid row, or -1
+    uint8_t k[6];    // x0, x1, y0, y1, z0, z1
+    uint8_t active;  // 1: the node is active
+    uint8_t below;   // 1: some descendant is active (traversal continues)
     float diag;
 };
+
+__host__ __device__ constexpr int64_t tree_nodes(int D)
+{
+    int64_t n = 0, p = 1;
+    for (int i = 0; i <= D; ++i, p *= 8) n += p;
+    return n;
+}
 static_assert(sizeof(NodeEntry) == 16, "NodeEntry must be 16 bytes");
 
 __device__ __forceinline__ float plane_coord(int k, int D)

@@ -20,17 +20,17 @@ struct __align__(16) SegRec
 };
 static_assert(sizeof(SegRec) == 32, "SegRec must be 32 bytes");
 
-// Pass 1 of the step: rays from (uv, image) and per-ray / per-node counts.
-cudaError_t launch_step_rays_count(const float* uv, const int32_t* image_id, int64_t R, int w, int h,
-                                   const double* intr, const double* rot, const double* trans, const void* table,
-                                   int A, int D, int M, float* origin, float* direction, int* ray_nseg,
-                                   int* node_nseg, int64_t* counters, int* status, cudaStream_t st);
+// Pass 1 of the step: rays from (uv, image), one octree walk per ray, the
+// canonical hit list of ray r at ray_hits[r * cap_ray ...], per-node counts.
+cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R, int w, int h, const double* intr,
+                             const double* rot, const double* trans, const void* table, int D, int M, int cap_ray,
+                             float* origin, float* direction, SegRec* ray_hits, int* ray_nseg, int* node_nseg,
+                             int64_t* counters, int* status, cudaStream_t st);
 
-// Pass 2 of the step: canonical per-ray segment lists, bucketed by node.
-cudaError_t launch_step_rays_write(const float* origin, const float* direction, int64_t R, const void* table, int A,
-                                   int D, int M, const int* ray_seg_off, const int* node_seg_off, int* node_cursor,
-                                   SegRec* segs, int* seg_n, const int64_t* nseg_eff, int64_t cap, int* status,
-                                   cudaStream_t st);
+// Pass 2: place the per-ray lists into node-major buckets.
+cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,
+                              int cap_ray, const int* node_seg_off, int* node_cursor, SegRec* segs, int* seg_n,
+                              const int64_t* nseg_eff, int64_t cap, cudaStream_t st);
 
 int sm_count();
 

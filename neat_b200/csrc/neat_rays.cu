@@ -4,9 +4,14 @@
 //
 // One warp per ray.  The warp first evaluates the slab parameter of every
 // dyadic plane the tree can have, T[a][k] = (plane_k - o_a) / d_a (3 * 17
-// divisions at depth 4, instead of 6 per node), then tests all active nodes
-// 32 at a time with table lookups, compacts the hits with a ballot into
-// shared memory and rank-sorts them by (tmin, node_id).  Segments and
+// divisions at depth 4, instead of 6 per node box), then walks the octree
+// top-down, one level per iteration: the 8 children of every frontier node
+// are slab-tested 32 at a time, active children that are hit become segments
+// and hit children with active descendants form the next frontier.  The
+// reference tests every active node (HyperTree.cu:258-292); the walk finds
+// the same set because the float slab interval of a child lies inside its
+// parent's (fl((p - o) / d) is monotone in p), so a missed parent has only
+// missed children.  Hits are rank-sorted by (tmin, node_id).  Segments and
 // samples are written in that canonical order; the reference's order comes
 // from a shared-memory atomic (src/structure/HyperTree.cu:281) and is not
 // reproducible, its content (hit set, tmin/tmax, sample counts) is matched
@@ -23,6 +28,8 @@ namespace neat
 constexpr int RAY_WARPS = 4;  // rays per 128-thread block
 constexpr int MAX_PLANES = (1 << kMaxDepth) + 1;
 
+constexpr int MAX_FRONT = 256;  // a line meets at most 3 * 2^d - 2 nodes of level d (d <= 6 here)
+
 struct WarpHits
 {
     float T[3 * MAX_PLANES];
@@ -33,12 +40,14 @@ struct WarpHits
     int n[kMaxHits];     // samples of the segment
     int ord[kMaxHits];   // sorted position -> hit index
     int pre[kMaxHits];   // exclusive prefix of n in sorted order
+    int front[2][MAX_FRONT];
 };
 
-// Hits of one ray against all active nodes; returns the raw count (may
-// exceed kMaxHits, in which case only the first kMaxHits are stored).
-__device__ int warp_find_hits(const NodeEntry* __restrict__ table, int A, int D, int M, const float o[3],
-                              const float d[3], WarpHits& ws, int lane)
+// Hits of one ray: active nodes whose slab test passes and whose segment is
+// at least 1e-5 long (HyperTree.cu:274-277).  Returns the raw count (only
+// the first kMaxHits are stored); sets *overflow if a frontier overflowed.
+__device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int M, const float o[3], const float d[3],
+                                  WarpHits& ws, int lane, bool& overflow)
 {
     const int P = (1 << D) + 1;
     for (int i = lane; i < 3 * P; i += 32)
@@ -48,42 +57,87 @@ __device__ int warp_find_hits(const NodeEntry* __restrict__ table, int A, int D,
         ws.T[i]        = (dv != 0.0f) ? __fdiv_rn(__fsub_rn(plane_coord(k, D), o[ax]), dv) : 0.0f;
     }
     __syncwarp();
-    int count = 0;
-    for (int base = 0; base < A; base += 32)
+    int count = 0, fsz = 0, cur = 0;
+    overflow  = false;
+    // level 0: the root
     {
-        const int a = base + lane;
-        bool hit    = false;
+        bool act = false, below = false;
         float t0 = 0.0f, t1 = 0.0f;
-        int n = 0, node = 0;
-        if (a < A)
+        if (lane == 0)
         {
-            const NodeEntry e = table[a];
+            const NodeEntry e = tab[0];
             const bool h      = slab_test(e, ws.T, P, D, o, d, t0, t1);
-            const float dt    = __fsub_rn(t1, t0);
-            // HyperTree.cu:274-277: skip when tmax - tmin < 1e-5 (float diff, double compare)
-            if (h && !((double)dt < 1e-5))
+            act               = h && e.active && !((double)__fsub_rn(t1, t0) < 1e-5);
+            below             = h && e.below;
+            if (act)
             {
-                hit  = true;
-                n    = iceil_pos(__fmul_rn(__fdiv_rn(dt, e.diag), (float)M));
-                node = e.node_id;
+                ws.tmin[0] = t0;
+                ws.tmax[0] = t1;
+                ws.a[0]    = e.local;
+                ws.node[0] = 0;
+                ws.n[0]    = iceil_pos(__fmul_rn(__fdiv_rn(__fsub_rn(t1, t0), e.diag), (float)M));
             }
+            if (below) ws.front[0][0] = 0;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (hit)
-        {
-            const int pos = count + __popc(m & ((1u << lane) - 1u));
-            if (pos < kMaxHits)
-            {
-                ws.tmin[pos] = t0;
-                ws.tmax[pos] = t1;
-                ws.a[pos]    = a;
-                ws.node[pos] = node;
-                ws.n[pos]    = n;
-            }
-        }
-        count += __popc(m);
+        count = __shfl_sync(0xffffffffu, act ? 1 : 0, 0);
+        fsz   = __shfl_sync(0xffffffffu, below ? 1 : 0, 0);
+        __syncwarp();
     }
-    __syncwarp();
+    while (fsz > 0)
+    {
+        const int total = fsz * 8;
+        int nfsz        = 0;
+        for (int base = 0; base < total; base += 32)
+        {
+            const int i = base + lane;
+            bool act = false, below = false;
+            float t0 = 0.0f, t1 = 0.0f;
+            int node = 0, local = 0, n = 0;
+            if (i < total)
+            {
+                node              = 8 * ws.front[cur][i >> 3] + 1 + (i & 7);
+                const NodeEntry e = tab[node];
+                const bool h      = slab_test(e, ws.T, P, D, o, d, t0, t1);
+                const float dt    = __fsub_rn(t1, t0);
+                act               = h && e.active && !((double)dt < 1e-5);
+                below             = h && e.below;
+                if (act)
+                {
+                    local = e.local;
+                    n     = iceil_pos(__fmul_rn(__fdiv_rn(dt, e.diag), (float)M));
+                }
+            }
+            const unsigned ma = __ballot_sync(0xffffffffu, act);
+            const unsigned mb = __ballot_sync(0xffffffffu, below);
+            const unsigned lt = (1u << lane) - 1u;
+            if (act)
+            {
+                const int pos = count + __popc(ma & lt);
+                if (pos < kMaxHits)
+                {
+                    ws.tmin[pos] = t0;
+                    ws.tmax[pos] = t1;
+                    ws.a[pos]    = local;
+                    ws.node[pos] = node;
+                    ws.n[pos]    = n;
+                }
+            }
+            if (below)
+            {
+                const int pos = nfsz + __popc(mb & lt);
+                if (pos < MAX_FRONT)
+                    ws.front[cur ^ 1][pos] = node;
+                else
+                    overflow = true;
+            }
+            count += __popc(ma);
+            nfsz += __popc(mb);
+        }
+        __syncwarp();
+        fsz = nfsz < MAX_FRONT ? nfsz : MAX_FRONT;
+        cur ^= 1;
+    }
+    overflow = __any_sync(0xffffffffu, overflow);
     return count;
 }
 
@@ -126,18 +180,18 @@ __device__ int warp_sort_prefix(WarpHits& ws, int k, int lane)
 // ---------------------------------------------------------------------------
 // Node table
 // ---------------------------------------------------------------------------
-__global__ void k_tree_prepare(const float* __restrict__ nmin, const float* __restrict__ nmax,
-                               const int64_t* __restrict__ active_ids, int A, int D, NodeEntry* __restrict__ table,
-                               int* status)
+// Node table pass 1: every node of the complete tree (plane indices, diagonal).
+__global__ void k_tree_nodes(const float* __restrict__ nmin, const float* __restrict__ nmax, int64_t N, int D,
+                             NodeEntry* __restrict__ table, uint32_t* __restrict__ below, int* status)
 {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A) return;
-    const int64_t id = active_ids[a];
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N) return;
     NodeEntry e;
-    e.node_id = (int32_t)id;
-    e.pad[0] = e.pad[1] = 0;
-    const float scale   = (float)(1 << (D - 1));
-    bool ok             = true;
+    e.local           = -1;
+    e.active          = 0;
+    e.below           = 0;
+    const float scale = (float)(1 << (D - 1));
+    bool ok           = true;
     float ext[3];
     for (int ax = 0; ax < 3; ++ax)
     {
@@ -145,17 +199,47 @@ __global__ void k_tree_prepare(const float* __restrict__ nmin, const float* __re
         ext[ax]        = __fsub_rn(hi, lo);
         for (int side = 0; side < 2; ++side)
         {
-            const float c  = side ? hi : lo;
-            const float kf = __fmul_rn(__fadd_rn(c, 1.0f), scale);
-            int k          = (int)kf;
+            const float c   = side ? hi : lo;
+            const float kf  = __fmul_rn(__fadd_rn(c, 1.0f), scale);
+            const int k     = (int)kf;
             const bool good = (kf == (float)k) && k >= 0 && k <= (1 << D) && plane_coord(k, D) == c;
             ok              = ok && good;
             e.k[2 * ax + side] = (uint8_t)(good ? k : 0);
         }
     }
-    e.diag = node_diag(ext[0], ext[1], ext[2]);
+    e.diag    = node_diag(ext[0], ext[1], ext[2]);
+    table[id] = e;
+    below[id] = 0;
     if (!ok) raise_status(status, NEAT_ERR_NON_DYADIC);
-    table[a] = e;
+}
+
+// Pass 2: active nodes get their grid row; their ancestors are marked.
+__global__ void k_tree_active(const int64_t* __restrict__ active_ids, int A, int64_t N, NodeEntry* __restrict__ table,
+                              uint32_t* __restrict__ below, int* status)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A) return;
+    const int64_t id = active_ids[a];
+    if (id < 0 || id >= N)
+    {
+        raise_status(status, NEAT_ERR_BAD_INPUT);
+        return;
+    }
+    table[id].local  = a;
+    table[id].active = 1;
+    for (int64_t p = id; p > 0;)
+    {
+        p = (p - 1) >> 3;
+        atomicOr(&below[p], 1u);
+    }
+}
+
+// Pass 3: copy the descendant marks into the entries.
+__global__ void k_tree_below(int64_t N, NodeEntry* __restrict__ table, const uint32_t* __restrict__ below)
+{
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N) return;
+    table[id].below = below[id] ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -200,11 +284,12 @@ __global__ void __launch_bounds__(32 * RAY_WARPS) k_samples_count(const float* _
         d[c] = direction[3 * r + c];
     }
     WarpHits& ws = sh[warp];
-    int k        = warp_find_hits(table, A, D, M, o, d, ws, lane);
-    if (k > kMaxHits)
+    bool ovf     = false;
+    int k        = warp_traverse_hits(table, D, M, o, d, ws, lane, ovf);
+    if (k > kMaxHits || ovf)
     {
         if (lane == 0) raise_status(status, NEAT_ERR_TOO_MANY_HITS);
-        k = kMaxHits;
+        k = min(k, kMaxHits);
     }
     int s = 0;
     for (int i = lane; i < k; i += 32) s += ws.n[i];
@@ -235,17 +320,18 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         d[c] = direction[3 * r + c];
     }
     WarpHits& ws = sh[warp];
-    int k        = warp_find_hits(table, A, D, M, o, d, ws, lane);
-    if (k > kMaxHits) k = kMaxHits;
+    bool ovf     = false;
+    int k        = warp_traverse_hits(table, D, M, o, d, ws, lane, ovf);
+    k            = min(k, kMaxHits);
     warp_sort_prefix(ws, k, lane);
     const int64_t base = samp_off[r];
     bool overflow      = false;
     for (int p = 0; p < k; ++p)
     {
-        const int i = ws.ord[p];
-        const int n = ws.n[i];
-        const float t0 = ws.tmin[i], t1 = ws.tmax[i];
-        const int lb    = ws.pre[p];
+        const int i      = ws.ord[p];
+        const int n      = ws.n[i];
+        const float t0   = ws.tmin[i], t1 = ws.tmax[i];
+        const int lb     = ws.pre[p];
         const int64_t nd = ws.node[i];
         for (int j = lane; j < n; j += 32)
         {
@@ -269,14 +355,15 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
 }
 
 // ---------------------------------------------------------------------------
-// Fused step: pass 1 (rays + counts) and pass 2 (segment lists)
+// Fused step: one traversal per ray (canonical hit list kept per ray), then
+// the lists are placed node-major.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(32 * RAY_WARPS)
-    k_step_rays_count(const float* __restrict__ uv, const int32_t* __restrict__ image_id, int64_t R, int w, int h,
-                      const double* __restrict__ intr, const double* __restrict__ rot,
-                      const double* __restrict__ trans, const NodeEntry* __restrict__ table, int A, int D, int M,
-                      float* __restrict__ origin, float* __restrict__ direction, int* __restrict__ ray_nseg,
-                      int* __restrict__ node_nseg, int64_t* counters, int* status)
+    k_step_rays(const float* __restrict__ uv, const int32_t* __restrict__ image_id, int64_t R, int w, int h,
+                const double* __restrict__ intr, const double* __restrict__ rot, const double* __restrict__ trans,
+                const NodeEntry* __restrict__ table, int D, int M, int cap_ray, float* __restrict__ origin,
+                float* __restrict__ direction, SegRec* __restrict__ ray_hits, int* __restrict__ ray_nseg,
+                int* __restrict__ node_nseg, int64_t* counters, int* status)
 {
     __shared__ WarpHits sh[RAY_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,13 +378,35 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         direction[3 * r + lane] = d[lane];
     }
     WarpHits& ws = sh[warp];
-    int k        = warp_find_hits(table, A, D, M, o, d, ws, lane);
-    if (k > kMaxHits)
+    bool ovf     = false;
+    int k        = warp_traverse_hits(table, D, M, o, d, ws, lane, ovf);
+    if (k > kMaxHits || ovf)
     {
         if (lane == 0) raise_status(status, NEAT_ERR_TOO_MANY_HITS);
-        k = kMaxHits;
+        k = min(k, kMaxHits);
     }
-    for (int i = lane; i < k; i += 32) atomicAdd(&node_nseg[ws.a[i]], 1);
+    if (k > cap_ray)
+    {
+        if (lane == 0) raise_status(status, NEAT_ERR_CAPACITY);
+        k = cap_ray;
+    }
+    warp_sort_prefix(ws, k, lane);
+    SegRec* out = ray_hits + r * (int64_t)cap_ray;
+    for (int p = lane; p < k; p += 32)
+    {
+        const int i = ws.ord[p];
+        SegRec sg;
+        sg.ray        = (int32_t)r;
+        sg.local_base = ws.pre[p];
+        sg.tmin       = ws.tmin[i];
+        sg.tmax       = ws.tmax[i];
+        sg.n          = ws.n[i];
+        sg.rm         = p;  // rank in the ray; made global when placed
+        sg.row        = ws.a[i];
+        sg.node       = ws.node[i];
+        out[p]        = sg;
+        atomicAdd(&node_nseg[sg.row], 1);
+    }
     if (lane == 0)
     {
         ray_nseg[r] = k;
@@ -305,76 +414,48 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
     }
 }
 
-__global__ void __launch_bounds__(32 * RAY_WARPS)
-    k_step_rays_write(const float* __restrict__ origin, const float* __restrict__ direction, int64_t R,
-                      const NodeEntry* __restrict__ table, int A, int D, int M, const int* __restrict__ ray_seg_off,
-                      const int* __restrict__ node_seg_off, int* __restrict__ node_cursor, SegRec* __restrict__ segs,
-                      int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap, int* status)
+// Place every ray's segments into its nodes' buckets (thread per segment).
+__global__ void k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_nseg,
+                             const int* __restrict__ ray_seg_off, int64_t R, int cap_ray,
+                             const int* __restrict__ node_seg_off, int* __restrict__ node_cursor,
+                             SegRec* __restrict__ segs, int* __restrict__ seg_n, const int64_t* nseg_eff,
+                             int64_t cap)
 {
-    __shared__ WarpHits sh[RAY_WARPS];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t r = (int64_t)blockIdx.x * RAY_WARPS + warp;
-    if (r >= R) return;
-    if (*nseg_eff == 0) return;  // nothing to place (no hits, or capacity overflow)
-    float o[3], d[3];
-    for (int c = 0; c < 3; ++c)
-    {
-        o[c] = origin[3 * r + c];
-        d[c] = direction[3 * r + c];
-    }
-    WarpHits& ws = sh[warp];
-    int k        = warp_find_hits(table, A, D, M, o, d, ws, lane);
-    if (k > kMaxHits) k = kMaxHits;
-    warp_sort_prefix(ws, k, lane);
-    const int rbase = ray_seg_off[r];
-    for (int p = lane; p < k; p += 32)
-    {
-        const int i  = ws.ord[p];
-        const int a  = ws.a[i];
-        const int rm = rbase + p;
-        const int nm = node_seg_off[a] + atomicAdd(&node_cursor[a], 1);
-        if (rm >= cap || nm >= cap)
-        {
-            raise_status(status, NEAT_ERR_CAPACITY);
-            continue;
-        }
-        SegRec s;
-        s.ray        = (int32_t)r;
-        s.local_base = ws.pre[p];
-        s.tmin       = ws.tmin[i];
-        s.tmax       = ws.tmax[i];
-        s.n          = ws.n[i];
-        s.rm         = rm;
-        s.row        = a;
-        s.node       = ws.node[i];
-        segs[nm]     = s;
-        seg_n[nm]    = s.n;
-    }
+    if (*nseg_eff == 0) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t r = i / cap_ray;
+    const int p     = (int)(i - r * cap_ray);
+    if (r >= R || p >= ray_nseg[r]) return;
+    SegRec sg    = ray_hits[i];
+    const int rm = ray_seg_off[r] + p;
+    const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
+    if (rm >= cap || nm >= cap) return;  // unreachable: the totals were checked against cap
+    sg.rm     = rm;
+    segs[nm]  = sg;
+    seg_n[nm] = sg.n;
 }
 
-cudaError_t launch_step_rays_count(const float* uv, const int32_t* image_id, int64_t R, int w, int h,
-                                   const double* intr, const double* rot, const double* trans, const void* table,
-                                   int A, int D, int M, float* origin, float* direction, int* ray_nseg,
-                                   int* node_nseg, int64_t* counters, int* status, cudaStream_t st)
+cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R, int w, int h, const double* intr,
+                             const double* rot, const double* trans, const void* table, int D, int M, int cap_ray,
+                             float* origin, float* direction, SegRec* ray_hits, int* ray_nseg, int* node_nseg,
+                             int64_t* counters, int* status, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
     const unsigned grid = (unsigned)((R + RAY_WARPS - 1) / RAY_WARPS);
-    k_step_rays_count<<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
-                                                       (const NodeEntry*)table, A, D, M, origin, direction, ray_nseg,
-                                                       node_nseg, counters, status);
+    k_step_rays<<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans, (const NodeEntry*)table, D,
+                                                 M, cap_ray, origin, direction, ray_hits, ray_nseg, node_nseg,
+                                                 counters, status);
     return cudaGetLastError();
 }
 
-cudaError_t launch_step_rays_write(const float* origin, const float* direction, int64_t R, const void* table, int A,
-                                   int D, int M, const int* ray_seg_off, const int* node_seg_off, int* node_cursor,
-                                   SegRec* segs, int* seg_n, const int64_t* nseg_eff, int64_t cap, int* status,
-                                   cudaStream_t st)
+cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,
+                              int cap_ray, const int* node_seg_off, int* node_cursor, SegRec* segs, int* seg_n,
+                              const int64_t* nseg_eff, int64_t cap, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
-    const unsigned grid = (unsigned)((R + RAY_WARPS - 1) / RAY_WARPS);
-    k_step_rays_write<<<grid, 32 * RAY_WARPS, 0, st>>>(origin, direction, R, (const NodeEntry*)table, A, D, M,
-                                                       ray_seg_off, node_seg_off, node_cursor, segs, seg_n, nseg_eff,
-                                                       cap, status);
+    const int64_t n = R * (int64_t)cap_ray;
+    k_step_place<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ray_hits, ray_nseg, ray_seg_off, R, cap_ray,
+                                                              node_seg_off, node_cursor, segs, seg_n, nseg_eff, cap);
     return cudaGetLastError();
 }
 
@@ -385,17 +466,28 @@ using namespace neat;
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-extern "C" size_t neat_tree_table_bytes(int num_active) { return (size_t)(num_active > 0 ? num_active : 0) * 16; }
+extern "C" size_t neat_tree_table_bytes(int max_depth)
+{
+    if (max_depth < 1 || max_depth > kMaxDepth) return 0;
+    const int64_t N = tree_nodes(max_depth);
+    return (size_t)N * sizeof(NodeEntry) + ((size_t)N * 4 + 255) / 256 * 256;
+}
 
 extern "C" int neat_tree_prepare(const float* node_min, const float* node_max, const int64_t* active_ids,
                                  int num_active, int max_depth, void* table, int* status, neat_stream_t stream)
 {
-    if (num_active < 0 || max_depth < 1 || max_depth > kMaxDepth || !node_min || !node_max ||
-        (num_active > 0 && (!active_ids || !table)))
+    if (num_active < 0 || max_depth < 1 || max_depth > kMaxDepth || !node_min || !node_max || !table ||
+        (num_active > 0 && !active_ids))
         return NEAT_ERR_BAD_INPUT;
-    if (num_active == 0) return NEAT_OK;
-    k_tree_prepare<<<(num_active + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
-        node_min, node_max, active_ids, num_active, max_depth, (NodeEntry*)table, status);
+    const int64_t N     = tree_nodes(max_depth);
+    NodeEntry* entries  = (NodeEntry*)table;
+    uint32_t* below     = (uint32_t*)((char*)table + (size_t)N * sizeof(NodeEntry));
+    cudaStream_t st     = (cudaStream_t)stream;
+    const unsigned gN   = (unsigned)((N + 255) / 256);
+    k_tree_nodes<<<gN, 256, 0, st>>>(node_min, node_max, N, max_depth, entries, below, status);
+    if (num_active > 0)
+        k_tree_active<<<(num_active + 255) / 256, 256, 0, st>>>(active_ids, num_active, N, entries, below, status);
+    k_tree_below<<<gN, 256, 0, st>>>(N, entries, below);
     return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 

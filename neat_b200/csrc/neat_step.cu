@@ -362,13 +362,13 @@ struct StepLayout
 {
     enum
     {
-        ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, SEGS, SEG_N, SAMP_OFF,
-        TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, NUM
+        ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
+        SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, NUM
     };
     size_t off[NUM];
     size_t total;
     int64_t tiles_cap, sample_cap;
-    int loss_blocks, bwd_grid;
+    int loss_blocks, bwd_grid, cap_ray;
 };
 
 static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
@@ -376,6 +376,7 @@ static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
 {
     const int64_t cap = d->seg_capacity, A = d->num_active, M = d->max_samples_per_node;
+    L.cap_ray         = (int)std::max<int64_t>(1, std::min<int64_t>(NEAT_MAX_HITS_PER_RAY, R > 0 ? cap / R : 1));
     L.sample_cap      = cap * (M + 1);
     L.tiles_cap       = (L.sample_cap + TT - 1) / TT + 1;
     L.loss_blocks     = (int)((R + 255) / 256);
@@ -388,7 +389,8 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
     const int64_t scan_max = std::max(std::max(R, A), cap) + 1;
     size_t sz[StepLayout::NUM] = {
         (size_t)R * 3 * 4, (size_t)R * 3 * 4, (size_t)R * 4, (size_t)(R + 1) * 4, (size_t)A * 4, (size_t)A * 4,
-        (size_t)(A + 1) * 4, (size_t)cap * sizeof(SegRec), (size_t)cap * 4, (size_t)(cap + 1) * 4,
+        (size_t)(A + 1) * 4, (size_t)R * L.cap_ray * sizeof(SegRec), (size_t)cap * sizeof(SegRec), (size_t)cap * 4,
+        (size_t)(cap + 1) * 4,
         (size_t)L.tiles_cap * 4, (size_t)cap * 4, (size_t)R * 4, (size_t)L.loss_blocks * 4,
         (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4};
     size_t o = 0;
@@ -489,6 +491,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     int* node_nseg    = (int*)P_(StepLayout::NODE_NSEG);
     int* node_cursor  = (int*)P_(StepLayout::NODE_CURSOR);
     int* node_seg_off = (int*)P_(StepLayout::NODE_SEG_OFF);
+    SegRec* ray_hits  = (SegRec*)P_(StepLayout::RAY_HITS);
     SegRec* segs      = (SegRec*)P_(StepLayout::SEGS);
     int* seg_n        = (int*)P_(StepLayout::SEG_N);
     int* samp_off     = (int*)P_(StepLayout::SAMP_OFF);
@@ -510,14 +513,14 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ok      = ok && cudaMemsetAsync(node_nseg, 0, (size_t)A * 4, st) == cudaSuccess;
     ok      = ok && cudaMemsetAsync(node_cursor, 0, (size_t)A * 4, st) == cudaSuccess;
     ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
-    ok      = ok && launch_step_rays_count(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation,
-                                           d->translation, d->tree_table, A, D, M, origin, direction, ray_nseg,
-                                           node_nseg, cnt, out->status, st) == cudaSuccess;
+    ok = ok && launch_step_rays(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation, d->translation,
+                                d->tree_table, D, M, L.cap_ray, origin, direction, ray_hits, ray_nseg, node_nseg, cnt,
+                                out->status, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(ray_nseg, nullptr, R, ray_seg_off, scratch, cnt + 0, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(node_nseg, nullptr, A, node_seg_off, scratch, nullptr, st) == cudaSuccess;
     k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, out->status);
-    ok = ok && launch_step_rays_write(origin, direction, R, d->tree_table, A, D, M, ray_seg_off, node_seg_off,
-                                      node_cursor, segs, seg_n, cnt + 0, cap, out->status, st) == cudaSuccess;
+    ok = ok && launch_step_place(ray_hits, ray_nseg, ray_seg_off, R, L.cap_ray, node_seg_off, node_cursor, segs,
+                                 seg_n, cnt + 0, cap, st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(partial, 0, (size_t)cap * 4, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(seg_n, cnt + 0, cap, samp_off, scratch, cnt + 1, st) == cudaSuccess;
     k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, out->status);

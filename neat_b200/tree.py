@@ -104,7 +104,7 @@ class HyperTreeBase:
             if device.type == "cuda":
                 lib = _lib.load()
                 A = self.NumActiveNodes()
-                table = torch.empty(max(lib.neat_tree_table_bytes(A), 16), dtype=torch.uint8, device=device)
+                table = torch.empty(lib.neat_tree_table_bytes(self.max_depth), dtype=torch.uint8, device=device)
                 status = torch.zeros(1, dtype=torch.int32, device=device)
                 stream = torch.cuda.current_stream(device).cuda_stream
                 _lib.check(lib.neat_tree_prepare(t["min"].data_ptr(), t["max"].data_ptr(), t["active"].data_ptr(), A,

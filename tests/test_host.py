@@ -35,7 +35,8 @@ def test_library_host_calls_without_gpu():
     lib = _lib.load()
     assert lib.neat_version() >= 1
     assert lib.neat_decoder_params(8) == 64 * 8 + 64 + 64 * 64 + 64 + 64 + 1
-    assert lib.neat_tree_table_bytes(100) == 1600
+    assert lib.neat_tree_table_bytes(2) == 73 * 16 + 512  # entries + descendant marks
+    assert lib.neat_tree_table_bytes(0) == 0
     assert b"capacity" in lib.neat_status_string(_lib.NEAT_ERR_CAPACITY)
     # argument validation happens on the host before any launch
     assert lib.neat_make_rays(None, None, None, -1, 16, 16, None, None, None, None, None, None) == \

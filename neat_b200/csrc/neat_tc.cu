@@ -1,8 +1,8 @@
 // neat_tc.cu -- the fused step's sample tiles with the decoder GEMMs on the
 // 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM).
 //
-// One CTA = one warpgroup (128 threads); thread s owns slot s of the tile and
-// TMEM lane s.  Per 128-sample tile:
+// One CTA = one or two warpgroups; thread s (and s+128) owns slot s of the
+// tile (TMEM lane s); with two warpgroups the 64 hidden units are split.  Per 128-sample tile:
 //   layer 1 (C -> 64, SIMT fp32)  -> h1 row s written into HB (core-matrix layout)
 //   Z2 = HB[:, :64] . W2^T          tcgen05 (A K-major, B K-major)          -> TMEM D2
 //   epilogue: y, softplus, dy; dz2 = dy w3 silu'(z2) -> AB[:, :64]
@@ -97,8 +97,9 @@ struct Cfg
     static constexpr int NF     = HH * C + 3 * HH + 4;
     static constexpr int OFF_I  = OFF_F + NF * 4;
     static constexpr int OFF_V  = OFF_I + 2 * 128 * 4;
-    static constexpr int OFF_R  = OFF_V + 128 * 4;
-    static constexpr int OFF_M  = ((OFF_R + 4 * (2 * HH + 4) * 4) + 15) / 16 * 16;
+    static constexpr int OFF_R  = OFF_V + 2 * 128 * 4;
+    static constexpr int NRED   = std::max(2 * 128 * C, 8 * HH);
+    static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
     static constexpr int NEED   = OFF_M + 16;
     // BF16 backward: pad so that at most two CTAs share an SM (2 x 256 TMEM columns)
     static constexpr int BYTES = (PREC == BF16 && BWD) ? std::max(NEED, 100 * 1024) : NEED;
@@ -219,16 +220,29 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
+// Threads per CTA: 128 (one thread per sample) or 256 (two threads per sample
+// splitting the hidden units; used where shared memory allows one CTA per SM).
+template <int PREC, bool BWD>
+struct TcThreads
+{
+    static constexpr int value = (PREC == BF16X3 && BWD) ? 256 : 128;
+};
+
 template <int C, int PREC, bool BWD>
-__global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
+__global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_tc(StepTcArgs a)
 {
     using K  = Cfg<C, PREC, BWD>;
     using P  = Prec<PREC>;
     using HB = typename K::HB;
     using AB = typename K::AB;
     using W2 = typename K::W2;
+    constexpr int TC_THREADS = TcThreads<PREC, BWD>::value;
+    constexpr int NH         = TC_THREADS / 128;  // threads per sample
+    constexpr int HALF       = HH / NH;           // hidden units per thread
     extern __shared__ __align__(128) unsigned char sm[];
-    const int t = threadIdx.x, w = t >> 5, l = t & 31;
+    // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
+    const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
+    const int c0 = h * HALF;  // first hidden column of this thread
     float* sW1    = reinterpret_cast<float*>(sm + K::OFF_F);
     float* sb1    = sW1 + HH * C;
     float* sb2    = sb1 + HH;
@@ -236,8 +250,8 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
     float* sb3    = sw3 + HH;
     int* mark     = reinterpret_cast<int*>(sm + K::OFF_I);
     int* slot_seg = mark + 128;
-    float* sval   = reinterpret_cast<float*>(sm + K::OFF_V);
-    float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);
+    float* sval   = reinterpret_cast<float*>(sm + K::OFF_V);  // [2][128]: y halves / contributions
+    float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);  // [2][128][C] dx halves; end: reductions
     uint64_t* mbar_p = reinterpret_cast<uint64_t*>(sm + K::OFF_M);
     uint32_t* tslot  = reinterpret_cast<uint32_t*>(sm + K::OFF_M + 8);
     unsigned char* pW2 = sm + K::OFF_W2;
@@ -248,20 +262,18 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
 
     // ---- decoder parameters: W1 / biases / w3 in fp32, W2 as MMA operand pieces
     using O = DecOff<C>;
-    for (int i = t; i < HH * C; i += 128) sW1[i] = a.decoder[O::W1 + i];
-    for (int i = t; i < HH; i += 128)
+    for (int i = t; i < HH * C; i += TC_THREADS) sW1[i] = a.decoder[O::W1 + i];
+    for (int i = t; i < HH; i += TC_THREADS)
     {
         sb1[i] = a.decoder[O::b1 + i];
         sb2[i] = a.decoder[O::b2 + i];
         sw3[i] = a.decoder[O::W3 + i];
     }
     if (t == 0) sb3[0] = a.decoder[O::b3];
-    for (int i = t; i < HH * HH; i += 128)
+    for (int i = t; i < HH * HH; i += TC_THREADS)
     {
-        const int h = i / HH, k = i % HH;
-        const float v = a.decoder[O::W2 + i];
-        const int off = W2::off(h, k);
-        float r       = v;
+        const int off = W2::off(i / HH, i % HH);
+        float r       = a.decoder[O::W2 + i];
 #pragma unroll
         for (int p = 0; p < P::PIECES; ++p)
         {
@@ -283,7 +295,7 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tslot;
-    const uint32_t lane = (uint32_t)(w * 32) << 16;
+    const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
     const uint32_t tD2 = tmem, tD3 = tmem + 64, tD4 = tmem + 128;
 
     const int nseg       = (int)a.counters[0];
@@ -293,9 +305,9 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
     bool ok              = true;
     bool wg_pending      = false;
     bool wg_started      = false;
-    float dw3_lo = 0.0f, dw3_hi = 0.0f, db3 = 0.0f;
+    float dw3[HALF / 32] = {};  // lane l: dW3[c0 + 32 i + l]
+    float db3           = 0.0f;
 
-    // All threads wait for the next MMA completion; the result is made uniform.
     auto wait_mma = [&]() -> bool {
         const bool mine = mbar_wait_bounded(mbar, phase);
         phase ^= 1u;
@@ -303,18 +315,17 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
         fence_after();
         return all;
     };
-    // MMA issue helpers (thread 0 only)
     constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);
     constexpr uint32_t idH  = make_idesc(P::FMT, 0, 1, 128, HH);
     constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);
-    constexpr int KS64      = HH / P::KI;   // k-steps over 64
-    constexpr int KS128     = 128 / P::KI;  // k-steps over the 128 samples
+    constexpr int KS64      = HH / P::KI;
+    constexpr int KS128     = 128 / P::KI;
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
         const int64_t g0 = tile * 128;
         tile_slot_segments(g0, a.tile_seg[tile], nseg, a.samp_off, mark, slot_seg);
-        const SlotSample q = slot_sample(a.segs, a.samp_off, mark[t], g0 + t, S, a.origin, a.direction, a.node_min,
+        const SlotSample q = slot_sample(a.segs, a.samp_off, mark[s], g0 + s, S, a.origin, a.direction, a.node_min,
                                          a.node_max, a.seed, a.step);
         float x[C];
         {
@@ -334,9 +345,9 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
                 break;
             }
         }
-        // ---- HB row t: [h1 | x | 1 0 .. 0]
+        // ---- HB row s: h1 columns of this half; half 0 adds [x | 1 0 ..]
 #pragma unroll 1
-        for (int k0 = 0; k0 < HH; k0 += P::E)
+        for (int k0 = c0; k0 < c0 + HALF; k0 += P::E)
         {
             float hv[P::E];
 #pragma unroll
@@ -347,26 +358,32 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
                 for (int c = 0; c < C; ++c) z = fmaf(x[c], sW1[(k0 + i) * C + c], z);
                 hv[i] = siluf_(z);
             }
-            store_chunk<PREC>(pHB, HB::BYTES, HB::off(t, k0), hv);
+            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, k0), hv);
         }
         if constexpr (BWD)
         {
-#pragma unroll
-            for (int c0 = 0; c0 < K::XW + 8; c0 += P::E)
+            if (h == 0)
             {
-                float v[P::E];
 #pragma unroll
-                for (int i = 0; i < P::E; ++i)
+                for (int cc = 0; cc < K::XW + 8; cc += P::E)
                 {
-                    const int c = c0 + i;
-                    v[i]        = (c < C) ? x[c] : ((c == K::XW) ? 1.0f : 0.0f);
+                    float v[P::E];
+#pragma unroll
+                    for (int i = 0; i < P::E; ++i)
+                    {
+                        const int c = cc + i;
+                        v[i]        = (c < C) ? x[c] : ((c == K::XW) ? 1.0f : 0.0f);
+                    }
+                    store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, K::XO + cc), v);
                 }
-                store_chunk<PREC>(pHB, HB::BYTES, HB::off(t, K::XO + c0), v);
             }
-            for (int c0 = K::OO + 8; c0 < K::NW; c0 += P::E)
+            if (h == NH - 1)
             {
-                float v[P::E] = {};
-                store_chunk<PREC>(pHB, HB::BYTES, HB::off(t, c0), v);
+                for (int cc = K::OO + 8; cc < K::NW; cc += P::E)
+                {
+                    float v[P::E] = {};
+                    store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, cc), v);
+                }
             }
         }
         fence_smem_async();
@@ -391,28 +408,35 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
             ok = false;
             break;
         }
-        // ---- epilogue 1: y
-        float y = sb3[0];
-#pragma unroll 1
-        for (int j = 0; j < HH / 16; ++j)
+        // ---- epilogue 1: y = b3 + sum over both halves
         {
-            float z[16];
-            tmem_ld16(tD2 + lane + 16 * j, z);
+            float yp = 0.0f;
+#pragma unroll 1
+            for (int j = 0; j < HALF / 16; ++j)
+            {
+                float z[16];
+                tmem_ld16(tD2 + lane + c0 + 16 * j, z);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) y = fmaf(siluf_(z[i] + sb2[16 * j + i]), sw3[16 * j + i], y);
+                for (int i = 0; i < 16; ++i)
+                    yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+            }
+            sval[h * 128 + s] = yp;
         }
+        fence_before();
+        __syncthreads();
+        const float y = sb3[0] + sval[s] + (NH == 2 ? sval[128 + s] : 0.0f);
         if constexpr (!BWD)
         {
-            sval[t] = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
-            fence_before();
+            __syncthreads();  // both halves read the y parts before they are overwritten
+            if (h == 0) sval[s] = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
             __syncthreads();
-            if (q.valid)
+            if (h == 0 && q.valid)
             {
-                const int seg = mark[t];
-                if (t == 0 || mark[t - 1] != seg)
+                const int seg = mark[s];
+                if (s == 0 || mark[s - 1] != seg)
                 {
                     float sum = 0.0f;
-                    for (int u = t; u < 128 && mark[u] == seg; ++u) sum += sval[u];
+                    for (int u = s; u < 128 && mark[u] == seg; ++u) sum += sval[u];
                     atomicAdd(a.partial + q.rm, sum);
                 }
             }
@@ -422,38 +446,26 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
         {
             const float dv = q.valid ? a.dpred[q.ray] : 0.0f;
             const float dy = dv * q.weight * softplus_grad(y, a.beta);
-            db3 += dy;
-            // dz2 -> AB[:, :64], dW3 += h2 dy
-            auto write_dz2 = [&](bool dw3) {
+            if (h == 0) db3 += dy;
+            // dz2 (this half's columns) -> AB[:, c0:c0+32]; dW3 += h2 dy
 #pragma unroll 1
-                for (int j = 0; j < HH / 16; ++j)
+            for (int j = 0; j < HALF / 16; ++j)
+            {
+                float z[16];
+                tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+                float d[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
                 {
-                    float z[16];
-                    tmem_ld16(tD2 + lane + 16 * j, z);
-                    float d[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                    {
-                        const float zz = z[i] + sb2[16 * j + i];
-                        d[i]           = dy * sw3[16 * j + i] * silu_grad(zz);
-                        if (dw3)
-                        {
-                            const float v = warp_sum(siluf_(zz) * dy);
-                            const int h   = 16 * j + i;
-                            if (l == (h & 31))
-                            {
-                                if (h < 32)
-                                    dw3_lo += v;
-                                else
-                                    dw3_hi += v;
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(t, 16 * j + i), d + i);
+                    const int col  = c0 + 16 * j + i;
+                    const float zz = z[i] + sb2[col];
+                    d[i]           = dy * sw3[col] * silu_grad(zz);
+                    const float v  = warp_sum(siluf_(zz) * dy);
+                    if (l == ((16 * j + i) & 31)) dw3[(16 * j + i) >> 5] += v;
                 }
-            };
-            write_dz2(true);
+#pragma unroll
+                for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
+            }
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -476,40 +488,34 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
                 ok = false;
                 break;
             }
-            // ---- epilogue 2: dz1 -> AB[:, 64:], dx, scatter
+            // ---- epilogue 2: dz1 (this half's k) -> AB[:, 64+c0 ..]; dx partial
             float dx[C];
 #pragma unroll
             for (int c = 0; c < C; ++c) dx[c] = 0.0f;
-            auto write_dz1 = [&]() {
 #pragma unroll 1
-                for (int j = 0; j < HH / 16; ++j)
-                {
-                    float g[16];
-                    tmem_ld16(tD3 + lane + 16 * j, g);
-                    float d[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                    {
-                        const int k = 16 * j + i;
-                        float z     = sb1[k];
-#pragma unroll
-                        for (int c = 0; c < C; ++c) z = fmaf(x[c], sW1[k * C + c], z);
-                        d[i] = g[i] * silu_grad(z);
-#pragma unroll
-                        for (int c = 0; c < C; ++c) dx[c] = fmaf(d[i], sW1[k * C + c], dx[c]);
-                    }
-#pragma unroll
-                    for (int i = 0; i < 16; i += P::E)
-                        store_chunk<PREC>(pAB, AB::BYTES, AB::off(t, HH + 16 * j + i), d + i);
-                }
-            };
-            write_dz1();
-            if (q.valid)
+            for (int j = 0; j < HALF / 16; ++j)
             {
-                Corners kc;
-                igs_corners(q.lu, q.lv, q.lw, a.G, a.G, a.G, kc);
-                scatter_cl<C>(a.grid_grad, q.row, a.G, kc, dx);
+                float g[16];
+                tmem_ld16(tD3 + lane + c0 + 16 * j, g);
+                float d[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                {
+                    const int k = c0 + 16 * j + i;
+                    float z     = sb1[k];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) z = fmaf(x[c], sW1[k * C + c], z);
+                    d[i] = g[i] * silu_grad(z);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) dx[c] = fmaf(d[i], sW1[k * C + c], dx[c]);
+                }
+#pragma unroll
+                for (int i = 0; i < 16; i += P::E)
+                    store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), d + i);
             }
+            if constexpr (NH == 2)
+#pragma unroll
+                for (int c = 0; c < C; ++c) sred[(h * 128 + s) * C + c] = dx[c];
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -530,6 +536,23 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
             }
             wg_started = true;
             wg_pending = true;
+            // dx of sample s (both halves when split; each half scatters four corners)
+            if (q.valid)
+            {
+                Corners kc;
+                igs_corners(q.lu, q.lv, q.lw, a.G, a.G, a.G, kc);
+                if constexpr (NH == 2)
+                {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) dx[c] = sred[s * C + c] + sred[(128 + s) * C + c];
+                    scatter_cl_half<C>(a.grid_grad, q.row, a.G, kc, dx, h);
+                }
+                else
+                {
+                    scatter_cl<C>(a.grid_grad, q.row, a.G, kc, dx);
+                }
+            }
+            __syncthreads();  // sred / sval reused by the next tile
         }
     }
     // ---- drain
@@ -540,10 +563,12 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
     if (!ok) raise_status(a.status, NEAT_ERR_TIMEOUT);
     if constexpr (BWD)
     {
-        // per-CTA decoder-gradient partial (deterministic layout)
+        // per-CTA decoder-gradient partial (deterministic layout); row s of D4,
+        // columns split between the halves
         float* dst = a.dec_part + (int64_t)blockIdx.x * O::total;
+        constexpr int NCH = K::NW / 16;
 #pragma unroll 1
-        for (int j = 0; j < K::NW / 16; ++j)
+        for (int j = h; j < NCH; j += NH)
         {
             float v[16];
             if (wg_started && ok)
@@ -555,35 +580,41 @@ __global__ void __launch_bounds__(128, 1) k_step_tiles_tc(StepTcArgs a)
             for (int i = 0; i < 16; ++i)
             {
                 const int n = 16 * j + i;
-                if (t < HH)
+                if (s < HH)
                 {
-                    if (n < HH) dst[O::W2 + t * HH + n] = v[i];
-                    if (n == K::OO) dst[O::b2 + t] = v[i];
+                    if (n < HH) dst[O::W2 + s * HH + n] = v[i];
+                    if (n == K::OO) dst[O::b2 + s] = v[i];
                 }
                 else
                 {
-                    const int k = t - HH;
+                    const int k = s - HH;
                     if (n >= K::XO && n < K::XO + C) dst[O::W1 + k * C + (n - K::XO)] = v[i];
                     if (n == K::OO) dst[O::b1 + k] = v[i];
                 }
             }
         }
-        // dW3 (lane h&31 of every warp holds a partial of h) and db3
-        sred[w * (2 * HH + 4) + l]      = dw3_lo;
-        sred[w * (2 * HH + 4) + l + 32] = dw3_hi;
-        sred[w * (2 * HH + 4) + HH + l] = warp_sum(db3);
+        // dW3: lane l of warp w holds partials of columns c0 + 32 i + l (c0 of
+        // the warp's part); db3 from the first part's threads
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < HALF / 32; ++i) sred[w * HH + c0 + 32 * i + l] = dw3[i];
+        const float b3w = warp_sum(db3);
         __syncthreads();
         if (t < HH)
         {
-            float s = 0.0f;
-            for (int ww = 0; ww < 4; ++ww) s += sred[ww * (2 * HH + 4) + t];
-            dst[O::W3 + t] = s;
+            const int part = t / HALF;
+            float acc      = 0.0f;
+            for (int ww = 4 * part; ww < 4 * part + 4; ++ww) acc += sred[ww * HH + t];
+            dst[O::W3 + t] = acc;
         }
+        __syncthreads();
+        if (l == 0) sred[w] = b3w;
+        __syncthreads();
         if (t == 0)
         {
-            float s = 0.0f;
-            for (int ww = 0; ww < 4; ++ww) s += sred[ww * (2 * HH + 4) + HH];
-            dst[O::b3] = s;
+            float acc = 0.0f;
+            for (int ww = 0; ww < TC_THREADS / 32; ++ww) acc += sred[ww];
+            dst[O::b3] = acc;
         }
     }
     fence_before();
@@ -603,7 +634,7 @@ static int tc_grid(size_t& smem)
     {
         cudaFuncSetAttribute(k_step_tiles_tc<C, PREC, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         // TMEM: 512 columns per SM shared by the resident CTAs
-        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, 128, smem, (int)(512 / K::TMEM_COLS)) *
+        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, TcThreads<PREC, BWD>::value, smem, (int)(512 / K::TMEM_COLS)) *
                  sm_count();
     }
     return blocks;
@@ -616,12 +647,12 @@ static cudaError_t launch(bool bwd, const StepTcArgs& args, cudaStream_t st)
     if (!bwd)
     {
         const int g = tc_grid<C, PREC, false>(smem);
-        k_step_tiles_tc<C, PREC, false><<<g, 128, smem, st>>>(args);
+        k_step_tiles_tc<C, PREC, false><<<g, TcThreads<PREC, false>::value, smem, st>>>(args);
     }
     else
     {
         const int g = tc_grid<C, PREC, true>(smem);
-        k_step_tiles_tc<C, PREC, true><<<g, 128, smem, st>>>(args);
+        k_step_tiles_tc<C, PREC, true><<<g, TcThreads<PREC, true>::value, smem, st>>>(args);
     }
     return cudaGetLastError();
 }

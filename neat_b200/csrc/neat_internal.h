@@ -8,6 +8,7 @@ namespace neat
 {
 
 // Node-major segment record of the fused step (one ray crossing one node).
+// It carries the ray and the node box so that a sample needs one record load.
 struct __align__(16) SegRec
 {
     int32_t ray;
@@ -17,8 +18,10 @@ struct __align__(16) SegRec
     int32_t rm;          // ray-major (canonical) segment index
     int32_t row;         // active (local) node id = grid row
     int32_t node;        // global node id
+    float o[3], d[3];    // the ray (f32, as GetRays returns it)
+    float mn[3], mx[3];  // the node box
 };
-static_assert(sizeof(SegRec) == 32, "SegRec must be 32 bytes");
+static_assert(sizeof(SegRec) == 80, "SegRec must be 80 bytes");
 
 // Pass 1 of the step: rays from (uv, image), one octree walk per ray, the
 // canonical hit list of ray r at ray_hits[r * cap_ray ...], per-node counts.

@@ -404,7 +404,16 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         sg.rm         = p;  // rank in the ray; made global when placed
         sg.row        = ws.a[i];
         sg.node       = ws.node[i];
-        out[p]        = sg;
+        const NodeEntry e = table[sg.node];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+        {
+            sg.o[c]  = o[c];
+            sg.d[c]  = d[c];
+            sg.mn[c] = plane_coord(e.k[2 * c], D);  // exact: the box lies on the plane grid
+            sg.mx[c] = plane_coord(e.k[2 * c + 1], D);
+        }
+        out[p] = sg;
         atomicAdd(&node_nseg[sg.row], 1);
     }
     if (lane == 0)

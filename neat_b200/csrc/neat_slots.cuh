@@ -12,11 +12,13 @@ namespace neat
 
 constexpr int SLOTS = 128;  // samples per tile
 
-// mark/slot_seg: shared int[128] each.  On return mark[s] is the node-major
-// segment of slot s (tile samples g0 .. g0+127; slots past S map to the last
-// segment).  All threads of the block must call it.
+// mark/slot_seg: shared int[128] each; starts (optional): shared int[129].
+// On return mark[s] is the node-major segment of slot s (tile samples
+// g0 .. g0+127; slots past S map to the last segment) and, if given,
+// starts[mark[s] - seg_lo] is that segment's first sample.  All threads of
+// the block must call it.
 __device__ __forceinline__ void tile_slot_segments(int64_t g0, int seg_lo, int nseg, const int* __restrict__ samp_off,
-                                                   int* mark, int* slot_seg)
+                                                   int* mark, int* slot_seg, int* starts = nullptr)
 {
     const int t = threadIdx.x;
     for (int i = t; i < SLOTS; i += blockDim.x) mark[i] = (i == 0) ? seg_lo : -1;
@@ -27,6 +29,7 @@ __device__ __forceinline__ void tile_slot_segments(int64_t g0, int seg_lo, int n
         if (seg < nseg)
         {
             const int64_t o = samp_off[seg];
+            if (starts) starts[i] = (int)o;
             if (o > g0 && o < g0 + SLOTS) mark[(int)(o - g0)] = seg;
         }
     }
@@ -60,26 +63,18 @@ struct SlotSample
     int ray, rm, row;
 };
 
-// Sample of slot s of segment seg: stratified jitter, o + d t, local coords.
-__device__ __forceinline__ SlotSample slot_sample(const SegRec* __restrict__ segs, const int* __restrict__ samp_off,
-                                                  int seg, int64_t gs, int64_t S, const float* __restrict__ origin,
-                                                  const float* __restrict__ direction,
-                                                  const float* __restrict__ node_min,
-                                                  const float* __restrict__ node_max, uint64_t seed, uint32_t step)
+// Sample of a slot whose segment record is r and whose index in the segment
+// is j: stratified jitter, o + d t, local coordinates.
+__device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool valid, uint64_t seed, uint32_t step)
 {
     SlotSample q;
-    q.valid        = gs < S;
-    const SegRec r = segs[seg];
-    const int j    = q.valid ? (int)(gs - samp_off[seg]) : 0;
+    q.valid = valid;
+    if (!valid) j = 0;
     float ts, ws;
     seg_sample(r.tmin, r.tmax, r.n, j, true, seed, step, r.ray, r.local_base, ts, ws);
-    const float* o  = origin + 3 * (int64_t)r.ray;
-    const float* d  = direction + 3 * (int64_t)r.ray;
-    const float* mn = node_min + 3 * (int64_t)r.node;
-    const float* mx = node_max + 3 * (int64_t)r.node;
-    q.lu            = local_coord(__fadd_rn(o[0], __fmul_rn(d[0], ts)), mn[0], mx[0]);
-    q.lv            = local_coord(__fadd_rn(o[1], __fmul_rn(d[1], ts)), mn[1], mx[1]);
-    q.lw            = local_coord(__fadd_rn(o[2], __fmul_rn(d[2], ts)), mn[2], mx[2]);
+    q.lu            = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], ts)), r.mn[0], r.mx[0]);
+    q.lv            = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], ts)), r.mn[1], r.mx[1]);
+    q.lw            = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], ts)), r.mn[2], r.mx[2]);
     q.weight        = q.valid ? ws : 0.0f;
     q.ray           = r.ray;
     q.rm            = r.rm;

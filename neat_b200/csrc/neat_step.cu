@@ -19,6 +19,7 @@
 
 #include "neat_internal.h"
 #include "neat_scan.cuh"
+#include "neat_slots.cuh"
 #include "neat_tiles.cuh"
 
 namespace neat
@@ -84,23 +85,18 @@ __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
             valid            = gs < S;
             const int seg    = sm.mark[t];
             const SegRec r   = a.segs[seg];
-            const int j      = valid ? (int)(gs - a.samp_off[seg]) : 0;
-            float ts, ws;
-            seg_sample(r.tmin, r.tmax, r.n, j, true, a.seed, a.step, r.ray, r.local_base, ts, ws);
-            const float* o  = a.origin + 3 * (int64_t)r.ray;
-            const float* d  = a.direction + 3 * (int64_t)r.ray;
-            const float* mn = a.node_min + 3 * (int64_t)r.node;
-            const float* mx = a.node_max + 3 * (int64_t)r.node;
-            lu              = local_coord(__fadd_rn(o[0], __fmul_rn(d[0], ts)), mn[0], mx[0]);
-            lv              = local_coord(__fadd_rn(o[1], __fmul_rn(d[1], ts)), mn[1], mx[1]);
-            lw              = local_coord(__fadd_rn(o[2], __fmul_rn(d[2], ts)), mn[2], mx[2]);
+            const SlotSample q =
+                slot_sample(r, valid ? (int)(gs - a.samp_off[seg]) : 0, valid, a.seed, a.step);
+            lu = q.lu;
+            lv = q.lv;
+            lw = q.lw;
             Corners k;
             igs_corners(lu, lv, lw, a.G, a.G, a.G, k);
             float x[C];
             gather_cl<C>(a.grid, r.row, a.G, k, x);
 #pragma unroll
             for (int c = 0; c < C; ++c) sm.XT[c * TT + t] = valid ? x[c] : 0.0f;
-            wgt = valid ? ws : 0.0f;
+            wgt = q.weight;
             ray = r.ray;
             rm  = r.rm;
             row = r.row;

@@ -96,7 +96,7 @@ struct Cfg
     static constexpr int OFF_F  = OFF_AB + (BWD ? P::PIECES * AB::BYTES : 0);
     static constexpr int NF     = HH * C + 3 * HH + 4;
     static constexpr int OFF_I  = OFF_F + NF * 4;
-    static constexpr int OFF_V  = OFF_I + 2 * 128 * 4;
+    static constexpr int OFF_V  = OFF_I + (2 * 128 + 128 + 2 * 132) * 4;
     static constexpr int OFF_R  = OFF_V + 2 * 128 * 4;
     static constexpr int NRED   = std::max(2 * 128 * C, 8 * HH);
     static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
@@ -248,8 +248,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
     float* sb2    = sb1 + HH;
     float* sw3    = sb2 + HH;
     float* sb3    = sw3 + HH;
-    int* mark     = reinterpret_cast<int*>(sm + K::OFF_I);
-    int* slot_seg = mark + 128;
+    int* marks    = reinterpret_cast<int*>(sm + K::OFF_I);  // [2][128] slot -> segment, double buffered
+    int* slot_seg = marks + 2 * 128;                           // scan scratch
+    int* starts   = slot_seg + 128;                            // [2][132] first sample of the tile's segments
     float* sval   = reinterpret_cast<float*>(sm + K::OFF_V);  // [2][128]: y halves / contributions
     float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);  // [2][128][C] dx halves; end: reductions
     uint64_t* mbar_p = reinterpret_cast<uint64_t*>(sm + K::OFF_M);
@@ -305,8 +306,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
     bool ok              = true;
     bool wg_pending      = false;
     bool wg_started      = false;
-    float dw3[HALF / 32] = {};  // lane l: dW3[c0 + 32 i + l]
-    float db3           = 0.0f;
+    float dw3[BWD ? HALF : 1] = {};  // this thread's columns: sum over its samples of h2 * dy
+    float db3                = 0.0f;
 
     auto wait_mma = [&]() -> bool {
         const bool mine = mbar_wait_bounded(mbar, phase);
@@ -321,21 +322,42 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
     constexpr int KS64      = HH / P::KI;
     constexpr int KS128     = 128 / P::KI;
 
+    // Tile set-up in two stages, run one tile ahead inside the MMA waits:
+    // A: slot -> segment map (tile_seg, segment starts, block scan) into buffer b;
+    // B: the slot's segment record, its sample and the grid gather.
+    auto stage_a = [&](int64_t tl, int b) {
+        tile_slot_segments(tl * 128, a.tile_seg[tl], nseg, a.samp_off, marks + 128 * b, slot_seg, starts + 132 * b);
+    };
+    auto stage_b = [&](int64_t tl, int b, SlotSample& qq, float* xx) {
+        const int* mk    = marks + 128 * b;
+        const int seg    = mk[s];
+        const int64_t gs = tl * 128 + s;
+        const bool valid = gs < S;
+        const SegRec r   = a.segs[seg];
+        const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
+        qq               = slot_sample(r, j, valid, a.seed, a.step);
+        Corners kc;
+        igs_corners(qq.lu, qq.lv, qq.lw, a.G, a.G, a.G, kc);
+        gather_cl<C>(a.grid, qq.row, a.G, kc, xx);
+    };
+    int buf = 0;
+    SlotSample q;
+    float x[C];
+    if (blockIdx.x < ntiles)
+    {
+        stage_a(blockIdx.x, 0);
+        stage_b(blockIdx.x, 0, q, x);
+    }
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const int64_t g0 = tile * 128;
-        tile_slot_segments(g0, a.tile_seg[tile], nseg, a.samp_off, mark, slot_seg);
-        const SlotSample q = slot_sample(a.segs, a.samp_off, mark[s], g0 + s, S, a.origin, a.direction, a.node_min,
-                                         a.node_max, a.seed, a.step);
-        float x[C];
-        {
-            Corners kc;
-            igs_corners(q.lu, q.lv, q.lw, a.G, a.G, a.G, kc);
-            gather_cl<C>(a.grid, q.row, a.G, kc, x);
-            if (!q.valid)
+        const int64_t nxt   = tile + gridDim.x;
+        const bool has_next = nxt < ntiles;
+        const int* mark     = marks + 128 * buf;
+        SlotSample qn;
+        float xn[C];
+        if (!q.valid)
 #pragma unroll
-                for (int c = 0; c < C; ++c) x[c] = 0.0f;
-        }
+            for (int c = 0; c < C; ++c) x[c] = 0.0f;
         if (BWD && wg_pending)
         {
             wg_pending = false;
@@ -403,6 +425,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                 }
             mma_commit(mbar);
         }
+        if (has_next)
+        {
+            stage_a(nxt, buf ^ 1);
+            if constexpr (!BWD) stage_b(nxt, buf ^ 1, qn, xn);
+        }
         if (!wait_mma())
         {
             ok = false;
@@ -448,7 +475,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
             const float dy = dv * q.weight * softplus_grad(y, a.beta);
             if (h == 0) db3 += dy;
             // dz2 (this half's columns) -> AB[:, c0:c0+32]; dW3 += h2 dy
-#pragma unroll 1
+#pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
                 float z[16];
@@ -459,9 +486,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                 {
                     const int col  = c0 + 16 * j + i;
                     const float zz = z[i] + sb2[col];
-                    d[i]           = dy * sw3[col] * silu_grad(zz);
-                    const float v  = warp_sum(siluf_(zz) * dy);
-                    if (l == ((16 * j + i) & 31)) dw3[(16 * j + i) >> 5] += v;
+                    const float sg = sigmoidf_(zz);
+                    d[i]           = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                    dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
                 }
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
@@ -483,6 +510,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                     }
                 mma_commit(mbar);
             }
+            if (has_next) stage_b(nxt, buf ^ 1, qn, xn);
             if (!wait_mma())
             {
                 ok = false;
@@ -554,6 +582,13 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
             }
             __syncthreads();  // sred / sval reused by the next tile
         }
+        if (has_next)
+        {
+            q = qn;
+#pragma unroll
+            for (int c = 0; c < C; ++c) x[c] = xn[c];
+        }
+        buf ^= 1;
     }
     // ---- drain
     if (BWD && wg_pending)
@@ -593,11 +628,28 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                 }
             }
         }
-        // dW3: lane l of warp w holds partials of columns c0 + 32 i + l (c0 of
-        // the warp's part); db3 from the first part's threads
+        // dW3: every thread holds its columns summed over its samples; reduce
+        // over the 32 lanes (transpose-reduce) and then over the 4 warps of a part
         __syncthreads();
+        {
+            float v[HALF];
 #pragma unroll
-        for (int i = 0; i < HALF / 32; ++i) sred[w * HH + c0 + 32 * i + l] = dw3[i];
+            for (int i = 0; i < HALF; ++i) v[i] = dw3[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+            {
+#pragma unroll
+                for (int i = 0; i < HALF; ++i)
+                {
+                    const float other = __shfl_xor_sync(0xffffffffu, v[i], o);
+                    v[i] += other;
+                }
+            }
+            // every lane holds the warp's sums; lane l writes columns c0 + l (+ 32)
+#pragma unroll
+            for (int i = 0; i < HALF; ++i)
+                if ((i & 31) == l) sred[w * HH + c0 + i] = v[i];
+        }
         const float b3w = warp_sum(db3);
         __syncthreads();
         if (t < HH)

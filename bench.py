@@ -47,6 +47,8 @@ METRIC = "train rays/s (fwd+bwd)"
 DECODER_DESC = {"simt": "FP32 FFMA (CUDA cores)",
                 "bf16x3": "tcgen05, FP32-accurate: operands split in 3 BF16 pieces, 6 products, FP32 accumulation",
                 "bf16": "tcgen05, BF16 operands, FP32 accumulation (precision variant)"}
+CPU_PATH_DESC = ("reference CPU IGS fwd/bwd compiled from its source (oracle/_ref), OpenMP C port of the CUDA-only "
+                 "ComputeRaySamples, libtorch-CPU decoder/softplus/index_add/MSE/autograd/Adam")
 PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 
 
@@ -169,8 +171,9 @@ def cpu_reference_rays_per_s(cfg, steps, warmup, budget_s=None):
         if budget_s is not None and time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
+    kind = "reference" if CR.reference_igs() is not None else "port"
     return R * done / dt, dict(cores=torch.get_num_threads(), rays=R, steps=done, seconds=dt,
-                               samples_per_ray=runner.last_samples / R)
+                               samples_per_ray=runner.last_samples / R, kind=kind)
 
 
 # --------------------------------------------------------------------------
@@ -206,8 +209,9 @@ def main():
                 "steps": info["steps"], "warmup": args.warmup, "ms_per_step": 1000.0 * info["seconds"] / info["steps"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": {"workload": cfg["desc"], "rays_per_step": info["rays"]},
-                "cpu_baseline": {"value": v, "unit": "rays/s", "cores": info["cores"], "kind": "port",
-                                 "sample": f"{info['rays']} rays/step of the same workload, {info['steps']} steps"},
+                "cpu_baseline": {"value": v, "unit": "rays/s", "cores": info["cores"], "kind": info["kind"],
+                                 "sample": f"{info['rays']} rays/step of the same workload, {info['steps']} steps; "
+                                           + CPU_PATH_DESC},
                 "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -326,9 +330,9 @@ def main():
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0)
-        cpu_base = {"value": cv, "unit": "rays/s", "cores": ci["cores"], "kind": "port",
+        cpu_base = {"value": cv, "unit": "rays/s", "cores": ci["cores"], "kind": ci["kind"],
                     "sample": f"{ci['rays']} rays/step of the same workload x {ci['steps']} steps "
-                              f"({ci['seconds']:.1f} s)"}
+                              f"({ci['seconds']:.1f} s); " + CPU_PATH_DESC}
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:

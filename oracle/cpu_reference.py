@@ -7,30 +7,78 @@ The reference (darglein/NeAT) has no CPU training path for the whole step:
 ComputeRaySamples is CUDA-only (src/structure/HyperTree.cu:206-438).  The CPU
 arm therefore runs, with all host threads:
   * GetRays + CreateSamplesForRays: the oracle's OpenMP C restatement;
-  * IndirectGridSample3D forward/backward: the reference's CPU algorithm
-    (src/modules/IndirectGridSample3D.cu:27-429) as restated in the oracle;
+  * IndirectGridSample3D forward/backward: the reference's own CPU code
+    (src/modules/IndirectGridSample3D.cu:27-429) compiled from its source into
+    oracle/_ref (make -C oracle ref); the oracle's bit-identical restatement
+    when that library is absent;
   * FCBlock, softplus(beta=2), index_add_, MSE, autograd, torch.optim.Adam:
     libtorch CPU, as the reference's geometry code calls them
     (src/geometry/geometry.cpp:102-163, :393-424, samples/reconstruct.cpp:378-396,
     src/geometry/geometry.h:66-88).
 """
+import ctypes
+import os
+
 import numpy as np
 import torch
 
 from oracle import oracle as O
 
+_REF_SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libneat_ref.so")
+_ref = None
+
+
+def reference_igs():
+    """The reference's compiled CPU IGS (None when oracle/_ref is not built)."""
+    global _ref
+    if _ref is None and os.path.exists(_REF_SO):
+        lib = ctypes.CDLL(_REF_SO)
+        P, L, I = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+        lib.ref_igs_forward.argtypes = [P, L, I, I, I, I, P, P, L, P]
+        lib.ref_igs_backward.argtypes = [P, L, I, I, I, I, P, P, L, P, P, P]
+        _ref = lib
+    return _ref
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def igs_forward(grid, index, uv):
+    ref = reference_igs()
+    if ref is None:
+        return O.igs_forward(grid, index, uv)
+    N, C, Z, Y, X = grid.shape
+    out = np.zeros((index.shape[0], C), np.float32)
+    ref.ref_igs_forward(_p(grid), N, C, Z, Y, X, _p(index), _p(uv), index.shape[0], _p(out))
+    return out
+
+
+def igs_backward(grid, index, uv, grad_out):
+    ref = reference_igs()
+    if ref is None:
+        return O.igs_backward(grid, index, uv, grad_out)[0]
+    N, C, Z, Y, X = grid.shape
+    gg = np.zeros_like(grid)
+    gu = np.zeros((index.shape[0], 3), np.float32)
+    ref.ref_igs_backward(_p(grid), N, C, Z, Y, X, _p(index), _p(uv), index.shape[0], _p(grad_out), _p(gg), _p(gu))
+    return gg
+
 
 class _IGS(torch.autograd.Function):
     @staticmethod
     def forward(ctx, grid, index, uv):
-        out = O.igs_forward(grid.detach().numpy(), index.numpy(), uv.numpy())
+        g = np.ascontiguousarray(grid.detach().numpy())
+        i = np.ascontiguousarray(index.numpy())
+        u = np.ascontiguousarray(uv.numpy())
         ctx.save_for_backward(grid, index, uv)
-        return torch.from_numpy(out)
+        return torch.from_numpy(igs_forward(g, i, u))
 
     @staticmethod
     def backward(ctx, go):
         grid, index, uv = ctx.saved_tensors
-        gg, _ = O.igs_backward(grid.detach().numpy(), index.numpy(), uv.numpy(), go.contiguous().numpy())
+        gg = igs_backward(np.ascontiguousarray(grid.detach().numpy()), np.ascontiguousarray(index.numpy()),
+                          np.ascontiguousarray(uv.numpy()), np.ascontiguousarray(go.numpy()))
         return torch.from_numpy(gg), None, None
 
 

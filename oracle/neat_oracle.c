@@ -221,6 +221,19 @@ int oracle_intersect_box(const float* pmin, const float* pmax, const float* o, c
     return 1;
 }
 
+/* Batch form: pair i tests box (pmin[i], pmax[i]) against ray (o[i], d[i]). */
+void oracle_intersect_boxes(long n, const float* pmin, const float* pmax, const float* o, const float* d, int* hit,
+                            float* tmin, float* tmax)
+{
+    for (long i = 0; i < n; ++i)
+    {
+        float t0 = 0, t1 = 0;
+        hit[i]  = oracle_intersect_box(pmin + 3 * i, pmax + 3 * i, o + 3 * i, d + 3 * i, &t0, &t1);
+        tmin[i] = t0;
+        tmax[i] = t1;
+    }
+}
+
 /* Node diagonal as (box_max - box_min).norm() in float (HyperTree.cu:286);  */
 /* Eigen's fixed-size reduction evaluates a0 + (a1 + a2).                    */
 float oracle_node_diag(const float* pmin, const float* pmax)

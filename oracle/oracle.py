@@ -40,6 +40,7 @@ _SIGS = {
     "oracle_tree_build": (None, [_i, _p, _p, _p, _p, _p]),
     "oracle_make_rays": (None, [_i, _p, _p, _i, _i, _p, _p, _p, _p, _p]),
     "oracle_intersect_box": (_i, [_p, _p, _p, _p, _p, _p]),
+    "oracle_intersect_boxes": (None, [_l, _p, _p, _p, _p, _p, _p, _p]),
     "oracle_node_diag": (_f, [_p, _p]),
     "oracle_create_samples": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _i, _u64, _u32, _l, _p, _p, _p, _p, _p, _p, _p]),
     "oracle_ray_segments": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _l, _p, _p, _p, _p, _p, _p, _p]),
@@ -123,6 +124,17 @@ def intersect_box(pmin, pmax, o, d):
     t1 = np.zeros(1, np.float32)
     hit = lib().oracle_intersect_box(_ptr(pmin), _ptr(pmax), _ptr(o), _ptr(d), _ptr(t0), _ptr(t1))
     return bool(hit), float(t0[0]), float(t1[0])
+
+
+def intersect_boxes(pmin, pmax, o, d):
+    """Vectorised slab test over pairs: arrays [n,3] -> (hit, tmin, tmax)."""
+    pmin, pmax, o, d = (_c(x, np.float32) for x in (pmin, pmax, o, d))
+    n = pmin.shape[0]
+    hit = np.zeros(n, np.int32)
+    t0 = np.zeros(n, np.float32)
+    t1 = np.zeros(n, np.float32)
+    lib().oracle_intersect_boxes(n, _ptr(pmin), _ptr(pmax), _ptr(o), _ptr(d), _ptr(hit), _ptr(t0), _ptr(t1))
+    return hit.astype(bool), t0, t1
 
 
 def create_samples(o, d, active_ids, pmin, pmax, M, jitter, seed=0, step=1, cap=None):

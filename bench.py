@@ -37,7 +37,7 @@ WORKLOADS = {
     "full": dict(desc="plain FP32 full size: 64 ellipsoids + 200 voids, 360 x 512^2 projections, Poisson I0=1e4, "
                       "adaptive octree depth 4 (~1500 active), C=8, G=17, decoder 8-64-64-1, M=32, 2^18 rays/batch",
                  n_ell=64, n_void=200, n_angles=360, w=512, h=512, photons=1e4, depth=4, active=1500, C=8, G=17,
-                 M=32, R=1 << 18, seed=2, cpu_rays=1 << 11),
+                 M=32, R=1 << 18, seed=2, cpu_rays=1 << 14),
     "small": dict(desc="plain FP32 small: 8 ellipsoids, 32 x 128^2 projections, octree depth 2 (64 leaves), C=4, "
                        "G=11, decoder 4-64-64-1, M=16, 4096 rays/batch",
                   n_ell=8, n_void=0, n_angles=32, w=128, h=128, photons=None, depth=2, active=None, C=4, G=11, M=16,

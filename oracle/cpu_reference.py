@@ -127,7 +127,7 @@ class CpuReferenceStep:
         T = self.tree
         o, d = O.make_rays(uv, img, self.w, self.h, self.intr, self.rot, self.trans)
         s = O.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, self.cfg["M"], True,
-                             seed=7, step=step, cap=int(uv.shape[0]) * 4096)
+                             seed=7, step=step)
         self.last_samples = s["ray_t"].shape[0]
         local = O.local_samples(s["coords"], s["node_id"], T.node_position_min, T.node_position_max)
         row = torch.from_numpy(T.node_active_prefix_sum[s["node_id"]])

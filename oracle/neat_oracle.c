@@ -330,7 +330,7 @@ static float seg_sample_w(float tmin, float tmax, float step, int n, int j, floa
 long oracle_create_samples(int R, const float* o, const float* d, int A, const long* active_ids, const float* pmin,
                            const float* pmax, int M, int jitter, uint64_t seed, uint32_t step_id, long cap,
                            float* coords, float* ray_t, float* weight, long* ray_index, long* local_index,
-                           long* node_id, int* max_per_ray)
+                           long* node_id, int* max_per_ray, long* needed)
 {
     /* pass 1: samples per ray (parallel over rays) */
     long* off = (long*)malloc(sizeof(long) * ((size_t)R + 1));
@@ -367,6 +367,7 @@ long oracle_create_samples(int R, const float* o, const float* d, int A, const l
         off[r + 1] += off[r];
     }
     long S = off[R];
+    if (needed) *needed = S;
     if (S > cap)
     {
         free(off);

@@ -42,7 +42,8 @@ _SIGS = {
     "oracle_intersect_box": (_i, [_p, _p, _p, _p, _p, _p]),
     "oracle_intersect_boxes": (None, [_l, _p, _p, _p, _p, _p, _p, _p]),
     "oracle_node_diag": (_f, [_p, _p]),
-    "oracle_create_samples": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _i, _u64, _u32, _l, _p, _p, _p, _p, _p, _p, _p]),
+    "oracle_create_samples": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _i, _u64, _u32, _l, _p, _p, _p, _p, _p, _p, _p,
+                                   _p]),
     "oracle_ray_segments": (_l, [_i, _p, _p, _i, _p, _p, _p, _i, _l, _p, _p, _p, _p, _p, _p, _p]),
     "oracle_local_samples": (None, [_l, _p, _p, _p, _p, _p]),
     "oracle_igs_forward": (None, [_p, _l, _i, _i, _i, _i, _p, _p, _l, _p]),
@@ -138,25 +139,31 @@ def intersect_boxes(pmin, pmax, o, d):
 
 
 def create_samples(o, d, active_ids, pmin, pmax, M, jitter, seed=0, step=1, cap=None):
+    """Canonical SampleList of the rays; the arrays are sized to the exact
+    sample count (a first call reports it when the estimate is short)."""
     o, d = _c(o, np.float32), _c(d, np.float32)
     act = _c(active_ids, np.int64)
     pmin, pmax = _c(pmin, np.float32), _c(pmax, np.float32)
     R = o.shape[0]
-    if cap is None:
-        cap = max(16, int(R * M * 3 * (1 << 5)))
-    out = dict(coords=np.zeros((cap, 3), np.float32), ray_t=np.zeros(cap, np.float32),
-               weight=np.zeros(cap, np.float32), ray_index=np.zeros(cap, np.int64),
-               local_index=np.zeros(cap, np.int64), node_id=np.zeros(cap, np.int64))
-    mx = np.zeros(1, np.int32)
-    S = lib().oracle_create_samples(R, _ptr(o), _ptr(d), act.shape[0], _ptr(act), _ptr(pmin), _ptr(pmax), M,
-                                    int(jitter), seed, step, cap, _ptr(out["coords"]), _ptr(out["ray_t"]),
-                                    _ptr(out["weight"]), _ptr(out["ray_index"]), _ptr(out["local_index"]),
-                                    _ptr(out["node_id"]), _ptr(mx))
-    if S < 0:
-        raise RuntimeError(f"oracle_create_samples failed ({S})")
-    res = {k: v[:S].copy() for k, v in out.items()}
-    res["max_per_ray"] = int(mx[0])
-    return res
+    cap = max(16, int(R * M * 4) if cap is None else int(cap))
+    while True:
+        out = dict(coords=np.empty((cap, 3), np.float32), ray_t=np.empty(cap, np.float32),
+                   weight=np.empty(cap, np.float32), ray_index=np.empty(cap, np.int64),
+                   local_index=np.empty(cap, np.int64), node_id=np.empty(cap, np.int64))
+        mx = np.zeros(1, np.int32)
+        need = np.zeros(1, np.int64)
+        S = lib().oracle_create_samples(R, _ptr(o), _ptr(d), act.shape[0], _ptr(act), _ptr(pmin), _ptr(pmax), M,
+                                        int(jitter), seed, step, cap, _ptr(out["coords"]), _ptr(out["ray_t"]),
+                                        _ptr(out["weight"]), _ptr(out["ray_index"]), _ptr(out["local_index"]),
+                                        _ptr(out["node_id"]), _ptr(mx), _ptr(need))
+        if S == -1 and need[0] > cap:
+            cap = int(need[0])
+            continue
+        if S < 0:
+            raise RuntimeError(f"oracle_create_samples failed ({S})")
+        res = {k: v[:S] for k, v in out.items()}
+        res["max_per_ray"] = int(mx[0])
+        return res
 
 
 def ray_segments(o, d, active_ids, pmin, pmax, M, cap=None):

@@ -269,6 +269,46 @@ int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, co
                     uint64_t seed, int step, const neat_step_out* out, void* workspace, size_t workspace_bytes,
                     neat_stream_t stream);
 
+/* ----------------------------------------------------------------------- */
+/* Projection (evaluation).                                                  */
+/* Replaces the per-batch forward of EvalStepProjection                     */
+/* (samples/reconstruct.cpp:551-583): GetRays -> CreateSamplesForRays with   */
+/* interval_jitter = false (a = 0.5, HyperTree.cu:347-358) -> ComputeImage, */
+/* through the step's segment pipeline and forward tiles; no gradients, no */
+/* parameter update.  grid: channel-last [A, G,G,G, C]; decoder packed as   */
+/* above.  batch->target may be NULL unless error_sums is given.            */
+/* error_sums (optional, device f64[2]): += sum (pred - target)^2 and        */
+/* += sum |pred - target| over the batch, added in a fixed order.            */
+/* Workspace: neat_train_step_workspace_bytes(desc, num_rays) bytes.         */
+/* ----------------------------------------------------------------------- */
+typedef struct
+{
+    float* prediction;  /* device [R] */
+    double* error_sums; /* optional device f64[2], accumulated */
+    int64_t* counters;  /* device int64[4], as neat_step_out */
+    int* status;        /* device int, OR-ed neat_status flags */
+} neat_project_out;
+
+int neat_project(const neat_step_desc* desc, const float* grid, const float* decoder, const neat_step_batch* batch,
+                 const neat_project_out* out, void* workspace, size_t workspace_bytes, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Volume export.                                                            */
+/* Replaces HierarchicalNeuralGeometry::UniformSampledVolume                */
+/* (src/geometry/geometry.cpp:166-248) with VolumeSamples / NodeIdForPositionGPU */
+/* (src/structure/HyperTree.cu:546-672): voxel (x,y,z) of an nx*ny*nz volume */
+/* sits at p = (c / (n-1)) * 2 - 1 per axis and takes the decoded density   */
+/* (softplus output) of the active node that the top-down descent finds;    */
+/* voxels outside every active node get value 0, node 0, valid 0.           */
+/* grid: channel-last [A,G,G,G,C] (channel_last != 0, 16-byte aligned) or   */
+/* the reference layout [A,C,G,G,G].  out: [nz][ny][nx] f32 (x fastest);    */
+/* out_node [nz][ny][nx] int64 and out_valid f32 are optional.              */
+/* ----------------------------------------------------------------------- */
+int neat_sample_volume(const void* tree_table, int max_depth, const float* node_min, const float* node_max,
+                       const float* grid, int channel_last, int C, int G, const float* decoder, float softplus_beta,
+                       int nx, int ny, int nz, float* out, int64_t* out_node, float* out_valid,
+                       neat_stream_t stream);
+
 /* Grid layout conversion between the reference's [A, C, G,G,G] and the     */
 /* step's channel-last [A, G,G,G, C].                                        */
 int neat_grid_to_channel_last(const float* src, float* dst, int64_t A, int C, int G, neat_stream_t stream);

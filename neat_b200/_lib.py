@@ -62,6 +62,10 @@ class StepOut(ctypes.Structure):
 NEAT_STEP_PHASES = 6
 
 
+class ProjectOut(ctypes.Structure):
+    _fields_ = [("prediction", c_void_p), ("error_sums", c_void_p), ("counters", c_void_p), ("status", c_void_p)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "neat_status_string": (ctypes.c_char_p, [c_int]),
@@ -94,6 +98,10 @@ _SIGS = {
     "neat_train_step_workspace_bytes": (c_size_t, [ctypes.POINTER(StepDesc), c_int64]),
     "neat_train_step": (c_int, [ctypes.POINTER(StepDesc), ctypes.POINTER(StepState), ctypes.POINTER(StepBatch),
                                 c_uint64, c_int, ctypes.POINTER(StepOut), c_void_p, c_size_t, c_void_p]),
+    "neat_project": (c_int, [ctypes.POINTER(StepDesc), c_void_p, c_void_p, ctypes.POINTER(StepBatch),
+                             ctypes.POINTER(ProjectOut), c_void_p, c_size_t, c_void_p]),
+    "neat_sample_volume": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p,
+                                   c_float, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_grid_to_channel_last": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     "neat_grid_from_channel_last": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     "neat_synth_project": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

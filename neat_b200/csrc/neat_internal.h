@@ -57,10 +57,11 @@ struct StepTileArgs
     const float* decoder;
     float* dec_part;
     const float* dpred;
-    float* partial;
+    double* partial;  // per-segment projection sums (ray-major segment index)
     int* status;
     uint64_t seed;
     uint32_t step;
+    int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;
 };

@@ -64,14 +64,16 @@ struct SlotSample
 };
 
 // Sample of a slot whose segment record is r and whose index in the segment
-// is j: stratified jitter, o + d t, local coordinates.
-__device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool valid, uint64_t seed, uint32_t step)
+// is j: stratified jitter (a = 0.5 when jitter is off), o + d t, local
+// coordinates.
+__device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool valid, bool jitter, uint64_t seed,
+                                                  uint32_t step)
 {
     SlotSample q;
     q.valid = valid;
     if (!valid) j = 0;
     float ts, ws;
-    seg_sample(r.tmin, r.tmax, r.n, j, true, seed, step, r.ray, r.local_base, ts, ws);
+    seg_sample(r.tmin, r.tmax, r.n, j, jitter, seed, step, r.ray, r.local_base, ts, ws);
     q.lu            = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], ts)), r.mn[0], r.mx[0]);
     q.lv            = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], ts)), r.mn[1], r.mx[1]);
     q.lw            = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], ts)), r.mn[2], r.mx[2]);

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
             const int seg    = sm.mark[t];
             const SegRec r   = a.segs[seg];
             const SlotSample q =
-                slot_sample(r, valid ? (int)(gs - a.samp_off[seg]) : 0, valid, a.seed, a.step);
+                slot_sample(r, valid ? (int)(gs - a.samp_off[seg]) : 0, valid, a.jitter != 0, a.seed, a.step);
             lu = q.lu;
             lv = q.lv;
             lw = q.lw;
@@ -127,15 +127,16 @@ __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
         __syncthreads();
         if constexpr (!BWD)
         {
-            // per-segment sums in sample order; a segment crossing the tile
-            // boundary gets exactly two commutative adds onto a zeroed slot.
+            // per-segment sums, in f64 so that the split of a segment across
+            // two tiles (which follows the node-bucket order) does not change
+            // the result; at most two adds onto a zeroed slot
             if (t < TT && valid)
             {
                 const int seg = sm.mark[t];
                 if (t == 0 || sm.mark[t - 1] != seg)
                 {
-                    float sum = 0.0f;
-                    for (int u = t; u < TT && sm.mark[u] == seg; ++u) sum += sm.val[u];
+                    double sum = 0.0;
+                    for (int u = t; u < TT && sm.mark[u] == seg; ++u) sum += (double)sm.val[u];
                     atomicAdd(a.partial + rm, sum);
                 }
             }
@@ -176,6 +177,14 @@ __global__ void k_clamp_samples(int64_t* counters, int64_t sample_cap, int* stat
     counters[3] = (counters[1] + TT - 1) / TT;
 }
 
+// Zero the per-segment partials of this step's segments (counters[0] of them).
+__global__ void k_zero_partial(double* __restrict__ partial, const int64_t* counters)
+{
+    const int64_t n = counters[0];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        partial[i] = 0.0;
+}
+
 __global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, const int64_t* counters,
                            int* __restrict__ tile_seg, int64_t tiles_cap)
 {
@@ -187,7 +196,7 @@ __global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restri
     if (t * TT < e && t < tiles_cap) tile_seg[t] = (int)i;
 }
 
-__global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const float* __restrict__ partial,
+__global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const double* __restrict__ partial,
                            const float* __restrict__ target, float* __restrict__ dpred, float* __restrict__ pred_out,
                            float* __restrict__ loss_part, float invR, const int64_t* nseg_eff)
 {
@@ -200,7 +209,9 @@ __global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const
         if (*nseg_eff > 0)
         {
             const int b = ray_seg_off[r], e = ray_seg_off[r + 1];
-            for (int k = b; k < e; ++k) pred += partial[k];
+            double acc  = 0.0;
+            for (int k = b; k < e; ++k) acc += partial[k];
+            pred = (float)acc;
         }
         const float diff = pred - target[r];
         dpred[r]         = 2.0f * diff * invR;
@@ -387,7 +398,7 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)R * 3 * 4, (size_t)R * 3 * 4, (size_t)R * 4, (size_t)(R + 1) * 4, (size_t)A * 4, (size_t)A * 4,
         (size_t)(A + 1) * 4, (size_t)R * L.cap_ray * sizeof(SegRec), (size_t)cap * sizeof(SegRec), (size_t)cap * 4,
         (size_t)(cap + 1) * 4,
-        (size_t)L.tiles_cap * 4, (size_t)cap * 4, (size_t)R * 4, (size_t)L.loss_blocks * 4,
+        (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
         (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4};
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
@@ -457,11 +468,49 @@ extern "C" int neat_adam(float* param, float* grad, float* exp_avg, float* exp_a
     return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 
-extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
-                               uint64_t seed, int step, const neat_step_out* out, void* workspace,
-                               size_t workspace_bytes, neat_stream_t stream)
+namespace neat
 {
-    if (!d || !s || !b || !out || !out->loss || !out->counters || step < 1) return NEAT_ERR_BAD_INPUT;
+
+// Device pointers of the step workspace.
+struct StepBufs
+{
+    float *origin, *direction;
+    int *ray_nseg, *ray_seg_off, *node_nseg, *node_cursor, *node_seg_off;
+    SegRec *ray_hits, *segs;
+    int *seg_n, *samp_off, *tile_seg;
+    double* partial;
+    float *dpred, *loss_part, *dec_part;
+    int* scratch;
+};
+
+static StepBufs step_bufs(const StepLayout& L, void* workspace)
+{
+    char* ws = (char*)workspace;
+    auto P_  = [&](int i) { return (void*)(ws + L.off[i]); };
+    StepBufs w;
+    w.origin       = (float*)P_(StepLayout::ORIGIN);
+    w.direction    = (float*)P_(StepLayout::DIRECTION);
+    w.ray_nseg     = (int*)P_(StepLayout::RAY_NSEG);
+    w.ray_seg_off  = (int*)P_(StepLayout::RAY_SEG_OFF);
+    w.node_nseg    = (int*)P_(StepLayout::NODE_NSEG);
+    w.node_cursor  = (int*)P_(StepLayout::NODE_CURSOR);
+    w.node_seg_off = (int*)P_(StepLayout::NODE_SEG_OFF);
+    w.ray_hits     = (SegRec*)P_(StepLayout::RAY_HITS);
+    w.segs         = (SegRec*)P_(StepLayout::SEGS);
+    w.seg_n        = (int*)P_(StepLayout::SEG_N);
+    w.samp_off     = (int*)P_(StepLayout::SAMP_OFF);
+    w.tile_seg     = (int*)P_(StepLayout::TILE_SEG);
+    w.partial      = (double*)P_(StepLayout::PARTIAL);
+    w.dpred        = (float*)P_(StepLayout::DPRED);
+    w.loss_part    = (float*)P_(StepLayout::LOSS_PART);
+    w.dec_part     = (float*)P_(StepLayout::DEC_PART);
+    w.scratch      = (int*)P_(StepLayout::SCAN_SCRATCH);
+    return w;
+}
+
+// Host-side checks shared by the step and the projection.
+static int check_desc(const neat_step_desc* d, const neat_step_batch* b)
+{
     if (d->C != 4 && d->C != 8 && d->C != 16) return NEAT_ERR_UNSUPPORTED;
     if (d->decoder_path != NEAT_DECODER_SIMT_FP32 && d->decoder_path != NEAT_DECODER_TC_BF16X3 &&
         d->decoder_path != NEAT_DECODER_TC_BF16)
@@ -472,96 +521,175 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
         return NEAT_ERR_BAD_INPUT;
     if (d->seg_capacity * (int64_t)(d->max_samples_per_node + 1) >= (1ll << 31)) return NEAT_ERR_BAD_INPUT;
     if (!d->tree_table || !d->node_min || !d->node_max || !d->intrinsics || !d->rotation || !d->translation ||
-        !s->grid || !s->grid_m || !s->grid_v || !s->grid_grad || !s->decoder || !s->decoder_m || !s->decoder_v ||
-        !s->decoder_grad || !b->uv || !b->image_id || !b->target || !workspace)
+        !b->uv || !b->image_id)
         return NEAT_ERR_BAD_INPUT;
+    return NEAT_OK;
+}
+
+// Rays -> per-ray hit lists -> node-major segments -> sample offsets -> tile
+// map (phases 0..1 of the step).  counters[0..3] and *status are written.
+static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, const StepLayout& L, const StepBufs& w,
+                           int64_t* cnt, int* status, cudaStream_t st)
+{
+    const int64_t R = b->num_rays, cap = d->seg_capacity;
+    const int A = d->num_active, D = d->max_depth, M = d->max_samples_per_node;
+    bool ok = true;
+    ok      = ok && cudaMemsetAsync(w.node_nseg, 0, (size_t)A * 4, st) == cudaSuccess;
+    ok      = ok && cudaMemsetAsync(w.node_cursor, 0, (size_t)A * 4, st) == cudaSuccess;
+    ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
+    ok = ok && launch_step_rays(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation, d->translation,
+                                d->tree_table, D, M, L.cap_ray, w.origin, w.direction, w.ray_hits, w.ray_nseg,
+                                w.node_nseg, cnt, status, st) == cudaSuccess;
+    ok = ok && scan_exclusive<int>(w.ray_nseg, nullptr, R, w.ray_seg_off, w.scratch, cnt + 0, st) == cudaSuccess;
+    ok = ok && scan_exclusive<int>(w.node_nseg, nullptr, A, w.node_seg_off, w.scratch, nullptr, st) == cudaSuccess;
+    k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, status);
+    ok = ok && launch_step_place(w.ray_hits, w.ray_nseg, w.ray_seg_off, R, L.cap_ray, w.node_seg_off, w.node_cursor,
+                                 w.segs, w.seg_n, cnt + 0, cap, st) == cudaSuccess;
+    k_zero_partial<<<sm_count() * 4, 256, 0, st>>>(w.partial, cnt);
+    ok = ok && scan_exclusive<int>(w.seg_n, cnt + 0, cap, w.samp_off, w.scratch, cnt + 1, st) == cudaSuccess;
+    k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, status);
+    k_tile_seg<<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(w.samp_off, w.seg_n, cnt, w.tile_seg, L.tiles_cap);
+    return ok;
+}
+
+static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const float* grid, float* grid_grad,
+                              const float* decoder, int64_t* cnt, int* status, uint64_t seed, int step, int jitter)
+{
+    StepTileArgs ta;
+    ta.segs      = w.segs;
+    ta.samp_off  = w.samp_off;
+    ta.tile_seg  = w.tile_seg;
+    ta.counters  = cnt;
+    ta.origin    = w.origin;
+    ta.direction = w.direction;
+    ta.node_min  = d->node_min;
+    ta.node_max  = d->node_max;
+    ta.grid      = grid;
+    ta.grid_grad = grid_grad;
+    ta.decoder   = decoder;
+    ta.dec_part  = w.dec_part;
+    ta.dpred     = w.dpred;
+    ta.partial   = w.partial;
+    ta.status    = status;
+    ta.seed      = seed;
+    ta.step      = (uint32_t)step;
+    ta.jitter    = jitter;
+    ta.G         = d->G;
+    ta.beta      = d->softplus_beta;
+    return ta;
+}
+
+static cudaError_t launch_tiles_path(const neat_step_desc* d, bool bwd, const StepTileArgs& ta, cudaStream_t st)
+{
+    const int prec = d->decoder_path == NEAT_DECODER_TC_BF16 ? 0 : 1;
+    return d->decoder_path == NEAT_DECODER_SIMT_FP32 ? launch_tiles_any(d->C, bwd, ta, st)
+                                                     : launch_tiles_tc(d->C, prec, bwd, ta, st);
+}
+
+// Projection of each ray = sum of its segment partials in (tmin, node) order;
+// optional per-block squared and absolute error sums against the target.
+__global__ void k_ray_project(int64_t R, const int* __restrict__ ray_seg_off, const double* __restrict__ partial,
+                              const float* __restrict__ target, float* __restrict__ pred_out,
+                              double* __restrict__ err_part, const int64_t* nseg_eff)
+{
+    __shared__ double red[2][256];
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double sq = 0.0, ab = 0.0;
+    if (r < R)
+    {
+        float pred = 0.0f;
+        if (*nseg_eff > 0)
+        {
+            const int b = ray_seg_off[r], e = ray_seg_off[r + 1];
+            double acc  = 0.0;
+            for (int k = b; k < e; ++k) acc += partial[k];
+            pred = (float)acc;
+        }
+        pred_out[r] = pred;
+        if (target)
+        {
+            const float diff = pred - target[r];
+            sq               = (double)diff * (double)diff;
+            ab               = fabs((double)diff);
+        }
+    }
+    if (!err_part) return;
+    red[0][threadIdx.x] = sq;
+    red[1][threadIdx.x] = ab;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1)
+    {
+        if (threadIdx.x < o)
+        {
+            red[0][threadIdx.x] += red[0][threadIdx.x + o];
+            red[1][threadIdx.x] += red[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        err_part[2 * blockIdx.x]     = red[0][0];
+        err_part[2 * blockIdx.x + 1] = red[1][0];
+    }
+}
+
+// Adds the block sums to out[0..1] in block order (one thread: deterministic).
+__global__ void k_err_final(const double* __restrict__ err_part, int nb, double* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0, a = 0.0;
+    for (int i = 0; i < nb; ++i)
+    {
+        s += err_part[2 * i];
+        a += err_part[2 * i + 1];
+    }
+    out[0] += s;
+    out[1] += a;
+}
+
+}  // namespace neat
+
+extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
+                               uint64_t seed, int step, const neat_step_out* out, void* workspace,
+                               size_t workspace_bytes, neat_stream_t stream)
+{
+    if (!d || !s || !b || !out || !out->loss || !out->counters || step < 1) return NEAT_ERR_BAD_INPUT;
+    const int chk = check_desc(d, b);
+    if (chk != NEAT_OK) return chk;
+    if (!s->grid || !s->grid_m || !s->grid_v || !s->grid_grad || !s->decoder || !s->decoder_m || !s->decoder_v ||
+        !s->decoder_grad || !b->target || !workspace)
+        return NEAT_ERR_BAD_INPUT;
+    const int64_t R = b->num_rays;
     StepLayout L;
     if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
-    cudaStream_t st = (cudaStream_t)stream;
-    char* ws        = (char*)workspace;
-    auto P_ = [&](int i) { return (void*)(ws + L.off[i]); };
-    float* origin     = (float*)P_(StepLayout::ORIGIN);
-    float* direction  = (float*)P_(StepLayout::DIRECTION);
-    int* ray_nseg     = (int*)P_(StepLayout::RAY_NSEG);
-    int* ray_seg_off  = (int*)P_(StepLayout::RAY_SEG_OFF);
-    int* node_nseg    = (int*)P_(StepLayout::NODE_NSEG);
-    int* node_cursor  = (int*)P_(StepLayout::NODE_CURSOR);
-    int* node_seg_off = (int*)P_(StepLayout::NODE_SEG_OFF);
-    SegRec* ray_hits  = (SegRec*)P_(StepLayout::RAY_HITS);
-    SegRec* segs      = (SegRec*)P_(StepLayout::SEGS);
-    int* seg_n        = (int*)P_(StepLayout::SEG_N);
-    int* samp_off     = (int*)P_(StepLayout::SAMP_OFF);
-    int* tile_seg     = (int*)P_(StepLayout::TILE_SEG);
-    float* partial    = (float*)P_(StepLayout::PARTIAL);
-    float* dpred      = (float*)P_(StepLayout::DPRED);
-    float* loss_part  = (float*)P_(StepLayout::LOSS_PART);
-    float* dec_part   = (float*)P_(StepLayout::DEC_PART);
-    int* scratch      = (int*)P_(StepLayout::SCAN_SCRATCH);
-    int64_t* cnt      = out->counters;
-    const int A = d->num_active, D = d->max_depth, M = d->max_samples_per_node;
-    const int64_t cap = d->seg_capacity;
+    cudaStream_t st    = (cudaStream_t)stream;
+    const StepBufs w   = step_bufs(L, workspace);
+    int64_t* cnt       = out->counters;
+    const int A        = d->num_active;
 
     auto phase = [&](int i) {
         if (out->phase_events && out->phase_events[i]) cudaEventRecord((cudaEvent_t)out->phase_events[i], st);
     };
     bool ok = true;
     phase(0);
-    ok      = ok && cudaMemsetAsync(node_nseg, 0, (size_t)A * 4, st) == cudaSuccess;
-    ok      = ok && cudaMemsetAsync(node_cursor, 0, (size_t)A * 4, st) == cudaSuccess;
-    ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
-    ok = ok && launch_step_rays(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation, d->translation,
-                                d->tree_table, D, M, L.cap_ray, origin, direction, ray_hits, ray_nseg, node_nseg, cnt,
-                                out->status, st) == cudaSuccess;
-    ok = ok && scan_exclusive<int>(ray_nseg, nullptr, R, ray_seg_off, scratch, cnt + 0, st) == cudaSuccess;
-    ok = ok && scan_exclusive<int>(node_nseg, nullptr, A, node_seg_off, scratch, nullptr, st) == cudaSuccess;
-    k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, out->status);
-    ok = ok && launch_step_place(ray_hits, ray_nseg, ray_seg_off, R, L.cap_ray, node_seg_off, node_cursor, segs,
-                                 seg_n, cnt + 0, cap, st) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(partial, 0, (size_t)cap * 4, st) == cudaSuccess;
-    ok = ok && scan_exclusive<int>(seg_n, cnt + 0, cap, samp_off, scratch, cnt + 1, st) == cudaSuccess;
-    k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, out->status);
-    k_tile_seg<<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(samp_off, seg_n, cnt, tile_seg, L.tiles_cap);
+    ok = build_segments(d, b, L, w, cnt, out->status, st);
     phase(1);
 
-    StepTileArgs ta;
-    ta.segs      = segs;
-    ta.samp_off  = samp_off;
-    ta.tile_seg  = tile_seg;
-    ta.counters  = cnt;
-    ta.origin    = origin;
-    ta.direction = direction;
-    ta.node_min  = d->node_min;
-    ta.node_max  = d->node_max;
-    ta.grid      = s->grid;
-    ta.grid_grad = s->grid_grad;
-    ta.decoder   = s->decoder;
-    ta.dec_part  = dec_part;
-    ta.dpred     = dpred;
-    ta.partial   = partial;
-    ta.status    = out->status;
-    ta.seed      = seed;
-    ta.step      = (uint32_t)step;
-    ta.G         = d->G;
-    ta.beta      = d->softplus_beta;
-    const int prec = d->decoder_path == NEAT_DECODER_TC_BF16 ? 0 : 1;
-    auto tiles     = [&](bool bwd) {
-        return d->decoder_path == NEAT_DECODER_SIMT_FP32 ? launch_tiles_any(d->C, bwd, ta, st)
-                                                         : launch_tiles_tc(d->C, prec, bwd, ta, st);
-    };
-    ok = ok && tiles(false) == cudaSuccess;
+    const StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
+    ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
     phase(2);
     const float invR = (float)(1.0 / (double)R);
-    k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, ray_seg_off, partial, b->target, dpred, out->prediction, loss_part,
-                                               invR, cnt + 0);
-    k_loss_final<<<1, 1024, 0, st>>>(loss_part, L.loss_blocks, out->loss, invR);
+    k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, w.ray_seg_off, w.partial, b->target, w.dpred, out->prediction,
+                                               w.loss_part, invR, cnt + 0);
+    k_loss_final<<<1, 1024, 0, st>>>(w.loss_part, L.loss_blocks, out->loss, invR);
     phase(3);
-    ok = ok && tiles(true) == cudaSuccess;
+    ok = ok && launch_tiles_path(d, true, ta, st) == cudaSuccess;
     phase(4);
 
     const double bc1g = 1.0 - std::pow((double)d->beta1, step);
     const double bc2g = 1.0 - std::pow((double)d->beta2, step);
     const int P       = (int)decoder_params(d->C);
-    k_dec_reduce_adam<<<(P + 255) / 256, 256, 0, st>>>(dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
+    k_dec_reduce_adam<<<(P + 255) / 256, 256, 0, st>>>(w.dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
                                                         s->decoder_m, s->decoder_v, d->beta1, d->beta2, d->eps,
                                                         (float)(d->lr_decoder / bc1g), (float)std::sqrt(bc2g));
     const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;
@@ -569,6 +697,34 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
                                   (float)(d->lr_grid / bc1g), (float)std::sqrt(bc2g), 1);
     phase(5);
+    ok = ok && cudaGetLastError() == cudaSuccess;
+    return ok ? NEAT_OK : NEAT_ERR_CUDA;
+}
+
+extern "C" int neat_project(const neat_step_desc* d, const float* grid, const float* decoder,
+                            const neat_step_batch* b, const neat_project_out* out, void* workspace,
+                            size_t workspace_bytes, neat_stream_t stream)
+{
+    if (!d || !b || !out || !out->prediction || !out->counters || !out->status || !grid || !decoder || !workspace)
+        return NEAT_ERR_BAD_INPUT;
+    if (out->error_sums && !b->target) return NEAT_ERR_BAD_INPUT;
+    const int chk = check_desc(d, b);
+    if (chk != NEAT_OK) return chk;
+    const int64_t R = b->num_rays;
+    StepLayout L;
+    if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
+    cudaStream_t st  = (cudaStream_t)stream;
+    const StepBufs w = step_bufs(L, workspace);
+    int64_t* cnt     = out->counters;
+    bool ok          = build_segments(d, b, L, w, cnt, out->status, st);
+    const StepTileArgs ta = tile_args(d, w, grid, nullptr, decoder, cnt, out->status, 0, 1, 0);
+    ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
+    // the loss-partials slab holds L.loss_blocks floats; the error sums need two
+    // doubles per block, which the (larger) dpred slab of R floats provides
+    double* err_part = out->error_sums ? (double*)w.dpred : nullptr;
+    k_ray_project<<<L.loss_blocks, 256, 0, st>>>(R, w.ray_seg_off, w.partial, b->target, out->prediction, err_part,
+                                                  cnt + 0);
+    if (err_part) k_err_final<<<1, 32, 0, st>>>(err_part, L.loss_blocks, out->error_sums);
     ok = ok && cudaGetLastError() == cudaSuccess;
     return ok ? NEAT_OK : NEAT_ERR_CUDA;
 }

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
         const bool valid = gs < S;
         const SegRec r   = a.segs[seg];
         const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
-        qq               = slot_sample(r, j, valid, a.seed, a.step);
+        qq               = slot_sample(r, j, valid, a.jitter != 0, a.seed, a.step);
         Corners kc;
         igs_corners(qq.lu, qq.lv, qq.lw, a.G, a.G, a.G, kc);
         gather_cl<C>(a.grid, qq.row, a.G, kc, xx);
@@ -462,8 +462,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                 const int seg = mark[s];
                 if (s == 0 || mark[s - 1] != seg)
                 {
-                    float sum = 0.0f;
-                    for (int u = s; u < 128 && mark[u] == seg; ++u) sum += sval[u];
+                    double sum = 0.0;  // f64: independent of where the tile boundary splits the segment
+                    for (int u = s; u < 128 && mark[u] == seg; ++u) sum += (double)sval[u];
                     atomicAdd(a.partial + q.rm, sum);
                 }
             }

@@ -8,6 +8,7 @@ the current stream.  Nothing is synchronised inside a step; the loss stays on
 the device until the caller reads it.
 """
 import ctypes
+import math
 
 import torch
 
@@ -111,6 +112,75 @@ class FusedTrainer:
                                       self._stream())
         _lib.check(rc, "neat_train_step")
         return self.loss
+
+    def project(self, uv, image_id, target=None, error_sums=None, prediction=None):
+        """Deterministic projection (a = 0.5) of a ray batch with the current
+        parameters: the forward of EvalStepProjection
+        (samples/reconstruct.cpp:551-559).  error_sums: optional device f64[2]
+        that receives += sum (pred-target)^2 and += sum |pred-target|."""
+        R = uv.shape[0]
+        self.reserve(R)
+        if prediction is None:
+            prediction = torch.empty(R, dtype=torch.float32, device=self.dev)
+        if error_sums is not None and target is None:
+            raise ValueError("error_sums needs a target")
+        batch = _lib.StepBatch(uv=uv.data_ptr(), image_id=image_id.data_ptr(),
+                               target=target.data_ptr() if target is not None else None, num_rays=R)
+        out = _lib.ProjectOut(prediction=prediction.data_ptr(),
+                              error_sums=error_sums.data_ptr() if error_sums is not None else None,
+                              counters=self.counters.data_ptr(), status=self.status.data_ptr())
+        rc = self.lib.neat_project(ctypes.byref(self.desc), self.grid.data_ptr(), self.decoder.data_ptr(),
+                                   ctypes.byref(batch), ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
+                                   self._stream())
+        _lib.check(rc, "neat_project")
+        return prediction
+
+    def eval_projection(self, image_ids, projections, rows_per_batch=None):
+        """EvalStepProjection (samples/reconstruct.cpp:504-707) at eval_scale 1:
+        every pixel of each listed image, row batches of rows_per_batch rows
+        (default: as many as fit the reserved workspace), uv = (x/(w-1),
+        y/(h-1)) (CoordinatesRow, src/data/SceneBase.cpp:40-58).  Per image
+        MSE and L1 are means over its pixels; the results average them over the
+        images and PSNR = 10 log10(1 / MSE) (reconstruct.cpp:686-688).
+        projections: device [num_images, h, w] f32 targets.  Returns dict(mse,
+        l1, psnr, images) with images the predicted [len(image_ids), h, w]."""
+        w, h = self.camera.w, self.camera.h
+        if rows_per_batch is None:
+            rows_per_batch = max(1, min(h, max(self.ws_rays, 1 << 16) // w))
+        xs = torch.arange(w, device=self.dev, dtype=torch.float32) / float(w - 1)
+        out_imgs = torch.empty((len(image_ids), h, w), dtype=torch.float32, device=self.dev)
+        sums = torch.zeros((len(image_ids), 2), dtype=torch.float64, device=self.dev)
+        for k, img in enumerate(image_ids):
+            for r0 in range(0, h, rows_per_batch):
+                r1 = min(h, r0 + rows_per_batch)
+                ys = torch.arange(r0, r1, device=self.dev, dtype=torch.float32) / float(h - 1)
+                uv = torch.stack([xs.repeat(r1 - r0), ys.repeat_interleave(w)], 1).contiguous()
+                ids = torch.full((uv.shape[0],), int(img), dtype=torch.int32, device=self.dev)
+                tgt = projections[int(img), r0:r1].reshape(-1).contiguous()
+                self.project(uv, ids, tgt, sums[k], out_imgs[k, r0:r1].view(-1))
+        self.check_status()
+        per = (sums / float(w * h)).cpu().numpy()
+        mse = float(per[:, 0].mean())
+        l1 = float(per[:, 1].mean())
+        psnr = 10.0 * math.log10(1.0 / mse) if mse > 0 else float("inf")
+        return dict(mse=mse, l1=l1, psnr=psnr, images=out_imgs)
+
+    def UniformSampledVolume(self, shape):
+        """UniformSampledVolume (src/geometry/geometry.cpp:166-248): the decoded
+        density on an nx*ny*nz voxel-corner grid of [-1,1]^3, shape = (nx, ny,
+        nz).  Returns (volume [1, nz, ny, nx], node_id [nz, ny, nx] int64,
+        valid [nz, ny, nx] f32) on the device; voxels outside every active
+        node are 0 / node 0 / invalid."""
+        nx, ny, nz = (int(v) for v in shape)
+        vol = torch.empty((1, nz, ny, nx), dtype=torch.float32, device=self.dev)
+        node = torch.empty((nz, ny, nx), dtype=torch.int64, device=self.dev)
+        valid = torch.empty((nz, ny, nx), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.neat_sample_volume(
+            self.tables["table"].data_ptr(), self.tree.max_depth, self.tables["min"].data_ptr(),
+            self.tables["max"].data_ptr(), self.grid.data_ptr(), 1, self.C, self.G, self.decoder.data_ptr(),
+            float(self.desc.softplus_beta), nx, ny, nz, vol.data_ptr(), node.data_ptr(), valid.data_ptr(),
+            self._stream()), "neat_sample_volume")
+        return vol, node, valid
 
     def check_status(self):
         st = int(self.status.item())

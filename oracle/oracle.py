@@ -283,7 +283,7 @@ def decoder_f64(torch, x, dec, C, beta):
 
 
 def image_f64(samples, grid, dec, node_min, node_max, prefix, R, beta=2.0):
-    """Forward projection in f64 with autograd graph; returns (pred [R], ctx)."""
+    """Forward projection in f64 (with autograd graph); returns pred [R]."""
     import torch
     g = torch.from_numpy(samples["coords"]).double()
     nid = torch.from_numpy(samples["node_id"])
@@ -297,6 +297,70 @@ def image_f64(samples, grid, dec, node_min, node_max, prefix, R, beta=2.0):
     val = dens * torch.from_numpy(samples["weight"]).double()
     pred = torch.zeros(R, dtype=torch.float64).index_add(0, torch.from_numpy(samples["ray_index"]), val)
     return pred
+
+
+def volume_positions(nx, ny, nz):
+    """VolumeSamples (src/structure/HyperTree.cu:546-580, swap_xy = false):
+    voxel v = x + nx (y + ny z) at p_d = (c_d / (n_d - 1)) * 2 - 1, each op
+    rounded to float32.  Returns [V, 3] f32."""
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    c = np.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], 1).astype(np.float32)
+    n1 = np.array([nx - 1, ny - 1, nz - 1], np.float32)
+    return (c / n1) * np.float32(2) - np.float32(1)
+
+
+def active_node_for_positions(p, node_active, node_min, node_max, max_depth):
+    """ActiveNodeIdForGlobalPosition (src/structure/HyperTree.cu:598-637) for
+    every row of p: descend from the root into the first child (order 0..7)
+    whose closed box holds the point until an active node; -1 when a leaf is
+    inactive or no child holds the point."""
+    first_leaf = sum(8 ** d for d in range(max_depth))
+    V = p.shape[0]
+    cur = np.zeros(V, np.int64)
+    res = np.full(V, -2, np.int64)  # -2: still descending
+    for _ in range(max_depth + 1):
+        live = res == -2
+        act = live & (node_active[cur] > 0)
+        res[act] = cur[act]
+        live &= ~act
+        leaf = live & (cur >= first_leaf)
+        res[leaf] = -1
+        live &= ~leaf
+        nxt = np.full(V, -1, np.int64)
+        for cid in range(8):
+            c = 8 * cur + 1 + cid
+            c = np.where(live, c, 0)
+            inside = np.all((node_min[c] <= p) & (node_max[c] >= p), axis=1)
+            take = live & (nxt < 0) & inside
+            nxt[take] = c[take]
+        none = live & (nxt < 0)
+        res[none] = -1
+        cur = np.where(live & (nxt >= 0), nxt, cur)
+    res[res == -2] = -1
+    return res
+
+
+def volume_f64(nx, ny, nz, grid, dec, node_active, node_min, node_max, prefix, max_depth, beta=2.0):
+    """UniformSampledVolume (src/geometry/geometry.cpp:166-248) in f64: density
+    of every voxel in its active node, 0 outside.  Returns (vol [V], node [V],
+    valid [V])."""
+    import torch
+    p = volume_positions(nx, ny, nz)
+    node = active_node_for_positions(p, node_active, node_min, node_max, max_depth)
+    valid = node >= 0
+    vol = np.zeros(p.shape[0], np.float64)
+    if valid.any():
+        nid = node[valid]
+        g = torch.from_numpy(p[valid]).double()
+        mn = torch.from_numpy(node_min[nid]).double()
+        mx = torch.from_numpy(node_max[nid]).double()
+        local = (g - mn) / (mx - mn) * 2 - 1
+        row = torch.from_numpy(prefix[nid])
+        grid_t = torch.as_tensor(np.asarray(grid, np.float64))
+        dec_t = torch.as_tensor(np.asarray(dec, np.float64))
+        feat = _trilinear_f64(torch, grid_t, row, local)
+        vol[valid] = decoder_f64(torch, feat, dec_t, grid_t.shape[1], beta).numpy()
+    return vol, np.where(valid, node, 0), valid.astype(np.float32)
 
 
 def adam_f64(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):

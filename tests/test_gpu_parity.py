@@ -297,3 +297,83 @@ def test_projector_matches_oracle(neat, oracle):
     np.testing.assert_allclose(sc.projection.cpu().numpy(), ref, rtol=0, atol=1e-6)
     pts = np.random.default_rng(0).uniform(-1, 1, (500, 3))
     np.testing.assert_array_equal(sc.density(pts), oracle.phantom_density(objs, pts))
+
+
+# ---------------------------------------------------------------- projection (evaluation)
+@pytest.mark.parametrize("path", list(PATHS))
+@pytest.mark.parametrize("which", ["cfg1", "adaptive"])
+def test_project_matches_f64(neat, oracle, case, adaptive_case, which, path):
+    """Deterministic projection (a = 0.5): sample set bit-exact, projection and
+    error sums within the path's tolerance of the f64 oracle."""
+    c = {"cfg1": case, "adaptive": adaptive_case}[which]
+    _, tol_p, _, _ = PATHS[path]
+    tr = _trainer(c, path)
+    sums = torch.zeros(2, dtype=torch.float64, device="cuda")
+    pred = tr.project(_dev(c.uv), _dev(c.img), _dev(c.target), sums)
+    torch.cuda.synchronize()
+    tr.check_status()
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, False)
+    assert int(tr.counters[1].item()) == ref_s["ray_t"].shape[0]
+    import torch as _t
+    ref = oracle.image_f64(ref_s, _t.from_numpy(c.grid.astype(np.float64)), _t.from_numpy(c.dec.astype(np.float64)),
+                           T.node_position_min, T.node_position_max, T.node_active_prefix_sum, c.R).numpy()
+    assert _rel2(pred.cpu().numpy(), ref) < tol_p
+    diff = ref - c.target.astype(np.float64)
+    s = sums.cpu().numpy()
+    assert abs(s[0] - (diff ** 2).sum()) <= 2 * tol_p * (diff ** 2).sum()
+    assert abs(s[1] - np.abs(diff).sum()) <= 2 * tol_p * np.abs(diff).sum()
+    # parameters untouched, deterministic across calls
+    pred2 = tr.project(_dev(c.uv), _dev(c.img))
+    assert torch.equal(pred, pred2)
+    assert tr.step_id == 0
+
+
+def test_eval_projection_psnr(neat, oracle, case):
+    """EvalStepProjection over whole images: per-image MSE/L1 means and
+    PSNR = 10 log10(1/MSE), against the f64 oracle on the same pixels."""
+    c = case
+    tr = _trainer(c, "bf16x3")
+    imgs = [3, 17]
+    proj = _dev(c.proj.astype(np.float32))
+    res = tr.eval_projection(imgs, proj, rows_per_batch=40)
+    o_mse, o_l1 = [], []
+    T = c.tree
+    import torch as _t
+    for i in imgs:
+        ys, xs = np.meshgrid(np.arange(c.h), np.arange(c.w), indexing="ij")
+        uv = np.stack([xs.reshape(-1).astype(np.float32) / np.float32(c.w - 1),
+                       ys.reshape(-1).astype(np.float32) / np.float32(c.h - 1)], 1)
+        ids = np.full(uv.shape[0], i, np.int32)
+        o, d = oracle.make_rays(uv, ids, c.w, c.h, c.intr, c.rot, c.trans)
+        s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, False)
+        p = oracle.image_f64(s, _t.from_numpy(c.grid.astype(np.float64)), _t.from_numpy(c.dec.astype(np.float64)),
+                             T.node_position_min, T.node_position_max, T.node_active_prefix_sum, uv.shape[0]).numpy()
+        np.testing.assert_allclose(res["images"][imgs.index(i)].cpu().numpy().reshape(-1), p, rtol=1e-4, atol=1e-5)
+        diff = p - c.proj[i].reshape(-1).astype(np.float32).astype(np.float64)
+        o_mse.append((diff ** 2).mean())
+        o_l1.append(np.abs(diff).mean())
+    mse, l1 = float(np.mean(o_mse)), float(np.mean(o_l1))
+    assert abs(res["mse"] - mse) <= 1e-5 * mse
+    assert abs(res["l1"] - l1) <= 1e-5 * l1
+    assert abs(res["psnr"] - 10 * np.log10(1 / mse)) < 1e-4
+
+
+# ---------------------------------------------------------------- volume export
+@pytest.mark.parametrize("which", ["cfg1", "adaptive"])
+def test_uniform_sampled_volume(neat, oracle, case, adaptive_case, which):
+    """Voxel-corner volume: node lookup bit-exact (including the inclusive
+    face ties of the descent), density within 1e-5 of f64."""
+    c = {"cfg1": case, "adaptive": adaptive_case}[which]
+    tr = _trainer(c, "simt")
+    n = (33, 17, 25)
+    vol, node, valid = tr.UniformSampledVolume(n)
+    T = c.tree
+    rv, rn, rval = oracle.volume_f64(*n, c.grid, c.dec, T.node_active, T.node_position_min, T.node_position_max,
+                                     T.node_active_prefix_sum, T.max_depth)
+    np.testing.assert_array_equal(node.cpu().numpy().reshape(-1), rn)
+    np.testing.assert_array_equal(valid.cpu().numpy().reshape(-1), rval)
+    v = vol.cpu().numpy().reshape(-1)
+    assert np.all(v[rval == 0] == 0)
+    assert _rel2(v, rv) < 1e-5

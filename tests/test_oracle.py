@@ -282,3 +282,21 @@ def test_oracle_matches_reference_cpu_live(oracle):
         lib.ref_igs_forward(grid.ctypes.data_as(P), N, C, G, G, G, idx.ctypes.data_as(P), uv.ctypes.data_as(P), S,
                             out.ctypes.data_as(P))
         np.testing.assert_array_equal(oracle.igs_forward(grid, idx, uv), out)
+
+
+def test_volume_descent_face_ties(oracle):
+    """ActiveNodeIdForGlobalPosition semantics: closed boxes, first child in
+    order 0..7 wins a shared face, an inactive leaf gives -1."""
+    from neat_b200.tree import HyperTreeBase
+    t = HyperTreeBase(3, 2)
+    t.SetActiveNodes([2] + list(range(9, 17)))  # root child 1 active; child 0 refined; others inactive leaves' parents
+    p = np.array([[0.0, -0.5, -0.5],    # face x = 0 between child 0 (refined) and child 1 -> child 0's leaf
+                  [0.5, -0.5, -0.5],    # inside child 1 (active)
+                  [-0.5, 0.5, -0.5],    # child 2: inactive with no active child -> its leaf 25.. inactive -> -1
+                  [-1.0, -1.0, -1.0]],  # corner: child 0 -> leaf 9
+                 np.float32)
+    n = oracle.active_node_for_positions(p, t.node_active, t.node_position_min, t.node_position_max, 2)
+    assert n[1] == 2 and n[2] == -1 and n[3] == 9
+    assert 9 <= n[0] <= 16 and (t.node_position_max[n[0]][0] == 0.0)
+    pos = oracle.volume_positions(3, 2, 2)
+    np.testing.assert_array_equal(pos[:4], np.array([[-1, -1, -1], [0, -1, -1], [1, -1, -1], [-1, 1, -1]], np.float32))

@@ -2,19 +2,25 @@
 // 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM).
 //
 // One CTA = one or two warpgroups; thread s (and s+128) owns slot s of the
-// tile (TMEM lane s); with two warpgroups the 64 hidden units are split.  Per 128-sample tile:
-//   layer 1 (C -> 64, SIMT fp32)  -> h1 row s written into HB (core-matrix layout)
-//   Z2 = HB[:, :64] . W2^T          tcgen05 (A K-major, B K-major)          -> TMEM D2
-//   epilogue: y, softplus, dy; dz2 = dy w3 silu'(z2) -> AB[:, :64]
-//   dH1 = AB[:, :64] . W2           tcgen05 (A K-major, B = W2 read MN-major) -> TMEM D3
-//   dz1 = dh1 silu'(z1) -> AB[:, 64:]; dx = dz1 . W1 -> grid scatter
-//   [dW2|db2 ; dW1|db1] += AB^T . HB  tcgen05 (A and B MN-major, K = samples)
-//                                    -> TMEM D4, accumulated over all tiles
-// HB holds [h1 | x | 1] per sample row, so the weight-gradient GEMM yields the
-// bias gradients from the ones column and dW1 from the x columns.  A row-major
-// core-matrix buffer [row][col] is at the same time a K-major operand (M=row)
-// and an MN-major operand (K=row): the reduction over samples reads the very
-// buffers the forward GEMM used.
+// tile (TMEM lane s); with two warpgroups the 64 hidden units are split.
+// Per 128-sample tile (HB row s = [h1 | x | 1 0 ..], AB row s = [dz2 | dz1]):
+//   Z1 = HB[:, x|1] . [W1 | b1]^T      tcgen05 (A, B K-major)           -> TMEM D1
+//   h1 = silu(Z1) -> HB[:, :64]
+//   Z2 = HB[:, :64] . W2^T              tcgen05 (A, B K-major)           -> TMEM D2
+//   epilogue: y, softplus (forward: contribution and per-segment sums)
+// backward, continuing:
+//   dz2 = dy w3 silu'(z2) -> AB[:, :64]
+//   dH1 = AB[:, :64] . W2               tcgen05 (B = W2 read MN-major)   -> TMEM D2
+//   dz1 = dH1 silu'(Z1) -> AB[:, 64:]   (Z1 still in D1: no recompute)
+//   dX  = AB[:, 64:] . [W1 | b1]        tcgen05 (B read MN-major)        -> TMEM D2
+//   [dW2|db2 ; dW1|db1] += AB^T . HB    tcgen05 (A and B MN-major, K = samples)
+//                                       -> TMEM D4, accumulated over all tiles
+//   dX scattered into the grid gradient with the trilinear corner weights.
+// The ones column of HB folds b1 into the layer-1 GEMM and yields the bias
+// gradients in the weight-gradient GEMM.  A row-major core-matrix buffer
+// [row][col] is at the same time a K-major operand (M=row) and an MN-major
+// operand (K=row): the reduction over samples reads the very buffers the
+// forward GEMMs used, and one [W1 | b1] buffer serves layer 1 and dX.
 //
 // Precision policies (both on kind::f16 with BF16 operands, FP32 accumulation):
 //   BF16X3: every operand split x = x0 + x1 + x2 into three BF16 pieces
@@ -58,8 +64,8 @@ struct Prec<BF16X3>
     static constexpr int EB = 2, E = 8, KI = 16, PIECES = 3, FMT = 1, NPROD = 6;
 };
 // products (a piece, b piece) with piece orders summing to <= 2
-__device__ __constant__ int kProdA[6] = {0, 0, 1, 0, 1, 2};
-__device__ __constant__ int kProdB[6] = {0, 1, 0, 2, 1, 0};
+__host__ __device__ constexpr int prod_a(int p) { return p == 2 || p == 4 ? 1 : (p == 5 ? 2 : 0); }
+__host__ __device__ constexpr int prod_b(int p) { return p == 1 || p == 4 ? 1 : (p == 3 ? 2 : 0); }
 
 // Core-matrix ("interleaved", no swizzle) layout of a [ROWS][COLS] operand:
 // 8 rows x 16 bytes per core matrix, core matrices of a row group contiguous
@@ -78,33 +84,66 @@ struct Buf
     }
 };
 
-template <int C, int PREC, bool BWD>
-struct Cfg
+// Threads per CTA: 256 (two threads per sample splitting the hidden units)
+// for the three-piece policy, 128 for BF16; and the CTAs per SM the
+// register budget is sized for.
+template <int PREC, bool BWD>
+struct TcThreads
+{
+    static constexpr int value      = (PREC == BF16X3) ? 256 : 128;
+    static constexpr int min_blocks = (PREC == BF16X3) ? (BWD ? 1 : 2) : (BWD ? 2 : 4);
+};
+
+// Shared-memory plan of a tile CTA.  HB rows hold [h1 | x | 1 0 ..] (the
+// weight-gradient B operand).  NX1 separate [x | 1] buffers (0 or 2): with
+// two, the backward issues the next tile's layer-1 GEMM from its own buffer
+// before the current tile's weight-gradient GEMM has finished reading HB.
+template <int C, int PREC, bool BWD, int NX1_>
+struct CfgPlan
 {
     using P                     = Prec<PREC>;
-    static constexpr int XO     = HH;                     // x block in HB
-    static constexpr int XW     = ((C + 7) / 8) * 8;
-    static constexpr int OO     = XO + XW;                // ones column block
-    static constexpr int NW     = ((OO + 8 + 15) / 16) * 16;
-    static constexpr int HBC    = BWD ? NW : HH;          // HB columns
-    using HB                    = Buf<PREC, 128, HBC>;
-    using AB                    = Buf<PREC, 128, 2 * HH>;
+    static constexpr int NX1    = NX1_;
+    static constexpr int XW     = ((C + 7) / 8) * 8;          // x columns (C padded)
+    static constexpr int K1     = ((XW + 1 + 15) / 16) * 16;  // layer-1 K: [x | 1 | 0 ..]
+    static constexpr int ONE    = XW;                         // column of the 1 in [x | 1]
+    static constexpr int NW     = HH + K1;                    // HB columns
+    using HB                    = Buf<PREC, 128, NW>;
+    using X1                    = Buf<PREC, 128, K1>;         // [x | 1 | 0 ..] rows
+    using AB                    = Buf<PREC, 128, 2 * HH>;     // [dz2 | dz1] rows
     using W2                    = Buf<PREC, HH, HH>;
+    using W1                    = Buf<PREC, HH, K1>;          // [h][x | 1]: W1 | b1
+    static constexpr int NH     = TcThreads<PREC, BWD>::value / 128;
     static constexpr int OFF_W2 = 0;
-    static constexpr int OFF_HB = OFF_W2 + P::PIECES * W2::BYTES;
-    static constexpr int OFF_AB = OFF_HB + P::PIECES * HB::BYTES;
+    static constexpr int OFF_W1 = OFF_W2 + P::PIECES * W2::BYTES;
+    static constexpr int OFF_HB = OFF_W1 + P::PIECES * W1::BYTES;
+    static constexpr int OFF_X1 = OFF_HB + P::PIECES * HB::BYTES;
+    static constexpr int X1SZ   = P::PIECES * X1::BYTES;      // one [x | 1] buffer, all pieces
+    static constexpr int OFF_AB = OFF_X1 + NX1 * X1SZ;
     static constexpr int OFF_F  = OFF_AB + (BWD ? P::PIECES * AB::BYTES : 0);
-    static constexpr int NF     = HH * C + 3 * HH + 4;
+    static constexpr int NF     = 2 * HH + 4;                 // b2, w3, b3
     static constexpr int OFF_I  = OFF_F + NF * 4;
     static constexpr int OFF_V  = OFF_I + (2 * 128 + 128 + 2 * 132) * 4;
-    static constexpr int OFF_R  = OFF_V + 2 * 128 * 4;
-    static constexpr int NRED   = std::max(2 * 128 * C, 8 * HH);
+    static constexpr int OFF_Q  = OFF_V + 2 * 128 * 4;        // [2][6][128] slot data for the second thread
+    static constexpr int NQ     = (BWD && NH == 2) ? 2 * 6 * 128 : 0;
+    static constexpr int OFF_R  = OFF_Q + NQ * 4;
+    static constexpr int NRED   = BWD ? 8 * HH : 0;
     static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
-    static constexpr int NEED   = OFF_M + 16;
-    // BF16 backward: pad so that at most two CTAs share an SM (2 x 256 TMEM columns)
-    static constexpr int BYTES = (PREC == BF16 && BWD) ? std::max(NEED, 100 * 1024) : NEED;
-    static constexpr uint32_t TMEM_COLS = BWD ? 256 : 64;
-    static_assert(!BWD || 128 + NW <= 256, "D4 must fit in the allocation");
+    static constexpr int NEED   = OFF_M + 32;                 // two mbarriers + TMEM slot
+};
+
+template <int C, int PREC, bool BWD>
+struct Cfg : CfgPlan<C, PREC, BWD, (BWD && CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
+{
+    using Base = CfgPlan<C, PREC, BWD, (BWD && CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
+    // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 [128, 192 + K1)
+    // weight gradients (h1 columns, then [x | 1] columns), D3 [192 + K1, 192 + 2 K1) dX
+    static constexpr uint32_t TMEM_COLS = BWD ? 256 : 128;
+    // pad so that no more CTAs share an SM than its 512 TMEM columns hold
+    // (233472 B of shared memory per SM, 1 KB reserved per CTA)
+    static constexpr int MIN_BYTES = 233472 / (512 / (int)TMEM_COLS + 1) - 1024 + 16;
+    static constexpr int BYTES     = Base::NEED > MIN_BYTES ? Base::NEED : MIN_BYTES;
+    static_assert(!BWD || 192 + 2 * Base::K1 <= 256, "D4 and D3 must fit in the allocation");
+    static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
 };
 
 // ---------------------------------------------------------------------------
@@ -145,6 +184,25 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
 }
+// All MMAs of one GEMM (every piece product, every K step), fully unrolled:
+// the operand descriptors advance by compile-time byte offsets (the start
+// address field counts 16-byte units and never carries: shared addresses are
+// below 2^18).  acc0: accumulate onto D from the first MMA on.
+template <int PREC, int KS, int A_PIECE, int A_K, int B_PIECE, int B_K>
+__device__ __forceinline__ void gemm(uint32_t d, uint64_t da, uint64_t db, uint32_t idesc, bool acc0)
+{
+    constexpr int NPROD = PREC == 1 ? 6 : 1;
+#pragma unroll
+    for (int p = 0; p < NPROD; ++p)
+#pragma unroll
+        for (int kk = 0; kk < KS; ++kk)
+        {
+            const uint64_t a = da + (uint64_t)((prod_a(p) * A_PIECE + kk * A_K) >> 4);
+            const uint64_t b = db + (uint64_t)((prod_b(p) * B_PIECE + kk * B_K) >> 4);
+            mma<1>(d, a, b, idesc, (acc0 || p || kk) ? 1u : 0u);
+        }
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -220,70 +278,86 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
-// Threads per CTA: 128 (one thread per sample) or 256 (two threads per sample
-// splitting the hidden units; used where shared memory allows one CTA per SM).
-template <int PREC, bool BWD>
-struct TcThreads
-{
-    static constexpr int value = (PREC == BF16X3 && BWD) ? 256 : 128;
-};
-
 template <int C, int PREC, bool BWD>
-__global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_tc(StepTcArgs a)
+__global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, BWD>::min_blocks)
+    k_step_tiles_tc(StepTcArgs a)
 {
     using K  = Cfg<C, PREC, BWD>;
     using P  = Prec<PREC>;
     using HB = typename K::HB;
+    using X1 = typename K::X1;
     using AB = typename K::AB;
     using W2 = typename K::W2;
+    using W1 = typename K::W1;
     constexpr int TC_THREADS = TcThreads<PREC, BWD>::value;
-    constexpr int NH         = TC_THREADS / 128;  // threads per sample
-    constexpr int HALF       = HH / NH;           // hidden units per thread
+    constexpr int NH         = K::NH;     // threads per sample
+    constexpr int HALF       = HH / NH;   // hidden units per thread
+    constexpr bool PIPE      = BWD && K::NX1 == 2;
     extern __shared__ __align__(128) unsigned char sm[];
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
     const int c0 = h * HALF;  // first hidden column of this thread
-    float* sW1    = reinterpret_cast<float*>(sm + K::OFF_F);
-    float* sb1    = sW1 + HH * C;
-    float* sb2    = sb1 + HH;
+    float* sb2    = reinterpret_cast<float*>(sm + K::OFF_F);
     float* sw3    = sb2 + HH;
     float* sb3    = sw3 + HH;
     int* marks    = reinterpret_cast<int*>(sm + K::OFF_I);  // [2][128] slot -> segment, double buffered
     int* slot_seg = marks + 2 * 128;                           // scan scratch
     int* starts   = slot_seg + 128;                            // [2][132] first sample of the tile's segments
     float* sval   = reinterpret_cast<float*>(sm + K::OFF_V);  // [2][128]: y halves / contributions
-    float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);  // [2][128][C] dx halves; end: reductions
+    float* sq     = reinterpret_cast<float*>(sm + K::OFF_Q);  // [2][6][128]: lu, lv, lw, weight, ray, row
+    float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);  // end-of-kernel reductions
     uint64_t* mbar_p = reinterpret_cast<uint64_t*>(sm + K::OFF_M);
-    uint32_t* tslot  = reinterpret_cast<uint32_t*>(sm + K::OFF_M + 8);
+    uint32_t* tslot  = reinterpret_cast<uint32_t*>(sm + K::OFF_M + 16);
     unsigned char* pW2 = sm + K::OFF_W2;
+    unsigned char* pW1 = sm + K::OFF_W1;
     unsigned char* pHB = sm + K::OFF_HB;
     unsigned char* pAB = sm + K::OFF_AB;
-    const uint32_t s_base = smem_u32(sm);
-    const uint32_t mbar   = smem_u32(mbar_p);
+    const uint32_t s_base  = smem_u32(sm);
+    const uint32_t mbar    = smem_u32(mbar_p);      // layer GEMMs
+    const uint32_t mbar_wg = smem_u32(mbar_p + 1);  // dX and weight-gradient GEMMs
 
-    // ---- decoder parameters: W1 / biases / w3 in fp32, W2 as MMA operand pieces
+    // ---- decoder parameters: b2 / w3 / b3 in fp32, [W1 | b1] and W2 as MMA operand pieces
     using O = DecOff<C>;
-    for (int i = t; i < HH * C; i += TC_THREADS) sW1[i] = a.decoder[O::W1 + i];
     for (int i = t; i < HH; i += TC_THREADS)
     {
-        sb1[i] = a.decoder[O::b1 + i];
         sb2[i] = a.decoder[O::b2 + i];
         sw3[i] = a.decoder[O::W3 + i];
     }
     if (t == 0) sb3[0] = a.decoder[O::b3];
-    for (int i = t; i < HH * HH; i += TC_THREADS)
+    for (int i = t; i < HH * HH + HH * K::K1; i += TC_THREADS)
     {
-        const int off = W2::off(i / HH, i % HH);
-        float r       = a.decoder[O::W2 + i];
+        float r;
+        int off;
+        unsigned char* dst;
+        int piece_bytes;
+        if (i < HH * HH)
+        {
+            r           = a.decoder[O::W2 + i];
+            off         = W2::off(i / HH, i % HH);
+            dst         = pW2;
+            piece_bytes = W2::BYTES;
+        }
+        else
+        {
+            const int e = i - HH * HH, hr = e / K::K1, col = e % K::K1;
+            r           = col < C ? a.decoder[O::W1 + hr * C + col] : (col == K::ONE ? a.decoder[O::b1 + hr] : 0.0f);
+            off         = W1::off(hr, col);
+            dst         = pW1;
+            piece_bytes = W1::BYTES;
+        }
 #pragma unroll
         for (int p = 0; p < P::PIECES; ++p)
         {
             const __nv_bfloat16 b = __float2bfloat16_rn(r);
-            *reinterpret_cast<__nv_bfloat16*>(pW2 + p * W2::BYTES + off) = b;
+            *reinterpret_cast<__nv_bfloat16*>(dst + p * piece_bytes + off) = b;
             r -= __bfloat162float(b);
         }
     }
-    if (t == 0) mbar_init(mbar, 1);
+    if (t == 0)
+    {
+        mbar_init(mbar, 1);
+        mbar_init(mbar_wg, 1);
+    }
     if (w == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -297,117 +371,232 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD2 = tmem, tD3 = tmem + 64, tD4 = tmem + 128;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + 128, tD3 = tmem + 192 + K::K1;
 
     const int nseg       = (int)a.counters[0];
     const int64_t S      = a.counters[1];
     const int64_t ntiles = (S + 127) / 128;
     uint32_t phase       = 0;
+    uint32_t phase_wg    = 0;
     bool ok              = true;
     bool wg_pending      = false;
     bool wg_started      = false;
     float dw3[BWD ? HALF : 1] = {};  // this thread's columns: sum over its samples of h2 * dy
     float db3                = 0.0f;
 
-    auto wait_mma = [&]() -> bool {
-        const bool mine = mbar_wait_bounded(mbar, phase);
-        phase ^= 1u;
+    auto wait_on = [&](uint32_t bar, uint32_t& ph) -> bool {
+        const bool mine = mbar_wait_bounded(bar, ph);
+        ph ^= 1u;
         const bool all = __syncthreads_and(mine) != 0;
         fence_after();
         return all;
     };
-    constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);
-    constexpr uint32_t idH  = make_idesc(P::FMT, 0, 1, 128, HH);
-    constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);
+    constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);       // layers 1 and 2
+    constexpr uint32_t idH  = make_idesc(P::FMT, 0, 1, 128, HH);       // dH1
+    constexpr uint32_t idX  = make_idesc(P::FMT, 0, 1, 128, K::K1);    // dX
+    constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);    // weight gradients
+    constexpr int KS1       = K::K1 / P::KI;
     constexpr int KS64      = HH / P::KI;
     constexpr int KS128     = 128 / P::KI;
+    auto x1_addr = [&](int b) -> uint32_t { return s_base + K::OFF_X1 + b * K::X1SZ; };
 
     // Tile set-up in two stages, run one tile ahead inside the MMA waits:
     // A: slot -> segment map (tile_seg, segment starts, block scan) into buffer b;
-    // B: the slot's segment record, its sample and the grid gather.
+    // B: the slot's segment record, its sample and the grid gather (first
+    //    thread of a sample only).
     auto stage_a = [&](int64_t tl, int b) {
         tile_slot_segments(tl * 128, a.tile_seg[tl], nseg, a.samp_off, marks + 128 * b, slot_seg, starts + 132 * b);
     };
-    auto stage_b = [&](int64_t tl, int b, SlotSample& qq, float* xx) {
+    struct Slot
+    {
+        SlotSample q;
+        float x[C];
+    };
+    auto stage_b = [&](int64_t tl, int b) -> Slot {
+        Slot o;
         const int* mk    = marks + 128 * b;
         const int seg    = mk[s];
         const int64_t gs = tl * 128 + s;
         const bool valid = gs < S;
         const SegRec r   = a.segs[seg];
         const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
-        qq               = slot_sample(r, j, valid, a.jitter != 0, a.seed, a.step);
+        o.q              = slot_sample(r, j, valid, a.jitter != 0, a.seed, a.step);
         Corners kc;
-        igs_corners(qq.lu, qq.lv, qq.lw, a.G, a.G, a.G, kc);
-        gather_cl<C>(a.grid, qq.row, a.G, kc, xx);
+        igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
+        gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);
+        if (!valid)
+#pragma unroll
+            for (int c = 0; c < C; ++c) o.x[c] = 0.0f;
+        return o;
     };
-    int buf = 0;
-    SlotSample q;
-    float x[C];
+    // Row s of an [x | 1 | 0 ..] block: the separate buffer b (b >= 0) or the
+    // columns [64, 64 + K1) of HB (b < 0).
+    auto put_x1 = [&](const float* xv, int b) {
+        unsigned char* base = b >= 0 ? sm + K::OFF_X1 + b * K::X1SZ : pHB;
+        const int pbytes    = b >= 0 ? X1::BYTES : HB::BYTES;
+#pragma unroll
+        for (int cc = 0; cc < K::K1; cc += P::E)
+        {
+            float v[P::E];
+#pragma unroll
+            for (int i = 0; i < P::E; ++i)
+            {
+                const int c = cc + i;
+                v[i]        = (c < C) ? xv[c] : ((c == K::ONE) ? 1.0f : 0.0f);
+            }
+            store_chunk<PREC>(base, pbytes, b >= 0 ? X1::off(s, cc) : HB::off(s, HH + cc), v);
+        }
+    };
+    // Slot data the second thread of a sample needs (backward), into buffer qb.
+    auto put_q = [&](const SlotSample& qq, int qb) {
+        if constexpr (K::NQ > 0)
+        {
+            float* qd       = sq + qb * 6 * 128;
+            qd[0 * 128 + s] = qq.lu;
+            qd[1 * 128 + s] = qq.lv;
+            qd[2 * 128 + s] = qq.lw;
+            qd[3 * 128 + s] = qq.valid ? qq.weight : 0.0f;
+            qd[4 * 128 + s] = __int_as_float(qq.valid ? qq.ray : -1);
+            qd[5 * 128 + s] = __int_as_float(qq.row);
+        }
+    };
+    // layer 1 from the separate buffer b (pipelined) or from HB's [x | 1] columns
+    auto issue_l1 = [&](int b) {
+        if constexpr (PIPE)
+            gemm<PREC, KS1, X1::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(x1_addr(b), 128, X1::RG),
+                                                            sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
+        else
+            gemm<PREC, KS1, HB::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(s_base + K::OFF_HB + (HH / 8) * 128, 128, HB::RG),
+                                                            sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
+        mma_commit(mbar);
+    };
+    // dX of the previous tile (TMEM D3), scattered with the trilinear weights;
+    // each thread of a sample takes 8 / NH corners.
+    SlotSample prev;
+    prev.valid = false;
+    auto scatter_prev = [&](int qb) {
+        float dxv[16];
+        tmem_ld16(tD3 + lane, dxv);
+        float dx[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) dx[c] = dxv[c];
+        float lu, lv, lw;
+        int row;
+        bool valid;
+        if (h == 0)
+        {
+            lu = prev.lu; lv = prev.lv; lw = prev.lw; row = prev.row; valid = prev.valid;
+        }
+        else
+        {
+            const float* qd = sq + qb * 6 * 128;
+            lu    = qd[0 * 128 + s];
+            lv    = qd[1 * 128 + s];
+            lw    = qd[2 * 128 + s];
+            valid = __float_as_int(qd[4 * 128 + s]) >= 0;
+            row   = __float_as_int(qd[5 * 128 + s]);
+        }
+        if (valid)
+        {
+            Corners kc;
+            igs_corners(lu, lv, lw, a.G, a.G, a.G, kc);
+            if constexpr (NH == 2)
+            {
+                // constant halves keep the corner arrays in registers
+                if (h == 0)
+                    scatter_cl_half<C>(a.grid_grad, row, a.G, kc, dx, 0);
+                else
+                    scatter_cl_half<C>(a.grid_grad, row, a.G, kc, dx, 1);
+            }
+            else
+            {
+                scatter_cl<C>(a.grid_grad, row, a.G, kc, dx);
+            }
+        }
+    };
+
+    Slot cur;
+    cur.q.valid = false;
+#pragma unroll
+    for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
     if (blockIdx.x < ntiles)
     {
         stage_a(blockIdx.x, 0);
-        stage_b(blockIdx.x, 0, q, x);
+        if (h == 0) cur = stage_b(blockIdx.x, 0);
+        if constexpr (PIPE)
+        {
+            if (h == 0)
+            {
+                put_x1(cur.x, 0);
+                put_q(cur.q, 0);
+            }
+            fence_smem_async();
+            fence_before();
+            __syncthreads();
+            if (t == 0)
+            {
+                fence_after();
+                issue_l1(0);
+            }
+        }
     }
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    int it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it)
     {
         const int64_t nxt   = tile + gridDim.x;
         const bool has_next = nxt < ntiles;
+        const int buf       = it & 1;                 // slot map and slot data of this tile
+        const int xb        = it & 1;                 // [x | 1] buffer of this tile (pipelined)
         const int* mark     = marks + 128 * buf;
-        SlotSample qn;
-        float xn[C];
-        if (!q.valid)
-#pragma unroll
-            for (int c = 0; c < C; ++c) x[c] = 0.0f;
+        const SlotSample& q = cur.q;
+        Slot nx;
+        nx.q.valid = false;
+        // ---- previous tile: dX and weight gradients done -> scatter dX
         if (BWD && wg_pending)
         {
             wg_pending = false;
-            if (!wait_mma())
+            if (!wait_on(mbar_wg, phase_wg))
             {
                 ok = false;
                 break;
             }
+            scatter_prev(buf ^ 1);
         }
-        // ---- HB row s: h1 columns of this half; half 0 adds [x | 1 0 ..]
-#pragma unroll 1
-        for (int k0 = c0; k0 < c0 + HALF; k0 += P::E)
-        {
-            float hv[P::E];
-#pragma unroll
-            for (int i = 0; i < P::E; ++i)
-            {
-                float z = sb1[k0 + i];
-#pragma unroll
-                for (int c = 0; c < C; ++c) z = fmaf(x[c], sW1[(k0 + i) * C + c], z);
-                hv[i] = siluf_(z);
-            }
-            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, k0), hv);
-        }
-        if constexpr (BWD)
+        // ---- Z1 = [x | 1] . [W1 | b1]^T (already in flight when pipelined)
+        if constexpr (!PIPE)
         {
             if (h == 0)
             {
-#pragma unroll
-                for (int cc = 0; cc < K::XW + 8; cc += P::E)
-                {
-                    float v[P::E];
-#pragma unroll
-                    for (int i = 0; i < P::E; ++i)
-                    {
-                        const int c = cc + i;
-                        v[i]        = (c < C) ? x[c] : ((c == K::XW) ? 1.0f : 0.0f);
-                    }
-                    store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, K::XO + cc), v);
-                }
+                put_x1(cur.x, -1);
+                put_q(cur.q, buf);
             }
-            if (h == NH - 1)
+            fence_smem_async();
+            fence_before();
+            __syncthreads();
+            if (t == 0)
             {
-                for (int cc = K::OO + 8; cc < K::NW; cc += P::E)
-                {
-                    float v[P::E] = {};
-                    store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, cc), v);
-                }
+                fence_after();
+                issue_l1(0);
             }
         }
+        if (has_next) stage_a(nxt, buf ^ 1);
+        if (!wait_on(mbar, phase))
+        {
+            ok = false;
+            break;
+        }
+        // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
+#pragma unroll 1
+        for (int j = 0; j < HALF / 16; ++j)
+        {
+            float z[16];
+            tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j), z);
+            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j + 8), z + 8);
+        }
+        if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
         fence_smem_async();
         fence_before();
         __syncthreads();
@@ -415,22 +604,12 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
         if (t == 0)
         {
             fence_after();
-#pragma unroll 1
-            for (int p = 0; p < P::NPROD; ++p)
-                for (int kk = 0; kk < KS64; ++kk)
-                {
-                    const uint32_t ab = s_base + K::OFF_HB + kProdA[p] * HB::BYTES + kk * 256;
-                    const uint32_t bb = s_base + K::OFF_W2 + kProdB[p] * W2::BYTES + kk * 256;
-                    mma<P::FMT>(tD2, sdesc(ab, 128, HB::RG), sdesc(bb, 128, W2::RG), idF, (p | kk) ? 1u : 0u);
-                }
+            gemm<PREC, KS64, HB::BYTES, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                                                             sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
             mma_commit(mbar);
         }
-        if (has_next)
-        {
-            stage_a(nxt, buf ^ 1);
-            if constexpr (!BWD) stage_b(nxt, buf ^ 1, qn, xn);
-        }
-        if (!wait_mma())
+        if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1);
+        if (!wait_on(mbar, phase))
         {
             ok = false;
             break;
@@ -471,10 +650,23 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
         }
         else
         {
-            const float dv = q.valid ? a.dpred[q.ray] : 0.0f;
-            const float dy = dv * q.weight * softplus_grad(y, a.beta);
+            float wgt;
+            int ray;
+            if (h == 0)
+            {
+                wgt = q.valid ? q.weight : 0.0f;
+                ray = q.valid ? q.ray : -1;
+            }
+            else
+            {
+                const float* qd = sq + buf * 6 * 128;
+                wgt             = qd[3 * 128 + s];
+                ray             = __float_as_int(qd[4 * 128 + s]);
+            }
+            const float dv = ray >= 0 ? a.dpred[ray] : 0.0f;
+            const float dy = dv * wgt * softplus_grad(y, a.beta);
             if (h == 0) db3 += dy;
-            // dz2 (this half's columns) -> AB[:, c0:c0+32]; dW3 += h2 dy
+            // dz2 (this thread's columns) -> AB[:, c0 ..]; dW3 += h2 dy
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
@@ -484,10 +676,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
                 {
-                    const int col  = c0 + 16 * j + i;
-                    const float zz = z[i] + sb2[col];
-                    const float sg = sigmoidf_(zz);
-                    d[i]           = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                    const int col   = c0 + 16 * j + i;
+                    const float zz  = z[i] + sb2[col];
+                    const float sg  = sigmoidf_(zz);
+                    d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
                     dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
                 }
 #pragma unroll
@@ -496,112 +688,82 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
             fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h)
+            // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h) -> D2
             if (t == 0)
             {
                 fence_after();
-#pragma unroll 1
-                for (int p = 0; p < P::NPROD; ++p)
-                    for (int kk = 0; kk < KS64; ++kk)
-                    {
-                        const uint32_t ab = s_base + K::OFF_AB + kProdA[p] * AB::BYTES + kk * 256;
-                        const uint32_t bb = s_base + K::OFF_W2 + kProdB[p] * W2::BYTES + kk * (P::KI / 8) * W2::RG;
-                        mma<P::FMT>(tD3, sdesc(ab, 128, AB::RG), sdesc(bb, W2::RG, 128), idH, (p | kk) ? 1u : 0u);
-                    }
+                gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
+                    tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), idH, false);
                 mma_commit(mbar);
             }
-            if (has_next) stage_b(nxt, buf ^ 1, qn, xn);
-            if (!wait_mma())
+            if (has_next && h == 0)
+            {
+                nx = stage_b(nxt, buf ^ 1);
+                // the next tile's [x | 1] buffer was last read by this CTA's
+                // previous tile, whose GEMMs have completed
+                if constexpr (PIPE)
+                {
+                    put_x1(nx.x, xb ^ 1);
+                    put_q(nx.q, buf ^ 1);
+                }
+            }
+            if (!wait_on(mbar, phase))
             {
                 ok = false;
                 break;
             }
-            // ---- epilogue 2: dz1 (this half's k) -> AB[:, 64+c0 ..]; dx partial
-            float dx[C];
-#pragma unroll
-            for (int c = 0; c < C; ++c) dx[c] = 0.0f;
+            // ---- epilogue 2: dz1 = dH1 silu'(Z1) (this thread's columns) -> AB[:, 64 + c0 ..]
 #pragma unroll 1
             for (int j = 0; j < HALF / 16; ++j)
             {
-                float g[16];
-                tmem_ld16(tD3 + lane + c0 + 16 * j, g);
-                float d[16];
+                float g[16], z[16];
+                tmem_ld16(tD2 + lane + c0 + 16 * j, g);
+                tmem_ld16(tD1 + lane + c0 + 16 * j, z);
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
-                {
-                    const int k = c0 + 16 * j + i;
-                    float z     = sb1[k];
-#pragma unroll
-                    for (int c = 0; c < C; ++c) z = fmaf(x[c], sW1[k * C + c], z);
-                    d[i] = g[i] * silu_grad(z);
-#pragma unroll
-                    for (int c = 0; c < C; ++c) dx[c] = fmaf(d[i], sW1[k * C + c], dx[c]);
-                }
+                for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E)
-                    store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), d + i);
+                    store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
             }
-            if constexpr (NH == 2)
-#pragma unroll
-                for (int c = 0; c < C; ++c) sred[(h * 128 + s) * C + c] = dx[c];
             fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- [dW2|db2 ; dW1|db1] += AB^T . HB   (K = samples)
+            // ---- dX = dz1 . [W1 | b1] -> D3;  [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4;
+            //      then (pipelined) the next tile's layer 1 -> D1
             if (t == 0)
             {
                 fence_after();
-#pragma unroll 1
-                for (int p = 0; p < P::NPROD; ++p)
-                    for (int kk = 0; kk < KS128; ++kk)
-                    {
-                        const uint32_t ab = s_base + K::OFF_AB + kProdA[p] * AB::BYTES + kk * (P::KI / 8) * AB::RG;
-                        const uint32_t bb = s_base + K::OFF_HB + kProdB[p] * HB::BYTES + kk * (P::KI / 8) * HB::RG;
-                        const uint32_t acc = (wg_started || p || kk) ? 1u : 0u;
-                        mma<P::FMT>(tD4, sdesc(ab, AB::RG, 128), sdesc(bb, HB::RG, 128), idW, acc);
-                    }
-                mma_commit(mbar);
+                gemm<PREC, KS64, AB::BYTES, 256, W1::BYTES, (P::KI / 8) * W1::RG>(
+                    tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
+                    idX, false);
+                gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, HB::BYTES, (P::KI / 8) * HB::RG>(
+                    tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
+                    wg_started);
+                mma_commit(mbar_wg);
+                if (PIPE && has_next) issue_l1(xb ^ 1);
             }
             wg_started = true;
             wg_pending = true;
-            // dx of sample s (both halves when split; each half scatters four corners)
-            if (q.valid)
-            {
-                Corners kc;
-                igs_corners(q.lu, q.lv, q.lw, a.G, a.G, a.G, kc);
-                if constexpr (NH == 2)
-                {
-#pragma unroll
-                    for (int c = 0; c < C; ++c) dx[c] = sred[s * C + c] + sred[(128 + s) * C + c];
-                    scatter_cl_half<C>(a.grid_grad, q.row, a.G, kc, dx, h);
-                }
-                else
-                {
-                    scatter_cl<C>(a.grid_grad, q.row, a.G, kc, dx);
-                }
-            }
-            __syncthreads();  // sred / sval reused by the next tile
+            prev       = cur.q;
         }
-        if (has_next)
-        {
-            q = qn;
-#pragma unroll
-            for (int c = 0; c < C; ++c) x[c] = xn[c];
-        }
-        buf ^= 1;
+        if (has_next && h == 0) cur = nx;
     }
-    // ---- drain
+    // ---- drain: the last tile's dX and weight gradients
     if (BWD && wg_pending)
     {
-        if (!wait_mma()) ok = false;
+        if (wait_on(mbar_wg, phase_wg))
+            scatter_prev((it - 1) & 1);
+        else
+            ok = false;
     }
     if (!ok) raise_status(a.status, NEAT_ERR_TIMEOUT);
     if constexpr (BWD)
     {
-        // per-CTA decoder-gradient partial (deterministic layout); row s of D4,
-        // columns split between the halves
+        // per-CTA decoder-gradient partial (deterministic layout): row s of D4.
+        // Rows < 64 (dz2 features): columns [0,64) dW2, column 64 + ONE db2;
+        // rows >= 64 (dz1 features): columns 64 + c dW1, column 64 + ONE db1.
         float* dst = a.dec_part + (int64_t)blockIdx.x * O::total;
-        constexpr int NCH = K::NW / 16;
+        constexpr int NCH = (HH + K::K1) / 16;
 #pragma unroll 1
         for (int j = h; j < NCH; j += NH)
         {
@@ -618,13 +780,13 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, 1) k_step_tiles_t
                 if (s < HH)
                 {
                     if (n < HH) dst[O::W2 + s * HH + n] = v[i];
-                    if (n == K::OO) dst[O::b2 + s] = v[i];
+                    if (n == HH + K::ONE) dst[O::b2 + s] = v[i];
                 }
                 else
                 {
                     const int k = s - HH;
-                    if (n >= K::XO && n < K::XO + C) dst[O::W1 + k * C + (n - K::XO)] = v[i];
-                    if (n == K::OO) dst[O::b1 + k] = v[i];
+                    if (n >= HH && n < HH + C) dst[O::W1 + k * C + (n - HH)] = v[i];
+                    if (n == HH + K::ONE) dst[O::b1 + k] = v[i];
                 }
             }
         }
@@ -686,7 +848,8 @@ static int tc_grid(size_t& smem)
     {
         cudaFuncSetAttribute(k_step_tiles_tc<C, PREC, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         // TMEM: 512 columns per SM shared by the resident CTAs
-        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, TcThreads<PREC, BWD>::value, smem, (int)(512 / K::TMEM_COLS)) *
+        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, TcThreads<PREC, BWD>::value, smem,
+                               (int)(512 / K::TMEM_COLS)) *
                  sm_count();
     }
     return blocks;

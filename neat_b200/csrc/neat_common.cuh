@@ -202,10 +202,19 @@ __device__ __forceinline__ void seg_sample(float tmin, float tmax, int n, int j,
 }
 
 // local = (g - min) / (max - min) * 2 - 1, every op rounded (HyperTree.cu:177-192).
+// Octree boxes have power-of-two sizes; dividing by 2^e is then the same
+// correctly rounded value as multiplying by 2^-e, which is what is computed.
 __device__ __forceinline__ float local_coord(float g, float mn, float mx)
 {
-    float size = __fsub_rn(mx, mn);
-    float v    = __fdiv_rn(__fsub_rn(g, mn), size);
+    const float size = __fsub_rn(mx, mn);
+    const float num  = __fsub_rn(g, mn);
+    const uint32_t b = __float_as_uint(size);
+    const uint32_t e = (b >> 23) & 0xFFu;
+    float v;
+    if ((b & 0x807FFFFFu) == 0u && e > 1u && e < 253u)
+        v = __fmul_rn(num, __uint_as_float((254u - e) << 23));
+    else
+        v = __fdiv_rn(num, size);
     return __fsub_rn(__fmul_rn(v, 2.0f), 1.0f);
 }
 

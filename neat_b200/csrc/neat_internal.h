@@ -17,7 +17,7 @@ struct __align__(16) SegRec
     int32_t n;           // samples in the segment
     int32_t rm;          // ray-major (canonical) segment index
     int32_t row;         // active (local) node id = grid row
-    int32_t node;        // global node id
+    float step;          // (tmax - tmin) / n, rounded as the sampler rounds it
     float o[3], d[3];    // the ray (f32, as GetRays returns it)
     float mn[3], mx[3];  // the node box
 };

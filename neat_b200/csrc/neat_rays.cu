@@ -403,8 +403,8 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         sg.n          = ws.n[i];
         sg.rm         = p;  // rank in the ray; made global when placed
         sg.row        = ws.a[i];
-        sg.node       = ws.node[i];
-        const NodeEntry e = table[sg.node];
+        sg.step       = __fdiv_rn(__fsub_rn(sg.tmax, sg.tmin), (float)sg.n);
+        const NodeEntry e = table[ws.node[i]];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
         {

@@ -84,4 +84,42 @@ __device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool v
     return q;
 }
 
+// slot_sample for a full warp of consecutive slots: each lane draws the
+// jitter of its own sample only and takes t of samples j-1 and j+1 from its
+// neighbour lanes (consecutive slots of one segment are consecutive samples);
+// lanes 0 and 31 draw the one neighbour outside the warp when they need it.
+// Same values as slot_sample.  All 32 lanes must call it.
+__device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, bool valid, bool jitter, uint64_t seed,
+                                                       uint32_t step)
+{
+    SlotSample q;
+    q.valid = valid;
+    if (!valid) j = 0;
+    const float t = seg_t(r.tmin, r.step, j, jitter_a(jitter, seed, step, r.ray, r.local_base + j));
+    const int lane = threadIdx.x & 31;
+    float tp       = __shfl_up_sync(0xffffffffu, t, 1);
+    float tn       = __shfl_down_sync(0xffffffffu, t, 1);
+    const bool np  = j > 0 && lane == 0;
+    const bool nn  = j < r.n - 1 && lane == 31;
+    if (np || nn)
+    {
+        const int jj   = np ? j - 1 : j + 1;
+        const float tx = seg_t(r.tmin, r.step, jj, jitter_a(jitter, seed, step, r.ray, r.local_base + jj));
+        if (np)
+            tp = tx;
+        else
+            tn = tx;
+    }
+    const float lo = j == 0 ? r.tmin : __fmul_rn(__fadd_rn(tp, t), 0.5f);
+    const float hi = j == r.n - 1 ? r.tmax : __fmul_rn(__fadd_rn(tn, t), 0.5f);
+    q.lu           = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], t)), r.mn[0], r.mx[0]);
+    q.lv           = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], t)), r.mn[1], r.mx[1]);
+    q.lw           = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], t)), r.mn[2], r.mx[2]);
+    q.weight       = q.valid ? __fsub_rn(hi, lo) : 0.0f;
+    q.ray          = r.ray;
+    q.rm           = r.rm;
+    q.row          = r.row;
+    return q;
+}
+
 }  // namespace neat

@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const bool valid = gs < S;
         const SegRec r   = a.segs[seg];
         const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
-        o.q              = slot_sample(r, j, valid, a.jitter != 0, a.seed, a.step);
+        o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, a.step);
         Corners kc;
         igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
         gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);

@@ -50,6 +50,14 @@ DECODER_DESC = {"simt": "FP32 FFMA (CUDA cores)",
 CPU_PATH_DESC = ("reference CPU IGS fwd/bwd compiled from its source (oracle/_ref), OpenMP C port of the CUDA-only "
                  "ComputeRaySamples, libtorch-CPU decoder/softplus/index_add/MSE/autograd/Adam")
 PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
+# kernels one neat_train_step launches: step scalars, rays + hit lists, 3 scans
+# x 3 kernels, segment clamp, placement, partial zeroing, sample clamp, tile
+# map, forward tiles, ray loss, loss total, backward tiles, decoder Adam, grid Adam
+STEP_LAUNCHES = 22
+KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
+               "bf16x3": "k_step_tiles_tc<C=%d, BF16x3, backward>",
+               "bf16": "k_step_tiles_tc<C=%d, BF16, backward>"}
+PSNR_TARGET_DB = 40.0
 
 
 def hidden_flops(C, H=64):
@@ -150,30 +158,87 @@ def cpu_tree(cfg, objs):
 # --------------------------------------------------------------------------
 # CPU path (oracle port of the reference's CPU execution) -- baseline only
 # --------------------------------------------------------------------------
-def cpu_reference_rays_per_s(cfg, steps, warmup, budget_s=None):
+def cpu_reference_rays_per_s(cfg, steps, warmup, budget_s=None, min_s=None):
     """Times the CPU restatement of the step: C oracle rays + samples + IGS
     (reference CPU semantics), libtorch-CPU decoder / softplus / index_add /
-    MSE / autograd / Adam, with all host threads.  Returns (rays/s, info)."""
+    MSE / autograd / Adam, with all host threads.  Runs `steps` steps, fewer
+    once budget_s is spent, more (up to 4x) until min_s is reached.
+    Returns (rays/s, info)."""
     from oracle import cpu_reference as CR
     from neat_b200 import scene as SC
     objs = SC.ellipsoid_phantom(cfg["n_ell"], cfg["n_void"], seed=cfg["seed"])
     tree = cpu_tree(cfg, objs)
     runner = CR.CpuReferenceStep(objs, tree, cfg)
     R = cfg["cpu_rays"]
-    batches = [runner.batch(R) for _ in range(warmup + steps)]  # host data loading is not timed
+    max_steps = steps if min_s is None else 4 * steps
+    batches = [runner.batch(R) for _ in range(warmup + max_steps)]  # host data loading is not timed
     for i in range(warmup):
         runner.run(*batches[i], i + 1)
     t0 = time.perf_counter()
     done = 0
-    for i in range(steps):
+    for i in range(max_steps):
         runner.run(*batches[warmup + i], warmup + i + 1)
         done += 1
-        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+        el = time.perf_counter() - t0
+        if budget_s is not None and el > budget_s:
+            break
+        if done >= steps and (min_s is None or el >= min_s):
             break
     dt = time.perf_counter() - t0
     kind = "reference" if CR.reference_igs() is not None else "port"
     return R * done / dt, dict(cores=torch.get_num_threads(), rays=R, steps=done, seconds=dt,
                                samples_per_ray=runner.last_samples / R, kind=kind)
+
+
+# --------------------------------------------------------------------------
+# time to PSNR (small workload, CUDA-graph steps)
+# --------------------------------------------------------------------------
+def time_to_psnr(dev, decoders, target_db=PSNR_TARGET_DB, max_steps=3000, every=50):
+    """Train the small workload (config-1 shapes) from the same initial state
+    with each decoder path until the projection PSNR of 4 held-out views
+    (every 8th of the 32) reaches target_db.  PSNR = 10 log10(1 / MSE), MSE
+    the mean over the views of each view's pixel mean (EvalStepProjection,
+    samples/reconstruct.cpp:504-707), squared errors summed in f64.  Training
+    time = CUDA-event time of the graph-replayed steps; evaluation not counted."""
+    from neat_b200 import _lib
+    from neat_b200.trainer import FusedTrainer
+    cfg = dict(WORKLOADS["small"])
+    scene, tree, cam = build_workload(cfg, dev)
+    n = cfg["n_angles"]
+    eval_ids = list(range(0, n, 8))
+    train_ids = [i for i in range(n) if i not in eval_ids]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(77)
+    batches = [scene.sample_batch(cfg["R"], gen, images=train_ids) for _ in range(max_steps)]
+    out = {}
+    for name in decoders:
+        path = {"simt": _lib.NEAT_DECODER_SIMT_FP32, "bf16x3": _lib.NEAT_DECODER_TC_BF16X3,
+                "bf16": _lib.NEAT_DECODER_TC_BF16}[name]
+        tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
+                          decoder_path=path, device=dev)
+        tr.graph_step(*batches[0])  # captures the graph (and runs step 1, not timed)
+        torch.cuda.synchronize()
+        ms, k, curve, reached, psnr = 0.0, 1, [], False, 0.0
+        while k < max_steps and not reached:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(min(every, max_steps - k)):
+                tr.graph_step(*batches[k])
+                k += 1
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            psnr = tr.eval_projection(eval_ids, scene.projection)["psnr"]
+            curve.append([k, round(ms, 3), round(psnr, 3)])
+            reached = psnr >= target_db
+        tr.check_status()
+        out[name] = {"reached": reached, "steps": k, "train_ms": ms, "psnr_db": psnr,
+                     "ms_per_step": ms / max(k - 1, 1), "curve_every_%d_steps" % every: curve}
+    return {"workload": cfg["desc"], "target_psnr_db": target_db, "lr_grid": 1e-2,
+            "eval": "4 held-out views (every 8th of 32), all pixels, a = 0.5 samples; PSNR = 10 log10(1/MSE)",
+            "timing": "CUDA events around CUDA-graph replays of the fused step (batches pre-staged on the "
+                      "device); evaluation excluded", "paths": out}
 
 
 # --------------------------------------------------------------------------
@@ -187,6 +252,7 @@ def main():
     ap.add_argument("--impl", default="neat", choices=["neat", "reference"])
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-psnr", action="store_true", help="skip the time-to-PSNR leg")
     ap.add_argument("--rays", type=int, default=0, help="override rays per batch (profiling runs only)")
     ap.add_argument("--decoder", default="bf16x3", choices=["simt", "bf16x3", "bf16"],
                     help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16")
@@ -327,9 +393,12 @@ def main():
     sm_mhz = clock_info.get("sm_mhz") or 1965.0
     simt_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
 
+    ttp = None
+    if not args.no_psnr:
+        ttp = time_to_psnr(dev, ["simt", "bf16x3", "bf16"])
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0)
+        cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0, min_s=12.0)
         cpu_base = {"value": cv, "unit": "rays/s", "cores": ci["cores"], "kind": ci["kind"],
                     "sample": f"{ci['rays']} rays/step of the same workload x {ci['steps']} steps "
                               f"({ci['seconds']:.1f} s); " + CPU_PATH_DESC}
@@ -347,15 +416,16 @@ def main():
                    "l2": "working set > L2: grid + Adam state %.2f GB per replica" % (
                        4 * 4 * tr.grid.numel() / 1e9)},
         "phase_ms": phase_ms,
-        "roofline": {"kernel": "k_step_tiles<C=%d,backward>" % cfg["C"], "bound": "tensor", "achieved": achieved,
+        "roofline": {"kernel": KERNEL_NAME[args.decoder] % cfg["C"], "bound": "tensor", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                      "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                      "fp32_simt_peak_tflops": simt_peak,
                      "frac_of_fp32_simt": achieved / simt_peak},
         "e2e": {"value": e2e, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
-        "gpu_launches": 20 * K,
+        "gpu_launches": STEP_LAUNCHES * K,
         "clocks": clock_info,
         "cpu_baseline": cpu_base,
+        "time_to_psnr": ttp,
     }
     print(json.dumps(line))
 

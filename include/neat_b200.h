@@ -239,6 +239,11 @@ typedef struct
     float* decoder_m;
     float* decoder_v;
     float* decoder_grad;
+    /* optional device int: when set, the step number is (*step_counter + 1),
+     * incremented on the device at the start of the step, and the `step`
+     * argument is ignored -- a captured CUDA graph of the step then advances
+     * by itself on every replay.  NULL: the `step` argument is used. */
+    int* step_counter;
 } neat_step_state;
 
 typedef struct

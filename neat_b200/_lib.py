@@ -47,7 +47,7 @@ class StepDesc(ctypes.Structure):
 
 class StepState(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("grid", "grid_m", "grid_v", "grid_grad",
-                                        "decoder", "decoder_m", "decoder_v", "decoder_grad")]
+                                        "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter")]
 
 
 class StepBatch(ctypes.Structure):

@@ -61,6 +61,7 @@ struct StepTileArgs
     int* status;
     uint64_t seed;
     uint32_t step;
+    const int* step_dev;  // when set, the step number is read here (device-side step counter)
     int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;

@@ -86,7 +86,8 @@ __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
             const int seg    = sm.mark[t];
             const SegRec r   = a.segs[seg];
             const SlotSample q =
-                slot_sample(r, valid ? (int)(gs - a.samp_off[seg]) : 0, valid, a.jitter != 0, a.seed, a.step);
+                slot_sample(r, valid ? (int)(gs - a.samp_off[seg]) : 0, valid, a.jitter != 0, a.seed,
+                            a.step_dev ? (uint32_t)*a.step_dev : a.step);
             lu = q.lu;
             lv = q.lv;
             lw = q.lw;
@@ -254,11 +255,41 @@ __device__ __forceinline__ void adam_update(float& p, float gr, float& m, float&
     p                 = fmaf(-step_size, m / denom, p);
 }
 
+// Per-step scalars written on the device at the start of the step: the step
+// number (host argument or device counter) and Adam's bias-corrected step
+// sizes, computed in double as torch::optim::Adam does.
+struct StepScalars
+{
+    int step;
+    float grid_step_size;  // lr_grid / (1 - beta1^t)
+    float dec_step_size;   // lr_decoder / (1 - beta1^t)
+    float sqrt_bc2;        // sqrt(1 - beta2^t)
+};
+
+__global__ void k_step_begin(int* counter, int host_step, double lr_grid, double lr_dec, double b1, double b2,
+                             StepScalars* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int t = host_step;
+    if (counter)
+    {
+        t        = *counter + 1;
+        *counter = t;
+    }
+    const double bc1    = 1.0 - pow(b1, (double)t);
+    const double bc2    = 1.0 - pow(b2, (double)t);
+    out->step           = t;
+    out->grid_step_size = (float)(lr_grid / bc1);
+    out->dec_step_size  = (float)(lr_dec / bc1);
+    out->sqrt_bc2       = (float)sqrt(bc2);
+}
+
 __global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, int P, float* __restrict__ grad,
                                   float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float b1,
-                                  float b2, float eps, float step_size, float sqrt_bc2)
+                                  float b2, float eps, const StepScalars* __restrict__ sc)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float step_size = sc->dec_step_size, sqrt_bc2 = sc->sqrt_bc2;
+    const int i           = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     float gsum = 0.0f;
     for (int b = 0; b < nparts; ++b) gsum += part[(int64_t)b * P + i];
@@ -271,8 +302,14 @@ __global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, in
 }
 
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
-                       int64_t n, float b1, float b2, float eps, float step_size, float sqrt_bc2, int zero_grad)
+                       int64_t n, float b1, float b2, float eps, float step_size, float sqrt_bc2, int zero_grad,
+                       const StepScalars* __restrict__ sc)
 {
+    if (sc)
+    {
+        step_size = sc->grid_step_size;
+        sqrt_bc2  = sc->sqrt_bc2;
+    }
     const int64_t n4     = n / 4;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride)
@@ -370,7 +407,7 @@ struct StepLayout
     enum
     {
         ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
-        SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, NUM
+        SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, NUM
     };
     size_t off[NUM];
     size_t total;
@@ -399,7 +436,7 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)(A + 1) * 4, (size_t)R * L.cap_ray * sizeof(SegRec), (size_t)cap * sizeof(SegRec), (size_t)cap * 4,
         (size_t)(cap + 1) * 4,
         (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
-        (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4};
+        (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars)};
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
     {
@@ -464,7 +501,7 @@ extern "C" int neat_adam(float* param, float* grad, float* exp_avg, float* exp_a
     const double bc2 = 1.0 - std::pow((double)beta2, step);
     const int grid   = std::min<int64_t>((n / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
     k_adam<<<grid, 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, beta1, beta2, eps,
-                                                   (float)(lr / bc1), (float)std::sqrt(bc2), zero_grad);
+                                                   (float)(lr / bc1), (float)std::sqrt(bc2), zero_grad, nullptr);
     return cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 
@@ -481,6 +518,7 @@ struct StepBufs
     double* partial;
     float *dpred, *loss_part, *dec_part;
     int* scratch;
+    StepScalars* scal;
 };
 
 static StepBufs step_bufs(const StepLayout& L, void* workspace)
@@ -505,6 +543,7 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.loss_part    = (float*)P_(StepLayout::LOSS_PART);
     w.dec_part     = (float*)P_(StepLayout::DEC_PART);
     w.scratch      = (int*)P_(StepLayout::SCAN_SCRATCH);
+    w.scal         = (StepScalars*)P_(StepLayout::SCAL);
     return w;
 }
 
@@ -573,6 +612,7 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.status    = status;
     ta.seed      = seed;
     ta.step      = (uint32_t)step;
+    ta.step_dev  = &w.scal->step;
     ta.jitter    = jitter;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;
@@ -653,7 +693,8 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
                                uint64_t seed, int step, const neat_step_out* out, void* workspace,
                                size_t workspace_bytes, neat_stream_t stream)
 {
-    if (!d || !s || !b || !out || !out->loss || !out->counters || step < 1) return NEAT_ERR_BAD_INPUT;
+    if (!d || !s || !b || !out || !out->loss || !out->counters || (!s->step_counter && step < 1))
+        return NEAT_ERR_BAD_INPUT;
     const int chk = check_desc(d, b);
     if (chk != NEAT_OK) return chk;
     if (!s->grid || !s->grid_m || !s->grid_v || !s->grid_grad || !s->decoder || !s->decoder_m || !s->decoder_v ||
@@ -672,6 +713,8 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     };
     bool ok = true;
     phase(0);
+    k_step_begin<<<1, 32, 0, st>>>(s->step_counter, step, (double)d->lr_grid, (double)d->lr_decoder,
+                                   (double)d->beta1, (double)d->beta2, w.scal);
     ok = build_segments(d, b, L, w, cnt, out->status, st);
     phase(1);
 
@@ -686,16 +729,14 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ok = ok && launch_tiles_path(d, true, ta, st) == cudaSuccess;
     phase(4);
 
-    const double bc1g = 1.0 - std::pow((double)d->beta1, step);
-    const double bc2g = 1.0 - std::pow((double)d->beta2, step);
-    const int P       = (int)decoder_params(d->C);
+    const int P = (int)decoder_params(d->C);
     k_dec_reduce_adam<<<(P + 255) / 256, 256, 0, st>>>(w.dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
                                                         s->decoder_m, s->decoder_v, d->beta1, d->beta2, d->eps,
-                                                        (float)(d->lr_decoder / bc1g), (float)std::sqrt(bc2g));
+                                                        w.scal);
     const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;
     const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
-                                  (float)(d->lr_grid / bc1g), (float)std::sqrt(bc2g), 1);
+                                  0.0f, 1.0f, 1, w.scal);
     phase(5);
     ok = ok && cudaGetLastError() == cudaSuccess;
     return ok ? NEAT_OK : NEAT_ERR_CUDA;
@@ -716,7 +757,8 @@ extern "C" int neat_project(const neat_step_desc* d, const float* grid, const fl
     cudaStream_t st  = (cudaStream_t)stream;
     const StepBufs w = step_bufs(L, workspace);
     int64_t* cnt     = out->counters;
-    bool ok          = build_segments(d, b, L, w, cnt, out->status, st);
+    k_step_begin<<<1, 32, 0, st>>>(nullptr, 1, 0.0, 0.0, 0.5, 0.5, w.scal);
+    bool ok               = build_segments(d, b, L, w, cnt, out->status, st);
     const StepTileArgs ta = tile_args(d, w, grid, nullptr, decoder, cnt, out->status, 0, 1, 0);
     ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
     // the loss-partials slab holds L.loss_blocks floats; the error sums need two

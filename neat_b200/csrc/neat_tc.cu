@@ -373,11 +373,12 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
     const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + 128, tD3 = tmem + 192 + K::K1;
 
-    const int nseg       = (int)a.counters[0];
-    const int64_t S      = a.counters[1];
-    const int64_t ntiles = (S + 127) / 128;
-    uint32_t phase       = 0;
-    uint32_t phase_wg    = 0;
+    const int nseg         = (int)a.counters[0];
+    const int64_t S        = a.counters[1];
+    const int64_t ntiles   = (S + 127) / 128;
+    const uint32_t step_no = a.step_dev ? (uint32_t)*a.step_dev : a.step;
+    uint32_t phase         = 0;
+    uint32_t phase_wg      = 0;
     bool ok              = true;
     bool wg_pending      = false;
     bool wg_started      = false;
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const bool valid = gs < S;
         const SegRec r   = a.segs[seg];
         const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
-        o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, a.step);
+        o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no);
         Corners kc;
         igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
         gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);

@@ -172,11 +172,18 @@ class SyntheticScene:
                                           torch.cuda.current_stream(self.device).cuda_stream), "neat_synth_density")
         return out.cpu().numpy()
 
-    def sample_batch(self, num_rays, generator, device=None):
-        """uv [R,2] f32, image_id [R] i32, target [R] f32 (a1 of the hot path)."""
+    def sample_batch(self, num_rays, generator, device=None, images=None):
+        """uv [R,2] f32, image_id [R] i32, target [R] f32 (a1 of the hot path):
+        uniform image (from `images`, the training split, when given), uniform
+        integer pixel, uv = pixel / (size - 1), target = that pixel
+        (RandomMultiSceneDataset::get_batch, src/data/Dataloader.cpp:8-49)."""
         dev = self.projection.device if device is None else torch.device(device)
         g = generator
-        img = torch.randint(0, self.n_img, (num_rays,), generator=g, device=g.device)
+        if images is None:
+            img = torch.randint(0, self.n_img, (num_rays,), generator=g, device=g.device)
+        else:
+            ids = torch.as_tensor(images, dtype=torch.int64, device=g.device)
+            img = ids[torch.randint(0, ids.numel(), (num_rays,), generator=g, device=g.device)]
         x = torch.randint(0, self.w, (num_rays,), generator=g, device=g.device)
         y = torch.randint(0, self.h, (num_rays,), generator=g, device=g.device)
         uv = torch.stack([x.float() / (self.w - 1), y.float() / (self.h - 1)], 1)

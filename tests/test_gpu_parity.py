@@ -377,3 +377,26 @@ def test_uniform_sampled_volume(neat, oracle, case, adaptive_case, which):
     v = vol.cpu().numpy().reshape(-1)
     assert np.all(v[rval == 0] == 0)
     assert _rel2(v, rv) < 1e-5
+
+
+# ---------------------------------------------------------------- CUDA graph replay
+def test_graph_step_matches_eager(neat, case):
+    """graph_step (captured once, replayed) follows step() over several steps;
+    the device step counter advances on every replay."""
+    c = case
+    rng = np.random.default_rng(11)
+    batches = []
+    for _ in range(5):
+        idx = rng.permutation(c.R)[:2048]
+        batches.append((_dev(c.uv[idx]), _dev(c.img[idx]), _dev(c.target[idx])))
+    a = _trainer(c, "bf16x3")
+    b = _trainer(c, "bf16x3")
+    la = [float(a.step(*bt).item()) for bt in batches]
+    lb = [float(b.graph_step(*bt).item()) for bt in batches]
+    torch.cuda.synchronize()
+    a.check_status()
+    b.check_status()
+    assert int(b.step_counter.item()) == 5 and int(a.step_counter.item()) == 5
+    np.testing.assert_allclose(lb, la, rtol=1e-5)
+    assert _rel2(b.grid.cpu().numpy(), a.grid.cpu().numpy()) < 1e-6
+    assert _rel2(b.decoder.cpu().numpy(), a.decoder.cpu().numpy()) < 1e-6

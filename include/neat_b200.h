@@ -215,6 +215,9 @@ typedef struct
     int64_t seg_capacity;
     /* decoder GEMMs: NEAT_DECODER_* */
     int decoder_path;
+    /* nonzero: the workspace also holds the proposal's per-segment CDFs and
+     * bins, so that state->proposal may be used */
+    int proposal;
 } neat_step_desc;
 
 /* Decoder paths of the fused step.
@@ -228,6 +231,55 @@ typedef struct
 #define NEAT_DECODER_SIMT_FP32 0
 #define NEAT_DECODER_TC_BF16X3 1
 #define NEAT_DECODER_TC_BF16 2
+
+/* ----------------------------------------------------------------------- */
+/* Learned sample proposal (no counterpart in the reference, whose sampler  */
+/* is uniform stratified: HyperTree.cu:347-358).  A tiny MLP maps a ray-node */
+/* segment -- the node's 6-float descriptor, entry and exit points in      */
+/* node-local coordinates, chord length over the node edge, the centroid's */
+/* projection onto the chord and its distance from it over the spread, one */
+/* zero: 16 inputs -- via 32 -> 32 SiLU units to 8 logits over equal sub-  */
+/* intervals */
+/* of [tmin,tmax].  The node descriptor is the method's own density in the */
+/* node, decoded on a 4^3 lattice at every TRAIN call: density-weighted     */
+/* centroid (3, local), spread (RMS distance from it), log mean density,   */
+/* log(peak / mean);                                                         */
+/* p = (1 - mix) softmax + mix / 8.  In SAMPLE mode the step places its     */
+/* samples by inverting that piecewise-linear CDF at (j + a_j) / n (weights */
+/* by the reference's midpoint rule on the placed positions).  In TRAIN mode */
+/* the step samples uniformly (the fallback and error judge), bins every    */
+/* sample's contribution density * weight into its segment's 8 sub-intervals */
+/* and, after its own update, runs `iters` Adam iterations of the proposal  */
+/* on the cross-entropy between p and where the density changes: bin b's    */
+/* target is |m_b - m_b-1| + |m_b+1 - m_b| of the binned masses m, each     */
+/* segment weighted by its total variation (the midpoint rule is exact on  */
+/* constant and linear stretches; its error sits at changes).               */
+/* params: neat_proposal_params() floats,                                   */
+/*   W1 [32][16] | b1 [32] | W2 [32][32] | b2 [32] | W3 [8][32] | b3 [8].    */
+/* ----------------------------------------------------------------------- */
+#define NEAT_PROPOSAL_IN 16
+#define NEAT_PROPOSAL_HIDDEN 32
+#define NEAT_PROPOSAL_BINS 8
+#define NEAT_PROPOSAL_OFF 0
+#define NEAT_PROPOSAL_SAMPLE 1
+#define NEAT_PROPOSAL_TRAIN 2
+int64_t neat_proposal_params(void);
+
+typedef struct
+{
+    int mode;          /* NEAT_PROPOSAL_* for this call */
+    float* params;     /* neat_proposal_params() floats */
+    float* m;          /* Adam first moment */
+    float* v;          /* Adam second moment */
+    float* grad;       /* out: gradient of the last training iteration */
+    int* step_counter; /* device int: proposal Adam steps taken (advanced on the device) */
+    float* loss;       /* optional device f32[2]: mass-weighted mean cross-entropy of the last
+                        * iteration and of its targets' entropy (their difference: the KL) */
+    float lr, beta1, beta2, eps;
+    float mix;         /* uniform share of the sample density, e.g. 0.1 */
+    int iters;         /* Adam iterations per TRAIN call */
+    float* node_desc;  /* [num_active][6] node descriptors, written by TRAIN calls */
+} neat_proposal;
 
 typedef struct
 {
@@ -244,6 +296,8 @@ typedef struct
      * argument is ignored -- a captured CUDA graph of the step then advances
      * by itself on every replay.  NULL: the `step` argument is used. */
     int* step_counter;
+    /* optional learned proposal (requires desc->proposal != 0); NULL: off */
+    const neat_proposal* proposal;
 } neat_step_state;
 
 typedef struct
@@ -285,6 +339,8 @@ int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, co
 /* error_sums (optional, device f64[2]): += sum (pred - target)^2 and        */
 /* += sum |pred - target| over the batch, added in a fixed order.            */
 /* Workspace: neat_train_step_workspace_bytes(desc, num_rays) bytes.         */
+/* proposal: NULL (uniform stratified, a = 0.5) or a learned proposal in    */
+/* NEAT_PROPOSAL_SAMPLE mode (samples at the CDF inverse of (j + 0.5) / n). */
 /* ----------------------------------------------------------------------- */
 typedef struct
 {
@@ -294,8 +350,9 @@ typedef struct
     int* status;        /* device int, OR-ed neat_status flags */
 } neat_project_out;
 
-int neat_project(const neat_step_desc* desc, const float* grid, const float* decoder, const neat_step_batch* batch,
-                 const neat_project_out* out, void* workspace, size_t workspace_bytes, neat_stream_t stream);
+int neat_project(const neat_step_desc* desc, const float* grid, const float* decoder, const neat_proposal* proposal,
+                 const neat_step_batch* batch, const neat_project_out* out, void* workspace, size_t workspace_bytes,
+                 neat_stream_t stream);
 
 /* ----------------------------------------------------------------------- */
 /* Volume export.                                                            */

@@ -41,13 +41,24 @@ class StepDesc(ctypes.Structure):
         ("intrinsics", c_void_p), ("rotation", c_void_p), ("translation", c_void_p),
         ("C", c_int), ("G", c_int), ("softplus_beta", c_float), ("max_samples_per_node", c_int),
         ("lr_grid", c_float), ("lr_decoder", c_float), ("beta1", c_float), ("beta2", c_float), ("eps", c_float),
-        ("seg_capacity", c_int64), ("decoder_path", c_int),
+        ("seg_capacity", c_int64), ("decoder_path", c_int), ("proposal", c_int),
     ]
+
+
+NEAT_PROPOSAL_OFF, NEAT_PROPOSAL_SAMPLE, NEAT_PROPOSAL_TRAIN = 0, 1, 2
+NEAT_PROPOSAL_IN, NEAT_PROPOSAL_HIDDEN, NEAT_PROPOSAL_BINS = 16, 32, 8
+
+
+class Proposal(ctypes.Structure):
+    _fields_ = [("mode", c_int), ("params", c_void_p), ("m", c_void_p), ("v", c_void_p), ("grad", c_void_p),
+                ("step_counter", c_void_p), ("loss", c_void_p), ("lr", c_float), ("beta1", c_float),
+                ("beta2", c_float), ("eps", c_float), ("mix", c_float), ("iters", c_int), ("node_desc", c_void_p)]
 
 
 class StepState(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("grid", "grid_m", "grid_v", "grid_grad",
-                                        "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter")]
+                                        "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter",
+                                        "proposal")]
 
 
 class StepBatch(ctypes.Structure):
@@ -98,8 +109,9 @@ _SIGS = {
     "neat_train_step_workspace_bytes": (c_size_t, [ctypes.POINTER(StepDesc), c_int64]),
     "neat_train_step": (c_int, [ctypes.POINTER(StepDesc), ctypes.POINTER(StepState), ctypes.POINTER(StepBatch),
                                 c_uint64, c_int, ctypes.POINTER(StepOut), c_void_p, c_size_t, c_void_p]),
-    "neat_project": (c_int, [ctypes.POINTER(StepDesc), c_void_p, c_void_p, ctypes.POINTER(StepBatch),
+    "neat_project": (c_int, [ctypes.POINTER(StepDesc), c_void_p, c_void_p, c_void_p, ctypes.POINTER(StepBatch),
                              ctypes.POINTER(ProjectOut), c_void_p, c_size_t, c_void_p]),
+    "neat_proposal_params": (c_int64, []),
     "neat_sample_volume": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p,
                                    c_float, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_grid_to_channel_last": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),

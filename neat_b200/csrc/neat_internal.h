@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/neat_b200.h"
+
 namespace neat
 {
 
@@ -62,11 +64,26 @@ struct StepTileArgs
     uint64_t seed;
     uint32_t step;
     const int* step_dev;  // when set, the step number is read here (device-side step counter)
+    const float* seg_cdf;  // proposal CDF per node-major segment [8] (null: uniform stratified)
+    float* seg_hist;       // per ray-major segment [8]: contribution mass per sub-interval (null: off)
     int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;
 };
 using StepTcArgs = StepTileArgs;
+
+// Learned proposal (neat_proposal.cu).
+// CDF of every node-major segment (counters[0] of them) from the proposal MLP.
+cudaError_t launch_proposal_cdf(const SegRec* segs, const int64_t* counters, const neat_proposal* pr, float* seg_cdf,
+                                cudaStream_t st);
+// Node descriptors from the current grid (channel-last) and decoder.
+cudaError_t launch_node_desc(const float* grid, int64_t A, int C, int G, const float* decoder, float beta,
+                             float* node_desc, cudaStream_t st);
+// Partials of one training iteration over a subset of the segments (iteration it).
+int proposal_grad_blocks();
+size_t proposal_part_floats();  // workspace floats of the training partials
+cudaError_t launch_proposal_train(const SegRec* segs, const int64_t* counters, const float* seg_hist,
+                                  const neat_proposal* pr, float* part, int iters, cudaStream_t st);
 
 // tcgen05 tile kernels (neat_tc.cu); prec 0 = BF16 operands, 1 = three-piece BF16 split.
 int tc_backward_grid(int C, int prec);

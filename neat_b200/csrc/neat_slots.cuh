@@ -6,6 +6,7 @@
 
 #include "neat_common.cuh"
 #include "neat_internal.h"
+#include "neat_proposal.cuh"
 
 namespace neat
 {
@@ -60,6 +61,7 @@ struct SlotSample
     bool valid;
     float weight;
     float lu, lv, lw;  // local coordinates in [-1,1]
+    float u;           // stratified CDF position (j + a) / n of the sample
     int ray, rm, row;
 };
 
@@ -78,6 +80,7 @@ __device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool v
     q.lv            = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], ts)), r.mn[1], r.mx[1]);
     q.lw            = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], ts)), r.mn[2], r.mx[2]);
     q.weight        = q.valid ? ws : 0.0f;
+    q.u             = 0.0f;
     q.ray           = r.ray;
     q.rm            = r.rm;
     q.row           = r.row;
@@ -88,14 +91,29 @@ __device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool v
 // jitter of its own sample only and takes t of samples j-1 and j+1 from its
 // neighbour lanes (consecutive slots of one segment are consecutive samples);
 // lanes 0 and 31 draw the one neighbour outside the warp when they need it.
-// Same values as slot_sample.  All 32 lanes must call it.
+// Same values as slot_sample when cdf is null; with a proposal CDF (8 bin
+// ends of this slot's segment) the positions come from its inverse.  All 32
+// lanes must call it.
 __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, bool valid, bool jitter, uint64_t seed,
-                                                       uint32_t step)
+                                                       uint32_t step, const float* cdf = nullptr)
 {
     SlotSample q;
     q.valid = valid;
     if (!valid) j = 0;
-    const float t = seg_t(r.tmin, r.step, j, jitter_a(jitter, seed, step, r.ray, r.local_base + j));
+    float c[PBIN];
+    if (cdf)
+    {
+        const float4 c0 = *reinterpret_cast<const float4*>(cdf);
+        const float4 c1 = *reinterpret_cast<const float4*>(cdf + 4);
+        c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+        c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+    }
+    auto t_of = [&](int jj) -> float {
+        const float a = jitter_a(jitter, seed, step, r.ray, r.local_base + jj);
+        return cdf ? proposal_t(r.tmin, r.tmax, r.n, jj, a, c) : seg_t(r.tmin, r.step, jj, a);
+    };
+    const float a = jitter_a(jitter, seed, step, r.ray, r.local_base + j);
+    const float t = cdf ? proposal_t(r.tmin, r.tmax, r.n, j, a, c) : seg_t(r.tmin, r.step, j, a);
     const int lane = threadIdx.x & 31;
     float tp       = __shfl_up_sync(0xffffffffu, t, 1);
     float tn       = __shfl_down_sync(0xffffffffu, t, 1);
@@ -103,8 +121,7 @@ __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, b
     const bool nn  = j < r.n - 1 && lane == 31;
     if (np || nn)
     {
-        const int jj   = np ? j - 1 : j + 1;
-        const float tx = seg_t(r.tmin, r.step, jj, jitter_a(jitter, seed, step, r.ray, r.local_base + jj));
+        const float tx = t_of(np ? j - 1 : j + 1);
         if (np)
             tp = tx;
         else
@@ -116,6 +133,7 @@ __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, b
     q.lv           = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], t)), r.mn[1], r.mx[1]);
     q.lw           = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], t)), r.mn[2], r.mx[2]);
     q.weight       = q.valid ? __fsub_rn(hi, lo) : 0.0f;
+    q.u            = __fdiv_rn(__fadd_rn((float)j, a), (float)r.n);
     q.ray          = r.ray;
     q.rm           = r.rm;
     q.row          = r.row;

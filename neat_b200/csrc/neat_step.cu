@@ -186,6 +186,14 @@ __global__ void k_zero_partial(double* __restrict__ partial, const int64_t* coun
         partial[i] = 0.0;
 }
 
+// Zero n = counters[0] * per floats.
+__global__ void k_zero_per_segment(float* __restrict__ p, const int64_t* counters, int per)
+{
+    const int64_t n = counters[0] * per;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 0.0f;
+}
+
 __global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, const int64_t* counters,
                            int* __restrict__ tile_seg, int64_t tiles_cap)
 {
@@ -407,7 +415,8 @@ struct StepLayout
     enum
     {
         ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
-        SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, NUM
+        SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, SEG_CDF, SEG_HIST,
+        PROP_PART, NUM
     };
     size_t off[NUM];
     size_t total;
@@ -436,7 +445,9 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)(A + 1) * 4, (size_t)R * L.cap_ray * sizeof(SegRec), (size_t)cap * sizeof(SegRec), (size_t)cap * 4,
         (size_t)(cap + 1) * 4,
         (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
-        (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars)};
+        (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars),
+        d->proposal ? (size_t)cap * 8 * 4 : 0, d->proposal ? (size_t)cap * 8 * 4 : 0,
+        d->proposal ? proposal_part_floats() * 4 : 0};
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
     {
@@ -519,6 +530,7 @@ struct StepBufs
     float *dpred, *loss_part, *dec_part;
     int* scratch;
     StepScalars* scal;
+    float *seg_cdf, *seg_hist, *prop_part;
 };
 
 static StepBufs step_bufs(const StepLayout& L, void* workspace)
@@ -544,6 +556,9 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.dec_part     = (float*)P_(StepLayout::DEC_PART);
     w.scratch      = (int*)P_(StepLayout::SCAN_SCRATCH);
     w.scal         = (StepScalars*)P_(StepLayout::SCAL);
+    w.seg_cdf      = (float*)P_(StepLayout::SEG_CDF);
+    w.seg_hist     = (float*)P_(StepLayout::SEG_HIST);
+    w.prop_part    = (float*)P_(StepLayout::PROP_PART);
     return w;
 }
 
@@ -613,6 +628,8 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.seed      = seed;
     ta.step      = (uint32_t)step;
     ta.step_dev  = &w.scal->step;
+    ta.seg_cdf   = nullptr;
+    ta.seg_hist  = nullptr;
     ta.jitter    = jitter;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;
@@ -687,6 +704,18 @@ __global__ void k_err_final(const double* __restrict__ err_part, int nb, double*
     out[1] += a;
 }
 
+// The proposal for this call (null when off); false when it cannot be used.
+static bool proposal_mode(const neat_step_desc* d, const neat_proposal* pr, int& mode)
+{
+    mode = pr ? pr->mode : NEAT_PROPOSAL_OFF;
+    if (mode == NEAT_PROPOSAL_OFF) return true;
+    if (mode != NEAT_PROPOSAL_SAMPLE && mode != NEAT_PROPOSAL_TRAIN) return false;
+    if (!d->proposal || d->decoder_path == NEAT_DECODER_SIMT_FP32 || !pr->params || !pr->node_desc) return false;
+    if (mode == NEAT_PROPOSAL_TRAIN && (!pr->m || !pr->v || !pr->grad || !pr->step_counter || pr->iters < 0))
+        return false;
+    return pr->mix >= 0.0f && pr->mix <= 1.0f;
+}
+
 }  // namespace neat
 
 extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
@@ -700,6 +729,8 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     if (!s->grid || !s->grid_m || !s->grid_v || !s->grid_grad || !s->decoder || !s->decoder_m || !s->decoder_v ||
         !s->decoder_grad || !b->target || !workspace)
         return NEAT_ERR_BAD_INPUT;
+    int pmode = NEAT_PROPOSAL_OFF;
+    if (!proposal_mode(d, s->proposal, pmode)) return NEAT_ERR_BAD_INPUT;
     const int64_t R = b->num_rays;
     StepLayout L;
     if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
@@ -707,6 +738,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     const StepBufs w   = step_bufs(L, workspace);
     int64_t* cnt       = out->counters;
     const int A        = d->num_active;
+    const neat_proposal* pr = s->proposal;
 
     auto phase = [&](int i) {
         if (out->phase_events && out->phase_events[i]) cudaEventRecord((cudaEvent_t)out->phase_events[i], st);
@@ -718,8 +750,19 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ok = build_segments(d, b, L, w, cnt, out->status, st);
     phase(1);
 
-    const StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
+    StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
+    if (pmode == NEAT_PROPOSAL_SAMPLE)
+    {
+        ok         = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;
+        ta.seg_cdf = w.seg_cdf;
+    }
+    else if (pmode == NEAT_PROPOSAL_TRAIN)
+    {
+        k_zero_per_segment<<<sm_count() * 4, 256, 0, st>>>(w.seg_hist, cnt, 8);
+        ta.seg_hist = w.seg_hist;
+    }
     ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
+    ta.seg_hist = nullptr;
     phase(2);
     const float invR = (float)(1.0 / (double)R);
     k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, w.ray_seg_off, w.partial, b->target, w.dpred, out->prediction,
@@ -737,15 +780,24 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
                                   0.0f, 1.0f, 1, w.scal);
+    if (pmode == NEAT_PROPOSAL_TRAIN)
+    {
+        ok = ok && launch_node_desc(s->grid, A, d->C, d->G, s->decoder, d->softplus_beta, pr->node_desc, st) ==
+                       cudaSuccess;
+        ok = ok && launch_proposal_train(w.segs, cnt, w.seg_hist, pr, w.prop_part, pr->iters, st) == cudaSuccess;
+    }
     phase(5);
     ok = ok && cudaGetLastError() == cudaSuccess;
     return ok ? NEAT_OK : NEAT_ERR_CUDA;
 }
 
 extern "C" int neat_project(const neat_step_desc* d, const float* grid, const float* decoder,
-                            const neat_step_batch* b, const neat_project_out* out, void* workspace,
-                            size_t workspace_bytes, neat_stream_t stream)
+                            const neat_proposal* proposal, const neat_step_batch* b, const neat_project_out* out,
+                            void* workspace, size_t workspace_bytes, neat_stream_t stream)
 {
+    int pmode = NEAT_PROPOSAL_OFF;
+    if (d && !proposal_mode(d, proposal, pmode)) return NEAT_ERR_BAD_INPUT;
+    if (pmode == NEAT_PROPOSAL_TRAIN) return NEAT_ERR_BAD_INPUT;
     if (!d || !b || !out || !out->prediction || !out->counters || !out->status || !grid || !decoder || !workspace)
         return NEAT_ERR_BAD_INPUT;
     if (out->error_sums && !b->target) return NEAT_ERR_BAD_INPUT;
@@ -759,7 +811,12 @@ extern "C" int neat_project(const neat_step_desc* d, const float* grid, const fl
     int64_t* cnt     = out->counters;
     k_step_begin<<<1, 32, 0, st>>>(nullptr, 1, 0.0, 0.0, 0.5, 0.5, w.scal);
     bool ok               = build_segments(d, b, L, w, cnt, out->status, st);
-    const StepTileArgs ta = tile_args(d, w, grid, nullptr, decoder, cnt, out->status, 0, 1, 0);
+    StepTileArgs ta = tile_args(d, w, grid, nullptr, decoder, cnt, out->status, 0, 1, 0);
+    if (pmode == NEAT_PROPOSAL_SAMPLE)
+    {
+        ok         = ok && launch_proposal_cdf(w.segs, cnt, proposal, w.seg_cdf, st) == cudaSuccess;
+        ta.seg_cdf = w.seg_cdf;
+    }
     ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
     // the loss-partials slab holds L.loss_blocks floats; the error sums need two
     // doubles per block, which the (larger) dpred slab of R floats provides

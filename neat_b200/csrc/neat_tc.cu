@@ -421,7 +421,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const bool valid = gs < S;
         const SegRec r   = a.segs[seg];
         const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
-        o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no);
+        o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no,
+                                            a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr);
         Corners kc;
         igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
         gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);
@@ -635,7 +636,13 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         if constexpr (!BWD)
         {
             __syncthreads();  // both halves read the y parts before they are overwritten
-            if (h == 0) sval[s] = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
+            if (h == 0)
+            {
+                sval[s] = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
+                // proposal targets: contribution mass per eighth of the segment
+                if (a.seg_hist && q.valid)
+                    atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), sval[s]);
+            }
             __syncthreads();
             if (h == 0 && q.valid)
             {

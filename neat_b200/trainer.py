@@ -14,13 +14,16 @@ import torch
 
 from . import _lib
 from .api import CameraModel, decoder_init, grid_init
+from .proposal import proposal_init
 from .tree import HyperTreeBase
 
 
 class FusedTrainer:
     def __init__(self, tree: HyperTreeBase, camera: CameraModel, num_features=4, grid_size=17,
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
-                 decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda"):
+                 decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
+                 proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
+                 proposal_mix=0.25):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -73,6 +76,32 @@ class FusedTrainer:
         self.ws_rays = 0
         self.step_id = 0
         self._graph = None
+        self._graphs = {}
+        # learned sample proposal: SAMPLE-mode steps place proposal_budget samples per
+        # node segment by the proposal's CDF; every proposal_every-th step (the first
+        # included) samples uniformly with max_samples_per_node, bins the
+        # contributions and trains the proposal on them
+        self.proposal = bool(proposal)
+        self.desc.proposal = 1 if self.proposal else 0
+        if self.proposal:
+            if decoder_path == _lib.NEAT_DECODER_SIMT_FP32:
+                raise ValueError("the learned proposal runs with the tensor-core decoder paths")
+            self.prop = proposal_init(gen).to(self.dev)
+            self.prop_m = torch.zeros_like(self.prop)
+            self.prop_v = torch.zeros_like(self.prop)
+            self.prop_grad = torch.zeros_like(self.prop)
+            self.prop_steps = torch.zeros(1, dtype=torch.int32, device=self.dev)
+            self.prop_loss = torch.zeros(2, dtype=torch.float32, device=self.dev)  # cross-entropy, target entropy
+            self.prop_node_desc = torch.zeros((A, 6), dtype=torch.float32, device=self.dev)
+            self.prop_every = int(proposal_every)
+            self.prop_struct = _lib.Proposal(
+                mode=_lib.NEAT_PROPOSAL_OFF, params=self.prop.data_ptr(), m=self.prop_m.data_ptr(),
+                v=self.prop_v.data_ptr(), grad=self.prop_grad.data_ptr(), step_counter=self.prop_steps.data_ptr(),
+                loss=self.prop_loss.data_ptr(), lr=float(proposal_lr), beta1=0.9, beta2=0.999, eps=1e-8,
+                mix=float(proposal_mix), iters=int(proposal_iters), node_desc=self.prop_node_desc.data_ptr())
+            self.state.proposal = ctypes.addressof(self.prop_struct)
+            self.desc_budget = _lib.StepDesc.from_buffer_copy(self.desc)
+            self.desc_budget.max_samples_per_node = int(proposal_budget)
 
     def _stream(self):
         return torch.cuda.current_stream(self.dev).cuda_stream
@@ -82,6 +111,8 @@ class FusedTrainer:
         if self.ws is not None and num_rays <= self.ws_rays:
             return
         self.desc.seg_capacity = int(num_rays) * self.seg_per_ray
+        if self.proposal:
+            self.desc_budget.seg_capacity = self.desc.seg_capacity
         nbytes = self.lib.neat_train_step_workspace_bytes(ctypes.byref(self.desc), int(num_rays))
         if nbytes == 0:
             raise _lib.NeatError(_lib.NEAT_ERR_UNSUPPORTED, "neat_train_step_workspace_bytes")
@@ -110,7 +141,12 @@ class FusedTrainer:
                            status=self.status.data_ptr(),
                            prediction=prediction.data_ptr() if prediction is not None else None,
                            phase_events=ev)
-        rc = self.lib.neat_train_step(ctypes.byref(self.desc), ctypes.byref(self.state), ctypes.byref(batch),
+        desc = self.desc
+        if self.proposal:
+            train = (self.step_id - 1) % self.prop_every == 0
+            self.prop_struct.mode = _lib.NEAT_PROPOSAL_TRAIN if train else _lib.NEAT_PROPOSAL_SAMPLE
+            desc = self.desc if train else self.desc_budget
+        rc = self.lib.neat_train_step(ctypes.byref(desc), ctypes.byref(self.state), ctypes.byref(batch),
                                       self.seed, self.step_id, ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
                                       self._stream())
         _lib.check(rc, "neat_train_step")
@@ -122,28 +158,36 @@ class FusedTrainer:
         the captured input buffers and replay (one graph launch instead of the
         step's ~20 kernel launches).  Same results as step()."""
         R = uv.shape[0]
-        if self._graph is None or self._graph_rays != R:
-            self._graph = None
+        train = self.proposal and self.step_id % self.prop_every == 0
+        key = (R, train)
+        if getattr(self, "_graph_rays", None) != R:
+            self._graphs = {}
             self.reserve(R)
             self._g_uv = uv.detach().clone().contiguous()
             self._g_img = image_id.detach().clone().contiguous()
             self._g_tgt = target.detach().clone().contiguous()
+            self._graph_rays = R
+        if key not in self._graphs:
+            self._g_uv.copy_(uv)
+            self._g_img.copy_(image_id)
+            self._g_tgt.copy_(target)
             self.step(self._g_uv, self._g_img, self._g_tgt)  # eager: also initialises per-kernel attributes
             torch.cuda.synchronize(self.dev)
             g = torch.cuda.CUDAGraph()
+            self.step_id -= 1
             with torch.cuda.graph(g):
-                self.step(self._g_uv, self._g_img, self._g_tgt)
-            self.step_id -= 1  # capturing does not run the step
-            self._graph, self._graph_rays = g, R
+                self.step(self._g_uv, self._g_img, self._g_tgt)  # captured for this step's mode, not run
+            self._graphs[key] = g
             return self.loss
         self._g_uv.copy_(uv, non_blocking=True)
         self._g_img.copy_(image_id, non_blocking=True)
         self._g_tgt.copy_(target, non_blocking=True)
-        self._graph.replay()
+        self._graphs[key].replay()
         self.step_id += 1
         return self.loss
 
-    def project(self, uv, image_id, target=None, error_sums=None, prediction=None):
+    def project(self, uv, image_id, target=None, error_sums=None, prediction=None, use_proposal=False,
+                samples_per_node=None):
         """Deterministic projection (a = 0.5) of a ray batch with the current
         parameters: the forward of EvalStepProjection
         (samples/reconstruct.cpp:551-559).  error_sums: optional device f64[2]
@@ -159,9 +203,21 @@ class FusedTrainer:
         out = _lib.ProjectOut(prediction=prediction.data_ptr(),
                               error_sums=error_sums.data_ptr() if error_sums is not None else None,
                               counters=self.counters.data_ptr(), status=self.status.data_ptr())
-        rc = self.lib.neat_project(ctypes.byref(self.desc), self.grid.data_ptr(), self.decoder.data_ptr(),
-                                   ctypes.byref(batch), ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
-                                   self._stream())
+        desc = _lib.StepDesc.from_buffer_copy(self.desc)
+        prop = None
+        if use_proposal:
+            if not self.proposal:
+                raise ValueError("this trainer has no proposal")
+            prop = _lib.Proposal.from_buffer_copy(self.prop_struct)
+            prop.mode = _lib.NEAT_PROPOSAL_SAMPLE
+            desc.max_samples_per_node = self.desc_budget.max_samples_per_node
+        if samples_per_node is not None:
+            if samples_per_node > self.desc.max_samples_per_node:
+                raise ValueError("samples_per_node above the workspace's max_samples_per_node")
+            desc.max_samples_per_node = int(samples_per_node)
+        rc = self.lib.neat_project(ctypes.byref(desc), self.grid.data_ptr(), self.decoder.data_ptr(),
+                                   ctypes.byref(prop) if prop is not None else None, ctypes.byref(batch),
+                                   ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(), self._stream())
         _lib.check(rc, "neat_project")
         return prediction
 

@@ -391,3 +391,167 @@ def step_f64(samples, grid_ref, dec, target, node_min, node_max, prefix, beta=2.
     new_dec, dm, dv = adam_f64(d.detach().numpy(), gd, state["dm"], state["dv"], lr_decoder, step)
     return dict(loss=float(loss.detach()), pred=pred.detach().numpy(), grad_grid=gg, grad_dec=gd, grid=new_grid, dec=new_dec,
                 state=dict(gm=gm, gv=gv, dm=dm, dv=dv))
+
+
+# --------------------------------------------------------------------------
+# learned sample proposal (restatement of neat_b200/csrc/neat_proposal.cuh)
+# --------------------------------------------------------------------------
+PROP_IN, PROP_H, PROP_B = 16, 32, 8
+JITTER_STREAM = 0x4a495454
+
+
+def node_descriptors_f64(grid, dec, beta=2.0):
+    """Per active node: the decoded density on the 4^3 lattice at local
+    coordinates (i + 0.5) / 2 - 1 -> [centroid (3), spread, log(mean + 1e-3),
+    log((peak + 1e-3) / (mean + 1e-3))], f64.  grid [A, C, G, G, G]."""
+    import torch
+    g = torch.as_tensor(np.asarray(grid, np.float64))
+    A = g.shape[0]
+    l = np.arange(4) * 0.5 - 0.75
+    z, y, x = np.meshgrid(l, l, l, indexing="ij")
+    pts = np.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], 1)  # thread t: x = t & 3, y = (t >> 2) & 3, z = t >> 4
+    uvw = torch.from_numpy(np.tile(pts, (A, 1)))
+    row = torch.from_numpy(np.repeat(np.arange(A), 64))
+    rho = decoder_f64(torch, _trilinear_f64(torch, g, row, uvw), torch.as_tensor(np.asarray(dec, np.float64)),
+                      g.shape[1], beta).numpy().reshape(A, 64)
+    S = rho.sum(1)
+    mean = S / 64
+    c = np.where(S[:, None] > 1e-12, (rho @ pts) / np.where(S > 1e-12, S, 1.0)[:, None], 0.0)
+    r2 = (rho * (pts ** 2).sum(1)).sum(1)
+    spread = np.where(S > 1e-12, np.sqrt(np.maximum(r2 / np.where(S > 1e-12, S, 1.0) - (c ** 2).sum(1), 0.0)), 0.968246)
+    return np.stack([c[:, 0], c[:, 1], c[:, 2], spread, np.log(mean + 1e-3),
+                     np.log((rho.max(1) + 1e-3) / (mean + 1e-3))], 1)
+
+
+def proposal_features(o, d, segs, pmin, pmax, node_desc, prefix):
+    """[Nseg, 16] f32: the node's descriptor, entry and exit points in
+    node-local coordinates (every op in f32 as the device computes them),
+    chord length over the node edge, three zeros."""
+    r, nd = segs["ray"], segs["node"]
+    mn, mx = pmin[nd].astype(np.float32), pmax[nd].astype(np.float32)
+    oo, dd = o[r].astype(np.float32), d[r].astype(np.float32)
+    t0, t1 = segs["tmin"].astype(np.float32)[:, None], segs["tmax"].astype(np.float32)[:, None]
+    size = mx - mn
+    loc = lambda g: ((g - mn) / size) * np.float32(2) - np.float32(1)
+    f = np.zeros((r.shape[0], PROP_IN), np.float32)
+    f[:, 0:6] = np.asarray(node_desc, np.float32)[prefix[nd]]
+    f[:, 6:9] = loc(oo + dd * t0)
+    f[:, 9:12] = loc(oo + dd * t1)
+    f[:, 12] = (t1[:, 0] - t0[:, 0]) / size[:, 0]
+    e = f[:, 9:12] - f[:, 6:9]
+    cv = f[:, 0:3] - f[:, 6:9]
+    L2 = (e * e).sum(1) + np.float32(1e-12)
+    us = (cv * e).sum(1) / L2
+    p2 = np.maximum((cv * cv).sum(1) - us * us * L2, 0)
+    f[:, 13] = np.clip(us, -0.5, 1.5)
+    f[:, 14] = np.sqrt(p2) / (f[:, 3] + np.float32(0.05))
+    return f
+
+
+def proposal_probs_f64(torch, params, f, mix):
+    """Mixed bin probabilities p = (1 - mix) softmax(MLP(f)) + mix / 8, f64."""
+    H, I, B = PROP_H, PROP_IN, PROP_B
+    W1, b1, W2, b2, W3, b3 = torch.split(params, [H * I, H, H * H, H, B * H, B])
+    x = torch.as_tensor(f, dtype=torch.float64)
+    h1 = torch.nn.functional.silu(x @ W1.reshape(H, I).T + b1)
+    h2 = torch.nn.functional.silu(h1 @ W2.reshape(H, H).T + b2)
+    z = h2 @ W3.reshape(B, H).T + b3
+    return (1 - mix) * torch.softmax(z, 1) + mix / B
+
+
+def proposal_inverse(c, u):
+    """Position in [0,1] of CDF value u under the piecewise-linear CDF with bin
+    ends c[:, 0..7] (c[:, 7] = 1), row-wise."""
+    b = (u[:, None] >= c[:, :PROP_B - 1]).sum(1)
+    lo = np.where(b > 0, np.take_along_axis(c, np.maximum(b - 1, 0)[:, None], 1)[:, 0], 0.0)
+    hi = np.take_along_axis(c, b[:, None], 1)[:, 0]
+    w = hi - lo
+    fr = np.where(w > 0, (u - lo) / np.where(w > 0, w, 1.0), 0.5)
+    return (b + np.clip(fr, 0.0, 1.0)) / PROP_B
+
+
+def sample_offsets(segs, jitter, seed, step):
+    """Per sample of the segments (segment-major, j inside): segment index, j,
+    stratified offset a (Philox jitter stream or 0.5) and u = (j + a) / n in f32."""
+    n = segs["n"].astype(np.int64)
+    sid = np.repeat(np.arange(n.shape[0]), n)
+    start = np.concatenate([[0], np.cumsum(n)[:-1]])
+    j = np.arange(sid.shape[0]) - start[sid]
+    # index in the ray of each segment's first sample (segments are ray-major)
+    first = np.concatenate([[0], np.cumsum(segs["ray_nseg"].astype(np.int64))[:-1]])
+    base = start - start[first[segs["ray"]]]
+    if jitter:
+        a = np.array([uniform(seed, int(segs["ray"][s]), int(base[s] + jj), step, JITTER_STREAM)
+                      for s, jj in zip(sid, j)], np.float32)
+    else:
+        a = np.full(sid.shape[0], 0.5, np.float32)
+    u = (j.astype(np.float32) + a) / n[sid].astype(np.float32)
+    return sid, j, a, u.astype(np.float32)
+
+
+def proposal_samples(o, d, segs, cdf, jitter, seed=0, step=1):
+    """Samples placed by the proposal CDF (one row of bin ends per segment):
+    t = tmin + (tmax - tmin) F^-1((j + a) / n), midpoint-rule weights on the
+    placed positions, f64.  Returns a SampleList-like dict for image_f64."""
+    sid, j, a, u = sample_offsets(segs, jitter, seed, step)
+    t0 = segs["tmin"].astype(np.float64)[sid]
+    t1 = segs["tmax"].astype(np.float64)[sid]
+    n = segs["n"][sid]
+    t = t0 + (t1 - t0) * proposal_inverse(np.asarray(cdf, np.float64)[sid], u.astype(np.float64))
+    tp = np.concatenate([[0.0], t[:-1]])
+    tn = np.concatenate([t[1:], [0.0]])
+    lo = np.where(j == 0, t0, (tp + t) * 0.5)
+    hi = np.where(j == n - 1, t1, (tn + t) * 0.5)
+    r = segs["ray"][sid]
+    coords = o[r].astype(np.float64) + d[r].astype(np.float64) * t[:, None]
+    return dict(coords=coords, weight=hi - lo, ray_index=r.astype(np.int64), node_id=segs["node"][sid].astype(np.int64))
+
+
+def proposal_targets(o, d, segs, M, grid, dec, node_min, node_max, prefix, jitter, seed, step, beta=2.0):
+    """Uniformly sampled contributions density * weight of every sample (f64),
+    binned into eighths of its segment by u = (j + a) / n: [Nseg, 8]."""
+    import torch
+    s = create_samples(o, d, np.nonzero(prefix >= 0)[0], node_min, node_max, M, jitter, seed, step)
+    sid, j, a, u = sample_offsets(segs, jitter, seed, step)
+    assert sid.shape[0] == s["ray_t"].shape[0]
+    g = torch.from_numpy(s["coords"]).double()
+    nid = torch.from_numpy(s["node_id"])
+    mn = torch.from_numpy(node_min).double()[nid]
+    mx = torch.from_numpy(node_max).double()[nid]
+    local = (g - mn) / (mx - mn) * 2 - 1
+    row = torch.from_numpy(prefix[s["node_id"]])
+    grid_t = torch.as_tensor(np.asarray(grid, np.float64))
+    feat = _trilinear_f64(torch, grid_t, row, local)
+    dens = decoder_f64(torch, feat, torch.as_tensor(np.asarray(dec, np.float64)), grid_t.shape[1], beta).numpy()
+    c = dens * s["weight"].astype(np.float64)
+    b = np.minimum(7, (u * np.float32(8)).astype(np.int64))
+    hist = np.zeros((segs["n"].shape[0], PROP_B))
+    np.add.at(hist, (sid, b), c)
+    return hist
+
+
+def proposal_variation_targets(hist):
+    """Binned masses m [Nseg, 8] -> (targets v / sum v with v_b = |m_b - m_b-1|
+    + |m_b+1 - m_b|, total variation sum_b |m_b - m_b-1| as the segment's weight)."""
+    dm = np.abs(np.diff(hist, axis=1))
+    v = np.zeros_like(hist)
+    v[:, 1:] += dm
+    v[:, :-1] += dm
+    tv = dm.sum(1)
+    return v / np.where(tv > 0, 2 * tv, 1.0)[:, None], tv
+
+
+def proposal_grad_f64(params, f, hist, mix):
+    """Cross-entropy between the variation targets of the binned masses and the
+    proposal, averaged over the segments weighted by their total variation,
+    and its gradient w.r.t. the packed parameters (f64)."""
+    import torch
+    qv, tv = proposal_variation_targets(hist)
+    use = tv > 1e-20
+    q = torch.from_numpy(qv[use])
+    m = torch.from_numpy(tv[use])
+    P = torch.tensor(np.asarray(params, np.float64), requires_grad=True)
+    p = proposal_probs_f64(torch, P, f[use], mix)
+    loss = (-(q * torch.log(p)).sum(1) * m).sum() / m.sum()
+    loss.backward()
+    return float(loss.detach()), P.grad.numpy()

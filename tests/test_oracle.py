@@ -300,3 +300,32 @@ def test_volume_descent_face_ties(oracle):
     assert 9 <= n[0] <= 16 and (t.node_position_max[n[0]][0] == 0.0)
     pos = oracle.volume_positions(3, 2, 2)
     np.testing.assert_array_equal(pos[:4], np.array([[-1, -1, -1], [0, -1, -1], [1, -1, -1], [-1, 1, -1]], np.float32))
+
+
+def test_proposal_inverse_cdf(oracle):
+    """Inverse of the piecewise-linear proposal CDF: uniform bins give the
+    identity, a bin holding 40% of the mass is sampled 40% of the time."""
+    u = np.linspace(0, 0.999, 50)
+    uni = np.tile(np.arange(1, 9) / 8.0, (50, 1))
+    np.testing.assert_allclose(oracle.proposal_inverse(uni, u), u, atol=1e-12)
+    c = np.tile(np.array([0.05, 0.1, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0]), (3, 1))
+    s = oracle.proposal_inverse(c, np.array([0.1, 0.3, 0.5 - 1e-12]))
+    np.testing.assert_allclose(s, [2 / 8, 2.5 / 8, 3 / 8], atol=1e-9)
+
+
+def test_proposal_gradient_matches_finite_differences(oracle):
+    """The f64 cross-entropy gradient of the proposal (the oracle the GPU
+    training kernel is checked against) matches central differences."""
+    import torch
+    rng = np.random.default_rng(4)
+    P = rng.normal(0, 0.3, 1864)
+    f = rng.uniform(-1, 1, (40, 16)).astype(np.float32)
+    f[:, 13:] = 0
+    hist = rng.uniform(0, 1, (40, 8)) * (rng.uniform(0, 1, (40, 1)) > 0.2)
+    loss, g = oracle.proposal_grad_f64(P, f, hist, 0.1)
+    for k in rng.choice(1864, 25, replace=False):
+        e = np.zeros_like(P)
+        e[k] = 1e-6
+        lp, _ = oracle.proposal_grad_f64(P + e, f, hist, 0.1)
+        lm, _ = oracle.proposal_grad_f64(P - e, f, hist, 0.1)
+        assert abs((lp - lm) / 2e-6 - g[k]) <= 1e-6 + 1e-5 * abs(g[k])

@@ -242,6 +242,105 @@ def time_to_psnr(dev, decoders, target_db=PSNR_TARGET_DB, max_steps=3000, every=
 
 
 # --------------------------------------------------------------------------
+# variants of the step at the full-size workload
+# --------------------------------------------------------------------------
+def step_variants(cfg, scene, tree, cam, dev, steps=50):
+    """rays/s of the plain FP32 SIMT step, the BF16 step and the BF16 step with
+    the learned proposal (12 samples per segment; one full 50-step cycle, its
+    uniform TRAIN step included), CUDA events around each timed loop."""
+    from neat_b200 import _lib
+    from neat_b200.trainer import FusedTrainer
+    R = cfg["R"]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(4242)
+    batches = [scene.sample_batch(R, gen) for _ in range(steps)]
+    out = {}
+    for name, path, prop in (("fp32_simt", _lib.NEAT_DECODER_SIMT_FP32, False),
+                             ("bf16", _lib.NEAT_DECODER_TC_BF16, False),
+                             ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
+        tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
+                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50)
+        tr.reserve(R)
+        k = steps if prop else 10
+        for i in range(3 if not prop else 0):
+            tr.step(*batches[i])
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(k):
+            tr.step(*batches[i])
+        e1.record()
+        torch.cuda.synchronize()
+        tr.check_status()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"rays_per_s": R * k / (ms / 1000.0), "ms_per_step": ms / k, "steps": k,
+                     "samples_last_step": int(tr.counters[1].item())}
+        del tr
+        torch.cuda.empty_cache()
+    out["bf16_proposal12_vs_fp32_simt"] = out["bf16_proposal12"]["rays_per_s"] / out["fp32_simt"]["rays_per_s"]
+    return out
+
+
+def volume_psnr_race(cfg, scene, tree, cam, dev, steps, n_eval=20, vol_n=256):
+    """Plain method (FP32-accurate decoder, uniform 32 samples) for `steps`
+    steps, then BF16 + learned proposal (12 samples) until it reaches the plain
+    method's final volume PSNR within 0.1 dB.  Volume PSNR = 10 log10(peak^2 /
+    MSE) over the vol_n^3 voxel-corner lattice against the phantom density,
+    peak = the phantom's maximum, MSE in f64.  Wall clock = CUDA-event time of
+    the training steps (evaluations excluded)."""
+    from neat_b200 import _lib
+    from neat_b200.trainer import FusedTrainer
+    gt = scene.density_volume(vol_n)
+    peak2 = float(gt.max()) ** 2
+    R = cfg["R"]
+
+    def vpsnr(tr):
+        vol, _, _ = tr.UniformSampledVolume((vol_n, vol_n, vol_n))
+        mse = float(((vol[0].double() - gt) ** 2).mean())
+        return 10.0 * np.log10(peak2 / mse)
+
+    res = {}
+    target = None
+    for name, path, prop in (("plain_fp32", _lib.NEAT_DECODER_TC_BF16X3, False),
+                             ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
+        tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
+                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50)
+        tr.reserve(R)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(777)
+        every = max(1, steps // n_eval)
+        ms, curve, k, reached_ms = 0.0, [], 0, None
+        while k < steps:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            bs = [scene.sample_batch(R, gen) for _ in range(every)]
+            e0.record()
+            for b in bs:
+                tr.step(*b)
+            e1.record()
+            torch.cuda.synchronize()
+            k += every
+            ms += e0.elapsed_time(e1)
+            p = vpsnr(tr)
+            curve.append([k, round(ms, 1), round(p, 3)])
+            if target is not None and reached_ms is None and p >= target - 0.1:
+                reached_ms = ms
+                break
+        tr.check_status()
+        res[name] = {"steps": k, "train_ms": ms, "volume_psnr_db": curve[-1][2], "curve": curve}
+        if target is None:
+            target = curve[-1][2]
+        else:
+            res[name]["reached_plain_minus_0.1dB_at_ms"] = reached_ms
+        del tr
+        torch.cuda.empty_cache()
+    res["definition"] = ("volume PSNR = 10 log10(peak^2 / MSE), %d^3 voxel-corner lattice vs the phantom density, "
+                         "f64" % vol_n)
+    return res
+
+
+# --------------------------------------------------------------------------
 # main
 # --------------------------------------------------------------------------
 def main():
@@ -253,6 +352,9 @@ def main():
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-psnr", action="store_true", help="skip the time-to-PSNR leg")
+    ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / BF16 / BF16+proposal step variants")
+    ap.add_argument("--volume-psnr", type=int, default=0,
+                    help="also race plain vs BF16+proposal to the plain method's volume PSNR over this many steps")
     ap.add_argument("--rays", type=int, default=0, help="override rays per batch (profiling runs only)")
     ap.add_argument("--decoder", default="bf16x3", choices=["simt", "bf16x3", "bf16"],
                     help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16")
@@ -396,6 +498,12 @@ def main():
     ttp = None
     if not args.no_psnr:
         ttp = time_to_psnr(dev, ["simt", "bf16x3", "bf16"])
+    variants = None
+    if not args.no_variants:
+        variants = step_variants(cfg, scene, tree, cam, dev)
+    vrace = None
+    if args.volume_psnr:
+        vrace = volume_psnr_race(cfg, scene, tree, cam, dev, args.volume_psnr)
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0, min_s=12.0)
@@ -426,6 +534,8 @@ def main():
         "clocks": clock_info,
         "cpu_baseline": cpu_base,
         "time_to_psnr": ttp,
+        "variants": variants,
+        "volume_psnr_race": vrace,
     }
     print(json.dumps(line))
 

@@ -172,6 +172,21 @@ class SyntheticScene:
                                           torch.cuda.current_stream(self.device).cuda_stream), "neat_synth_density")
         return out.cpu().numpy()
 
+    def density_volume(self, n):
+        """Phantom density on the n^3 voxel-corner lattice of [-1,1]^3 (the
+        positions of UniformSampledVolume: (c / (n-1)) * 2 - 1), f64 on the
+        device, [n (z), n (y), n (x)]."""
+        lib = _lib.load()
+        dev = self.device
+        obj = torch.from_numpy(self.objects).to(dev)
+        lin = torch.arange(n, dtype=torch.float64, device=dev) / (n - 1) * 2 - 1
+        z, y, x = torch.meshgrid(lin, lin, lin, indexing="ij")
+        pts = torch.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], 1).contiguous()
+        out = torch.empty(pts.shape[0], dtype=torch.float64, device=dev)
+        _lib.check(lib.neat_synth_density(obj.data_ptr(), obj.shape[0], pts.data_ptr(), pts.shape[0], out.data_ptr(),
+                                          torch.cuda.current_stream(dev).cuda_stream), "neat_synth_density")
+        return out.reshape(n, n, n)
+
     def sample_batch(self, num_rays, generator, device=None, images=None):
         """uv [R,2] f32, image_id [R] i32, target [R] f32 (a1 of the hot path):
         uniform image (from `images`, the training split, when given), uniform

@@ -139,15 +139,16 @@ __device__ __forceinline__ void proposal_cdf(const float p[PBIN], float c[PBIN])
 __device__ __forceinline__ float proposal_inverse(const float c[PBIN], float u)
 {
     int b    = 0;
-    float lo = 0.0f;
+    float lo = 0.0f, hi = c[0];  // selected with constant indices: c stays in registers
 #pragma unroll
     for (int i = 0; i < PBIN - 1; ++i)
         if (u >= c[i])
         {
             b  = i + 1;
             lo = c[i];
+            hi = c[i + 1];
         }
-    const float w = __fsub_rn(c[b], lo);
+    const float w = __fsub_rn(hi, lo);
     float fr      = w > 0.0f ? __fdiv_rn(__fsub_rn(u, lo), w) : 0.5f;
     fr            = fminf(fmaxf(fr, 0.0f), 1.0f);
     return __fmul_rn(__fadd_rn((float)b, fr), 1.0f / PBIN);

@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     {
         SlotSample q;
         float x[C];
+        float dvw;  // backward: dL/dpred of the sample's ray times its weight (0 when invalid)
     };
     auto stage_b = [&](int64_t tl, int b) -> Slot {
         Slot o;
@@ -429,11 +430,12 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         if (!valid)
 #pragma unroll
             for (int c = 0; c < C; ++c) o.x[c] = 0.0f;
+        o.dvw = (BWD && valid) ? a.dpred[o.q.ray] * o.q.weight : 0.0f;
         return o;
     };
     // Row s of an [x | 1 | 0 ..] block: the separate buffer b (b >= 0) or the
     // columns [64, 64 + K1) of HB (b < 0).
-    auto put_x1 = [&](const float* xv, int b) {
+    auto put_x1 = [&](const float (&xv)[C], int b) {
         unsigned char* base = b >= 0 ? sm + K::OFF_X1 + b * K::X1SZ : pHB;
         const int pbytes    = b >= 0 ? X1::BYTES : HB::BYTES;
 #pragma unroll
@@ -444,22 +446,22 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             for (int i = 0; i < P::E; ++i)
             {
                 const int c = cc + i;
-                v[i]        = (c < C) ? xv[c] : ((c == K::ONE) ? 1.0f : 0.0f);
+                v[i]        = (c < C) ? xv[c < C ? c : 0] : ((c == K::ONE) ? 1.0f : 0.0f);
             }
             store_chunk<PREC>(base, pbytes, b >= 0 ? X1::off(s, cc) : HB::off(s, HH + cc), v);
         }
     };
     // Slot data the second thread of a sample needs (backward), into buffer qb.
-    auto put_q = [&](const SlotSample& qq, int qb) {
+    auto put_q = [&](const Slot& sl, int qb) {
         if constexpr (K::NQ > 0)
         {
             float* qd       = sq + qb * 6 * 128;
-            qd[0 * 128 + s] = qq.lu;
-            qd[1 * 128 + s] = qq.lv;
-            qd[2 * 128 + s] = qq.lw;
-            qd[3 * 128 + s] = qq.valid ? qq.weight : 0.0f;
-            qd[4 * 128 + s] = __int_as_float(qq.valid ? qq.ray : -1);
-            qd[5 * 128 + s] = __int_as_float(qq.row);
+            qd[0 * 128 + s] = sl.q.lu;
+            qd[1 * 128 + s] = sl.q.lv;
+            qd[2 * 128 + s] = sl.q.lw;
+            qd[3 * 128 + s] = sl.dvw;
+            qd[4 * 128 + s] = __int_as_float(sl.q.valid ? sl.q.ray : -1);
+            qd[5 * 128 + s] = __int_as_float(sl.q.row);
         }
     };
     // layer 1 from the separate buffer b (pipelined) or from HB's [x | 1] columns
@@ -519,6 +521,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 
     Slot cur;
     cur.q.valid = false;
+    cur.dvw     = 0.0f;
 #pragma unroll
     for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
     if (blockIdx.x < ntiles)
@@ -530,7 +533,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (h == 0)
             {
                 put_x1(cur.x, 0);
-                put_q(cur.q, 0);
+                put_q(cur, 0);
             }
             fence_smem_async();
             fence_before();
@@ -553,6 +556,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const SlotSample& q = cur.q;
         Slot nx;
         nx.q.valid = false;
+        nx.dvw     = 0.0f;
         // ---- previous tile: dX and weight gradients done -> scatter dX
         if (BWD && wg_pending)
         {
@@ -570,7 +574,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (h == 0)
             {
                 put_x1(cur.x, -1);
-                put_q(cur.q, buf);
+                put_q(cur, buf);
             }
             fence_smem_async();
             fence_before();
@@ -658,21 +662,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         }
         else
         {
-            float wgt;
-            int ray;
-            if (h == 0)
-            {
-                wgt = q.valid ? q.weight : 0.0f;
-                ray = q.valid ? q.ray : -1;
-            }
-            else
-            {
-                const float* qd = sq + buf * 6 * 128;
-                wgt             = qd[3 * 128 + s];
-                ray             = __float_as_int(qd[4 * 128 + s]);
-            }
-            const float dv = ray >= 0 ? a.dpred[ray] : 0.0f;
-            const float dy = dv * wgt * softplus_grad(y, a.beta);
+            const float dvw = h == 0 ? cur.dvw : sq[buf * 6 * 128 + 3 * 128 + s];
+            const float dy  = dvw * softplus_grad(y, a.beta);
             if (h == 0) db3 += dy;
             // dz2 (this thread's columns) -> AB[:, c0 ..]; dW3 += h2 dy
 #pragma unroll
@@ -712,7 +703,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 if constexpr (PIPE)
                 {
                     put_x1(nx.x, xb ^ 1);
-                    put_q(nx.q, buf ^ 1);
+                    put_q(nx, buf ^ 1);
                 }
             }
             if (!wait_on(mbar, phase))

@@ -522,3 +522,50 @@ def test_proposal_gain_over_uniform(neat, oracle, case):
           "| projection error vs dense f64: proposal", np.abs(p_prop - ref).mean(), "uniform",
           np.abs(p_unif - ref).mean())
     assert ce < np.log(8) - 0.02
+
+
+# ---------------------------------------------------------------- finite differences
+def test_backward_matches_central_differences(neat, oracle):
+    """Config-5 style gradient check: the fused step's analytic gradients
+    (C = 16, FP32-accurate tensor-core path) on 1000 random parameters -- 900
+    grid entries the batch touches and 100 decoder weights -- against central
+    differences (eps 1e-4) of the f64 loss on the same samples."""
+    c = cfg1_case(R=384, seed=11, depth=3, C=16, G=9, M=16, oracle=oracle, adaptive=120)
+    tr = _trainer(c, "bf16x3")
+    tr.step(_dev(c.uv), _dev(c.img), _dev(c.target))
+    torch.cuda.synchronize()
+    tr.check_status()
+    g_grid = tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1  # m = (1 - b1) g
+    g_dec = tr.decoder_grad.cpu().numpy().astype(np.float64)
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                              seed=99, step=1)
+    tgt = torch.from_numpy(c.target.astype(np.float64))
+
+    def loss(grid, dec):
+        pred = oracle.image_f64(s, torch.from_numpy(grid), torch.from_numpy(dec), T.node_position_min,
+                                T.node_position_max, T.node_active_prefix_sum, c.R)
+        return float(((pred - tgt) ** 2).mean())
+
+    rng = np.random.default_rng(12)
+    grid0, dec0 = c.grid.astype(np.float64), c.dec.astype(np.float64)
+    touched = np.flatnonzero(np.abs(g_grid) > 1e-12 * np.abs(g_grid).max())
+    gi = rng.choice(touched, 900, replace=False)
+    di = rng.choice(dec0.size, 100, replace=False)
+    eps = 1e-4
+    fd, an = [], []
+    for arr, idx, ana in ((grid0, gi, g_grid), (dec0, di, g_dec)):
+        for k in idx:  # perturb in place, restore after
+            v = arr.flat[k]
+            arr.flat[k] = v + eps
+            lp = loss(grid0, dec0)
+            arr.flat[k] = v - eps
+            lm = loss(grid0, dec0)
+            arr.flat[k] = v
+            fd.append((lp - lm) / (2 * eps))
+            an.append(ana.flat[k])
+    fd, an = np.array(fd), np.array(an)
+    err = _rel2(an, fd)
+    print("finite differences vs analytic (1000 params): rel 2-norm err", err)
+    assert err < 1e-4

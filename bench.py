@@ -245,9 +245,10 @@ def time_to_psnr(dev, decoders, target_db=PSNR_TARGET_DB, max_steps=3000, every=
 # variants of the step at the full-size workload
 # --------------------------------------------------------------------------
 def step_variants(cfg, scene, tree, cam, dev, steps=50):
-    """rays/s of the plain FP32 SIMT step, the BF16 step and the BF16 step with
-    the learned proposal (12 samples per segment; one full 50-step cycle, its
-    uniform TRAIN step included), CUDA events around each timed loop."""
+    """rays/s of the plain FP32 SIMT step, the BF16 step (BF16 grid copy and
+    decoder operands, FP32 accumulation) and the BF16 step with the learned
+    proposal (12 samples per segment; one full 50-step cycle, its uniform
+    TRAIN step included), CUDA events around each timed loop."""
     from neat_b200 import _lib
     from neat_b200.trainer import FusedTrainer
     R = cfg["R"]
@@ -259,7 +260,8 @@ def step_variants(cfg, scene, tree, cam, dev, steps=50):
                              ("bf16", _lib.NEAT_DECODER_TC_BF16, False),
                              ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
         tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
-                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50)
+                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50,
+                          grid_bf16=path == _lib.NEAT_DECODER_TC_BF16)
         tr.reserve(R)
         k = steps if prop else 10
         for i in range(3 if not prop else 0):
@@ -305,7 +307,8 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, n_eval=20, vol_n=256):
     for name, path, prop in (("plain_fp32", _lib.NEAT_DECODER_TC_BF16X3, False),
                              ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
         tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
-                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50)
+                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50,
+                          grid_bf16=prop)
         tr.reserve(R)
         gen = torch.Generator(device=dev)
         gen.manual_seed(777)

@@ -298,6 +298,12 @@ typedef struct
     int* step_counter;
     /* optional learned proposal (requires desc->proposal != 0); NULL: off */
     const neat_proposal* proposal;
+    /* optional BF16 copy of the grid ([A, G,G,G, C] bf16, 16-byte aligned):
+     * when set, the sample gathers read it (the precision variant: BF16
+     * feature grids, FP32 accumulation) and Adam refreshes it from the FP32
+     * master after every update; gradients stay FP32.  Requires a tensor-core
+     * decoder path. */
+    uint16_t* grid_bf16;
 } neat_step_state;
 
 typedef struct

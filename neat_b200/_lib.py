@@ -58,7 +58,7 @@ class Proposal(ctypes.Structure):
 class StepState(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("grid", "grid_m", "grid_v", "grid_grad",
                                         "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter",
-                                        "proposal")]
+                                        "proposal", "grid_bf16")]
 
 
 class StepBatch(ctypes.Structure):

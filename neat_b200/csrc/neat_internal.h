@@ -55,6 +55,7 @@ struct StepTileArgs
     const float* node_min;
     const float* node_max;
     const float* grid;
+    const uint16_t* grid_bf16;  // when set: BF16 copy of the grid the gathers read
     float* grid_grad;
     const float* decoder;
     float* dec_part;

@@ -13,6 +13,8 @@
 //   6 loss          per ray: sum of its segments in tmin order, MSE, dL/dpred
 //   7 backward      same tiles: recompute, decoder backward, grid scatter
 //   8 Adam          decoder (deterministic reduce of per-CTA partials), grid
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -309,9 +311,16 @@ __global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, in
     v[i] = vi;
 }
 
+__device__ __forceinline__ uint16_t bf16_rn(float x)
+{
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    return *reinterpret_cast<const uint16_t*>(&b);
+}
+
+// p_bf16 (optional): BF16 copy of the updated parameters, written alongside.
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
                        int64_t n, float b1, float b2, float eps, float step_size, float sqrt_bc2, int zero_grad,
-                       const StepScalars* __restrict__ sc)
+                       const StepScalars* __restrict__ sc, uint16_t* __restrict__ p_bf16 = nullptr)
 {
     if (sc)
     {
@@ -334,6 +343,10 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ grad, float* _
         reinterpret_cast<float4*>(m)[i] = mm;
         reinterpret_cast<float4*>(v)[i] = vv;
         if (zero_grad) reinterpret_cast<float4*>(grad)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p_bf16)
+            reinterpret_cast<uint2*>(p_bf16)[i] =
+                make_uint2((uint32_t)bf16_rn(pp.x) | ((uint32_t)bf16_rn(pp.y) << 16),
+                           (uint32_t)bf16_rn(pp.z) | ((uint32_t)bf16_rn(pp.w) << 16));
     }
     for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     {
@@ -343,6 +356,7 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ grad, float* _
         m[i] = mi;
         v[i] = vi;
         if (zero_grad) grad[i] = 0.0f;
+        if (p_bf16) p_bf16[i] = bf16_rn(pi);
     }
 }
 
@@ -619,6 +633,7 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.node_min  = d->node_min;
     ta.node_max  = d->node_max;
     ta.grid      = grid;
+    ta.grid_bf16 = nullptr;
     ta.grid_grad = grid_grad;
     ta.decoder   = decoder;
     ta.dec_part  = w.dec_part;
@@ -731,6 +746,8 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
         return NEAT_ERR_BAD_INPUT;
     int pmode = NEAT_PROPOSAL_OFF;
     if (!proposal_mode(d, s->proposal, pmode)) return NEAT_ERR_BAD_INPUT;
+    if (s->grid_bf16 && (d->decoder_path == NEAT_DECODER_SIMT_FP32 || ((uintptr_t)s->grid_bf16 & 15)))
+        return NEAT_ERR_BAD_INPUT;
     const int64_t R = b->num_rays;
     StepLayout L;
     if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
@@ -751,6 +768,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     phase(1);
 
     StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
+    ta.grid_bf16    = s->grid_bf16;
     if (pmode == NEAT_PROPOSAL_SAMPLE)
     {
         ok         = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;
@@ -779,7 +797,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;
     const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
-                                  0.0f, 1.0f, 1, w.scal);
+                                  0.0f, 1.0f, 1, w.scal, s->grid_bf16);
     if (pmode == NEAT_PROPOSAL_TRAIN)
     {
         ok = ok && launch_node_desc(s->grid, A, d->C, d->G, s->decoder, d->softplus_beta, pr->node_desc, st) ==

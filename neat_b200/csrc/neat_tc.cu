@@ -426,7 +426,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                                             a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr);
         Corners kc;
         igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
-        gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);
+        if (a.grid_bf16)
+            gather_cl_bf16<C>(a.grid_bf16, o.q.row, a.G, kc, o.x);
+        else
+            gather_cl<C>(a.grid, o.q.row, a.G, kc, o.x);
         if (!valid)
 #pragma unroll
             for (int c = 0; c < C; ++c) o.x[c] = 0.0f;

@@ -422,6 +422,43 @@ __device__ __forceinline__ void gather_cl(const float* __restrict__ grid, int64_
     }
 }
 
+// BF16 channel-last copy of the grid: one corner is C bf16 (C = 8: one
+// 16-byte load); widened to f32, FP32 accumulation.
+template <int C>
+__device__ __forceinline__ void gather_cl_bf16(const uint16_t* __restrict__ grid, int64_t row, int G, const Corners& k,
+                                               float x[C])
+{
+    const int64_t base = row * (int64_t)G * G * G;
+#pragma unroll
+    for (int c = 0; c < C; ++c) x[c] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        const uint16_t* p = grid + (base + corner_cell(k, q, G, G)) * C;
+        const float wq    = k.w[q];
+        if constexpr (C % 8 == 0)
+        {
+#pragma unroll
+            for (int c8 = 0; c8 < C / 8; ++c8)
+            {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(p) + c8);
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                {
+                    x[8 * c8 + 2 * i]     = fmaf(__uint_as_float(w[i] << 16), wq, x[8 * c8 + 2 * i]);
+                    x[8 * c8 + 2 * i + 1] = fmaf(__uint_as_float(w[i] & 0xFFFF0000u), wq, x[8 * c8 + 2 * i + 1]);
+                }
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < C; ++c) x[c] = fmaf(__uint_as_float((uint32_t)__ldg(p + c) << 16), wq, x[c]);
+        }
+    }
+}
+
 __device__ __forceinline__ void red_add_v4(float* addr, float a, float b, float c, float d)
 {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)

@@ -23,7 +23,7 @@ class FusedTrainer:
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
-                 proposal_mix=0.25):
+                 proposal_mix=0.25, grid_bf16=False):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -77,6 +77,14 @@ class FusedTrainer:
         self.step_id = 0
         self._graph = None
         self._graphs = {}
+        # precision variant: the sample gathers read a BF16 copy of the grid that
+        # Adam refreshes from the FP32 master after every update
+        self.grid_bf16 = None
+        if grid_bf16:
+            if decoder_path == _lib.NEAT_DECODER_SIMT_FP32:
+                raise ValueError("BF16 grids run with the tensor-core decoder paths")
+            self.grid_bf16 = self.grid.to(torch.bfloat16).contiguous()
+            self.state.grid_bf16 = self.grid_bf16.data_ptr()
         # learned sample proposal: SAMPLE-mode steps place proposal_budget samples per
         # node segment by the proposal's CDF; every proposal_every-th step (the first
         # included) samples uniformly with max_samples_per_node, bins the

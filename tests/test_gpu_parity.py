@@ -569,3 +569,34 @@ def test_backward_matches_central_differences(neat, oracle):
     err = _rel2(an, fd)
     print("finite differences vs analytic (1000 params): rel 2-norm err", err)
     assert err < 1e-4
+
+
+# ---------------------------------------------------------------- precision variant (BF16 grids)
+@pytest.mark.parametrize("which", ["cfg1", "c8"])
+def test_bf16_grid_step_error_vs_f64(neat, oracle, case, c8_case, which):
+    """Config-3 precision variant: BF16 feature grid copy read by the gathers,
+    BF16 decoder operands, FP32 accumulation, f64 segment sums.  Projection and
+    gradients against the f64 evaluation of the same FP32 parameters within the
+    stated BF16 bounds (1e-2 projection, 5e-2 gradients); after the update the
+    BF16 copy equals the rounded FP32 master."""
+    from neat_b200.trainer import FusedTrainer
+    c = {"cfg1": case, "c8": c8_case}[which]
+    tr = FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
+                      grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec),
+                      decoder_path=PATHS["bf16"][0], grid_bf16=True)
+    pred = torch.zeros(c.R, device="cuda")
+    tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
+    torch.cuda.synchronize()
+    tr.check_status()
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                                  seed=99, step=1)
+    ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                          T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
+    e_pred = _rel2(pred.cpu().numpy(), ref["pred"])
+    e_dec = _rel2(tr.decoder_grad.cpu().numpy(), ref["grad_dec"])
+    e_grid = _rel2(tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1, ref["grad_grid"])
+    print(which, "BF16 grid + BF16 decoder vs f64: projection", e_pred, "grad decoder", e_dec, "grad grid", e_grid)
+    assert e_pred < 1e-2 and e_dec < 5e-2 and e_grid < 5e-2
+    assert torch.equal(tr.grid_bf16, tr.grid.to(torch.bfloat16))

@@ -286,7 +286,9 @@ typedef struct
     float* grid;       /* [A, G,G,G, C] channel-last */
     float* grid_m;     /* Adam first moment, same shape */
     float* grid_v;     /* Adam second moment */
-    float* grid_grad;  /* gradient scratch, same shape; zero on entry, left zero */
+    float* grid_grad;  /* gradient accumulator, same shape: zero on entry, or holding terms to add
+                        * (e.g. the regularisers'); the step adds its own, Adam applies the sum
+                        * and the step leaves it zero */
     float* decoder;    /* neat_decoder_params(C) */
     float* decoder_m;
     float* decoder_v;
@@ -359,6 +361,29 @@ typedef struct
 int neat_project(const neat_step_desc* desc, const float* grid, const float* decoder, const neat_proposal* proposal,
                  const neat_step_batch* batch, const neat_project_out* out, void* workspace, size_t workspace_bytes,
                  neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
+/* Volume regularisers (GeometryExEx::VolumeRegularizer,                    */
+/* src/geometry/geometry_ex_ex.cpp:86-156).  Both ADD their gradient into   */
+/* grid_grad (channel-last, may be NULL) and their loss into *loss (device  */
+/* f32): run them on the step's stream right before neat_train_step, whose  */
+/* Adam applies the summed gradient.  workspace:                             */
+/* neat_regularizer_workspace_bytes() bytes.                                 */
+/* TV (TVLoss, geometry_ex_ex.h:18-58): weight * C * sum over the 3 grid     */
+/* axes of mean_node mean_{c,cells} |neighbour difference|.                  */
+/* Edge (NodeNeighborSamples, src/structure/HyperTree.cu:830-928): on each  */
+/* face of each active node a G x G lattice of points; where the point      */
+/* moved by epsilon outwards lies in another active node, the pair's error  */
+/* is mean_c |f_node - f_other| * r, r uniform in [0,1) (Philox keyed on    */
+/* (node, face point, step) with seed; torch::rand_like in the reference);  */
+/* loss = weight * C * mean over pairs.                                      */
+/* ----------------------------------------------------------------------- */
+size_t neat_regularizer_workspace_bytes(void);
+int neat_tv_loss(const float* grid, int64_t A, int C, int G, float weight, float* loss, float* grid_grad,
+                 void* workspace, neat_stream_t stream);
+int neat_edge_loss(const void* tree_table, int max_depth, const float* node_min, const float* node_max,
+                   const int64_t* active_ids, int64_t A, const float* grid, int C, int G, float epsilon, float weight,
+                   uint64_t seed, uint32_t step, float* loss, float* grid_grad, void* workspace, neat_stream_t stream);
 
 /* ----------------------------------------------------------------------- */
 /* Volume export.                                                            */

@@ -112,6 +112,10 @@ _SIGS = {
     "neat_project": (c_int, [ctypes.POINTER(StepDesc), c_void_p, c_void_p, c_void_p, ctypes.POINTER(StepBatch),
                              ctypes.POINTER(ProjectOut), c_void_p, c_size_t, c_void_p]),
     "neat_proposal_params": (c_int64, []),
+    "neat_regularizer_workspace_bytes": (c_size_t, []),
+    "neat_tv_loss": (c_int, [c_void_p, c_int64, c_int, c_int, c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "neat_edge_loss": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int, c_int,
+                               c_float, c_float, c_uint64, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_sample_volume": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p,
                                    c_float, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_grid_to_channel_last": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),

@@ -23,7 +23,7 @@ class FusedTrainer:
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
-                 proposal_mix=0.25, grid_bf16=False):
+                 proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -77,6 +77,11 @@ class FusedTrainer:
         self.step_id = 0
         self._graph = None
         self._graphs = {}
+        # volume regularisers (GeometryExEx::VolumeRegularizer): their gradients go into
+        # grid_grad before the step, whose Adam applies the sum
+        self.loss_tv, self.loss_edge, self.edge_epsilon = float(loss_tv), float(loss_edge), float(edge_epsilon)
+        self.reg_loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
+        self.reg_ws = torch.empty(lib.neat_regularizer_workspace_bytes(), dtype=torch.uint8, device=self.dev)
         # precision variant: the sample gathers read a BF16 copy of the grid that
         # Adam refreshes from the FP32 master after every update
         self.grid_bf16 = None
@@ -149,6 +154,8 @@ class FusedTrainer:
                            status=self.status.data_ptr(),
                            prediction=prediction.data_ptr() if prediction is not None else None,
                            phase_events=ev)
+        if self.loss_tv > 0 or self.loss_edge > 0:
+            self.regularize()
         desc = self.desc
         if self.proposal:
             train = (self.step_id - 1) % self.prop_every == 0
@@ -159,6 +166,25 @@ class FusedTrainer:
                                       self._stream())
         _lib.check(rc, "neat_train_step")
         return self.loss
+
+    def regularize(self):
+        """VolumeRegularizer (src/geometry/geometry_ex_ex.cpp:86-156): TV and edge
+        losses into self.reg_loss, their gradients into grid_grad."""
+        self.reg_loss.zero_()
+        st = self._stream()
+        if self.loss_tv > 0:
+            _lib.check(self.lib.neat_tv_loss(self.grid.data_ptr(), self.A, self.C, self.G, self.loss_tv,
+                                             self.reg_loss.data_ptr(), self.grid_grad.data_ptr(),
+                                             self.reg_ws.data_ptr(), st), "neat_tv_loss")
+        if self.loss_edge > 0:
+            t = self.tables
+            _lib.check(self.lib.neat_edge_loss(t["table"].data_ptr(), self.tree.max_depth, t["min"].data_ptr(),
+                                               t["max"].data_ptr(), t["active"].data_ptr(), self.A,
+                                               self.grid.data_ptr(), self.C, self.G, self.edge_epsilon,
+                                               self.loss_edge, self.seed, self.step_id, self.reg_loss.data_ptr(),
+                                               self.grid_grad.data_ptr(), self.reg_ws.data_ptr(), st),
+                       "neat_edge_loss")
+        return self.reg_loss
 
     def graph_step(self, uv, image_id, target):
         """step() replayed from a CUDA graph: the first call for a batch size

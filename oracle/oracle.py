@@ -555,3 +555,70 @@ def proposal_grad_f64(params, f, hist, mix):
     loss = (-(q * torch.log(p)).sum(1) * m).sum() / m.sum()
     loss.backward()
     return float(loss.detach()), P.grad.numpy()
+
+
+# --------------------------------------------------------------------------
+# volume regularisers (src/geometry/geometry_ex_ex.h:18-58, geometry_ex_ex.cpp:86-156)
+# --------------------------------------------------------------------------
+def tv_f64(grid, w):
+    """TVLoss without weights: w * C * sum over the 3 grid axes of
+    mean_node mean_{c,cells} |difference|, and its gradient (f64)."""
+    import torch
+    g = torch.tensor(np.asarray(grid, np.float64), requires_grad=True)
+    C = g.shape[1]
+    loss = 0
+    for d in (2, 3, 4):
+        n = g.shape[d]
+        diff = (g.narrow(d, 0, n - 1) - g.narrow(d, 1, n - 1)).abs().mean((1, 2, 3, 4))
+        loss = loss + diff.mean()
+    loss = loss * C * w
+    loss.backward()
+    return float(loss.detach()), g.grad.numpy()
+
+
+def edge_pairs(tree_min, tree_max, node_active, active_ids, max_depth, G, eps):
+    """NodeNeighborSamples: (node, face, point index, other node, point) of
+    every pair, in (node, face, point) order; every op in f32."""
+    per = 6 * G * G
+    A = active_ids.shape[0]
+    a = np.repeat(np.arange(A), per)
+    f = np.tile(np.repeat(np.arange(6), G * G), A)
+    k = np.tile(np.arange(G * G), 6 * A)
+    node = active_ids[a]
+    side, front = f // 2, f % 2
+    sa, sb = (side + 1) % 3, (side + 2) % 3
+    loc = np.zeros((a.shape[0], 3), np.float32)
+    idx = np.arange(a.shape[0])
+    loc[idx, side] = front.astype(np.float32)
+    loc[idx, sa] = (k % G).astype(np.float32) / np.float32(G - 1)
+    loc[idx, sb] = (k // G).astype(np.float32) / np.float32(G - 1)
+    mn, mx = tree_min[node].astype(np.float32), tree_max[node].astype(np.float32)
+    p = loc * (mx - mn) + mn
+    q = p.copy()
+    q[idx, side] = q[idx, side] + np.where(front == 1, np.float32(eps), np.float32(-eps))
+    other = active_node_for_positions(q, node_active, tree_min, tree_max, max_depth)
+    keep = (other != -1) & (other != node)
+    return a[keep], f[keep], k[keep], node[keep], other[keep], p[keep]
+
+
+def edge_f64(grid, tree_min, tree_max, node_active, active_ids, prefix, max_depth, eps, w, seed, step):
+    """Edge loss and its gradient (f64): pairs of NodeNeighborSamples, error
+    mean_c |f_node - f_other| * r, loss = w * C * mean over pairs."""
+    import torch
+    G = grid.shape[2]
+    a, f, k, node, other, p = edge_pairs(tree_min, tree_max, node_active, active_ids, max_depth, G, eps)
+    g = torch.tensor(np.asarray(grid, np.float64), requires_grad=True)
+    C = g.shape[1]
+    pt = torch.from_numpy(p.astype(np.float64))
+
+    def feat(nd):
+        mn = torch.from_numpy(tree_min[nd].astype(np.float64))
+        mx = torch.from_numpy(tree_max[nd].astype(np.float64))
+        return _trilinear_f64(torch, g, torch.from_numpy(prefix[nd]), (pt - mn) / (mx - mn) * 2 - 1)
+
+    r = torch.tensor([uniform(seed, int(ai), int(fi * G * G + ki), step, 0x45444745) for ai, fi, ki in zip(a, f, k)],
+                     dtype=torch.float64)
+    err = (feat(node) - feat(other)).abs().mean(1) * r
+    loss = err.mean() * w * C
+    loss.backward()
+    return float(loss.detach()), g.grad.numpy(), a.shape[0]

@@ -600,3 +600,66 @@ def test_bf16_grid_step_error_vs_f64(neat, oracle, case, c8_case, which):
     print(which, "BF16 grid + BF16 decoder vs f64: projection", e_pred, "grad decoder", e_dec, "grad grid", e_grid)
     assert e_pred < 1e-2 and e_dec < 5e-2 and e_grid < 5e-2
     assert torch.equal(tr.grid_bf16, tr.grid.to(torch.bfloat16))
+
+
+# ---------------------------------------------------------------- regularisers
+def test_tv_and_edge_regularisers_match_f64(neat, oracle, adaptive_case):
+    """TV and edge losses and the gradients they add into the grid gradient,
+    against f64 autograd restatements (mixed node sizes: adaptive tree)."""
+    from neat_b200 import _lib
+    c = adaptive_case
+    tr = _trainer(c, "bf16x3")
+    lib = _lib.load()
+    T = c.tree
+    tab = tr.tables
+    ws = torch.empty(lib.neat_regularizer_workspace_bytes(), dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    loss = torch.zeros(1, device="cuda")
+    grad = torch.zeros_like(tr.grid)
+    _lib.check(lib.neat_tv_loss(tr.grid.data_ptr(), tr.A, c.C, c.G, 0.3, loss.data_ptr(), grad.data_ptr(),
+                                ws.data_ptr(), st))
+    torch.cuda.synchronize()
+    l_ref, g_ref = oracle.tv_f64(c.grid, 0.3)
+    g = tr.grad_reference_layout(grad).cpu().numpy()
+    print("tv", float(loss.item()), l_ref, _rel2(g, g_ref))
+    assert abs(float(loss.item()) - l_ref) <= 1e-5 * l_ref
+    assert _rel2(g, g_ref) < 1e-5
+    loss.zero_()
+    grad.zero_()
+    _lib.check(lib.neat_edge_loss(tab["table"].data_ptr(), T.max_depth, tab["min"].data_ptr(), tab["max"].data_ptr(),
+                                  tab["active"].data_ptr(), tr.A, tr.grid.data_ptr(), c.C, c.G, 0.001, 0.2, 5, 3,
+                                  loss.data_ptr(), grad.data_ptr(), ws.data_ptr(), st))
+    torch.cuda.synchronize()
+    l_ref, g_ref, npairs = oracle.edge_f64(c.grid, T.node_position_min, T.node_position_max, T.node_active,
+                                           T.active_node_ids, T.node_active_prefix_sum, T.max_depth, 0.001, 0.2, 5, 3)
+    g = tr.grad_reference_layout(grad).cpu().numpy()
+    print("edge", float(loss.item()), l_ref, npairs, _rel2(g, g_ref))
+    assert npairs > 0
+    assert abs(float(loss.item()) - l_ref) <= 1e-5 * l_ref
+    assert _rel2(g, g_ref) < 1e-4
+
+
+def test_step_with_regularisers(neat, oracle, case):
+    """A step with TV and edge weights: the grid gradient Adam sees is the
+    projection loss's plus the regularisers' (f64 references of each)."""
+    c = case
+    from neat_b200.trainer import FusedTrainer
+    tr = FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
+                      grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec), loss_tv=0.05, loss_edge=0.02)
+    tr.step(_dev(c.uv), _dev(c.img), _dev(c.target))
+    torch.cuda.synchronize()
+    tr.check_status()
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                                  seed=99, step=1)
+    ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                          T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
+    l_tv, g_tv = oracle.tv_f64(c.grid, 0.05)
+    l_ed, g_ed, _ = oracle.edge_f64(c.grid, T.node_position_min, T.node_position_max, T.node_active,
+                                    T.active_node_ids, T.node_active_prefix_sum, T.max_depth, 0.001, 0.02, 99, 1)
+    g = tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1
+    err = _rel2(g, ref["grad_grid"] + g_tv + g_ed)
+    print("regularised step grid-gradient rel err", err, "reg loss", float(tr.reg_loss.item()), l_tv + l_ed)
+    assert err < 1e-4
+    assert abs(float(tr.reg_loss.item()) - (l_tv + l_ed)) <= 1e-5 * (l_tv + l_ed)

@@ -386,6 +386,29 @@ int neat_edge_loss(const void* tree_table, int max_depth, const float* node_min,
                    uint64_t seed, uint32_t step, float* loss, float* grid_grad, void* workspace, neat_stream_t stream);
 
 /* ----------------------------------------------------------------------- */
+/* Structure updates (the decisions stay on the host).                       */
+/* neat_node_max_density: ComputeMaxDensity (samples/reconstruct.cpp:254-286): */
+/* per active node the max decoded density over its G^3 lattice (cell       */
+/* (x,y,z) at local (x,y,z)/(G-1) * size + min, UniformGlobalSamples,       */
+/* src/structure/HyperTree.cu:781-815), points outside every image masked   */
+/* to 0 when num_images > 0 (PointInAnyImage, src/data/SceneBase.cu:13-45). */
+/* grid channel-last; out_max [num_active] f32.                              */
+/* neat_interpolate_grid: InterpolateInactiveNodes                          */
+/* (src/geometry/geometry_ex_ex.cpp:182-209): the new tree's grid rows from */
+/* the old grid at the new nodes' lattice points (old node by the top-down  */
+/* descent in the old tree's table; outside every old active node the first */
+/* old active node, as NodeIdForPositionGPU returns).  Both grids channel-  */
+/* last; node_min/max of the complete tree (shared by old and new).         */
+/* ----------------------------------------------------------------------- */
+int neat_node_max_density(const int64_t* active_ids, int64_t num_active, const float* node_min, const float* node_max,
+                          const float* grid, int C, int G, const float* decoder, float softplus_beta, int num_images,
+                          int w, int h, const double* intrinsics, const double* rotation, const double* translation,
+                          float* out_max, neat_stream_t stream);
+int neat_interpolate_grid(const int64_t* new_active_ids, int64_t new_num_active, const float* node_min,
+                          const float* node_max, const void* old_tree_table, int max_depth, int64_t old_first_active,
+                          const float* old_grid, int C, int G, float* new_grid, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
 /* Volume export.                                                            */
 /* Replaces HierarchicalNeuralGeometry::UniformSampledVolume                */
 /* (src/geometry/geometry.cpp:166-248) with VolumeSamples / NodeIdForPositionGPU */

@@ -113,6 +113,11 @@ _SIGS = {
                              ctypes.POINTER(ProjectOut), c_void_p, c_size_t, c_void_p]),
     "neat_proposal_params": (c_int64, []),
     "neat_regularizer_workspace_bytes": (c_size_t, []),
+    "neat_node_max_density": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p,
+                                      c_float, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_void_p]),
+    "neat_interpolate_grid": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_int64, c_void_p,
+                                      c_int, c_int, c_void_p, c_void_p]),
     "neat_tv_loss": (c_int, [c_void_p, c_int64, c_int, c_int, c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
     "neat_edge_loss": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int, c_int,
                                c_float, c_float, c_uint64, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -285,6 +285,60 @@ class FusedTrainer:
         psnr = 10.0 * math.log10(1.0 / mse) if mse > 0 else float("inf")
         return dict(mse=mse, l1=l1, psnr=psnr, images=out_imgs)
 
+    def ComputeMaxDensity(self, image_mask=True):
+        """ComputeMaxDensity (samples/reconstruct.cpp:254-286): per active node the
+        max decoded density over its G^3 lattice, points outside every image
+        masked out (PointInAnyImage) when image_mask.  Writes the tree's
+        node_max_density and returns the per-active-node values [A] (device)."""
+        out = torch.empty(self.A, dtype=torch.float32, device=self.dev)
+        cam = self.camera
+        n_img = cam.rotation.shape[0] if image_mask else 0
+        t = self.tables
+        _lib.check(self.lib.neat_node_max_density(
+            t["active"].data_ptr(), self.A, t["min"].data_ptr(), t["max"].data_ptr(), self.grid.data_ptr(), self.C,
+            self.G, self.decoder.data_ptr(), float(self.desc.softplus_beta), n_img, cam.w, cam.h,
+            cam.intrinsics.data_ptr(), cam.rotation.data_ptr(), cam.translation.data_ptr(), out.data_ptr(),
+            self._stream()), "neat_node_max_density")
+        self.tree.node_max_density[self.tree.active_node_ids] = out.cpu().numpy()
+        return out
+
+    def restructure(self, new_tree):
+        """Move to a new active-node structure: InterpolateInactiveNodes
+        (src/geometry/geometry_ex_ex.cpp:182-209) fills the new grid rows from
+        the current grid, then the optimizer state restarts
+        (ResetGeometryOptimizer)."""
+        if new_tree.max_depth != self.tree.max_depth:
+            raise ValueError("the new tree must have the same max_depth")
+        old_tables, old_grid, old_first = self.tables, self.grid, int(self.tree.active_node_ids[0])
+        new_tables = new_tree.device_tables(self.dev)
+        A = new_tree.NumActiveNodes()
+        grid = torch.empty((A, self.G, self.G, self.G, self.C), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.neat_interpolate_grid(
+            new_tables["active"].data_ptr(), A, new_tables["min"].data_ptr(), new_tables["max"].data_ptr(),
+            old_tables["table"].data_ptr(), self.tree.max_depth, old_first, old_grid.data_ptr(), self.C, self.G,
+            grid.data_ptr(), self._stream()), "neat_interpolate_grid")
+        self.tree, self.tables, self.A, self.grid = new_tree, new_tables, A, grid
+        self.grid_m = torch.zeros_like(grid)
+        self.grid_v = torch.zeros_like(grid)
+        self.grid_grad = torch.zeros_like(grid)
+        self.decoder_m.zero_()
+        self.decoder_v.zero_()
+        self.step_counter.zero_()
+        for desc in [self.desc] + ([self.desc_budget] if self.proposal else []):
+            desc.tree_table = new_tables["table"].data_ptr()
+            desc.num_active = A
+        self.state.grid, self.state.grid_m = grid.data_ptr(), self.grid_m.data_ptr()
+        self.state.grid_v, self.state.grid_grad = self.grid_v.data_ptr(), self.grid_grad.data_ptr()
+        if self.grid_bf16 is not None:
+            self.grid_bf16 = grid.to(torch.bfloat16).contiguous()
+            self.state.grid_bf16 = self.grid_bf16.data_ptr()
+        if self.proposal:
+            self.prop_node_desc = torch.zeros((A, 6), dtype=torch.float32, device=self.dev)
+            self.prop_struct.node_desc = self.prop_node_desc.data_ptr()
+        self.ws, self.ws_rays, self._graphs = None, 0, {}
+        if hasattr(self, "_graph_rays"):
+            del self._graph_rays
+
     def UniformSampledVolume(self, shape):
         """UniformSampledVolume (src/geometry/geometry.cpp:166-248): the decoded
         density on an nx*ny*nz voxel-corner grid of [-1,1]^3, shape = (nx, ny,

@@ -56,6 +56,8 @@ class HyperTreeBase:
         self.node_parent = parent
         self.node_children = children
         self.node_active = np.zeros(n, np.int32)
+        self.node_culled = np.zeros(n, np.int32)
+        self.node_max_density = np.zeros(n, np.float32)
         self._dev = {}
         self.SetActive(0)
 
@@ -83,6 +85,24 @@ class HyperTreeBase:
         self.active_node_ids = ids
         self.node_active_prefix_sum = pre
         self._dev = {}
+
+    def NodeCulling(self, threshold):
+        """NodeCulling (samples/reconstruct.cpp:288-319): active nodes whose
+        node_max_density (from ComputeMaxDensity) is below threshold become
+        culled and inactive.  Returns the number of newly culled nodes."""
+        new = ((self.node_max_density < threshold) & (self.node_active == 1)).astype(np.int32)
+        k = int(new.sum())
+        if k:
+            self.node_culled = np.clip(self.node_culled + new, 0, 1)
+            self.node_active = np.clip(self.node_active - new, 0, 1)
+            self.UpdateActive()
+        return k
+
+    def copy(self):
+        t = HyperTreeBase.__new__(HyperTreeBase)
+        t.__dict__.update({k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
+        t._dev = {}
+        return t
 
     def GlobalNodeIdToLocalActiveId(self, node_id):
         if isinstance(node_id, torch.Tensor):

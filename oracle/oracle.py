@@ -622,3 +622,67 @@ def edge_f64(grid, tree_min, tree_max, node_active, active_ids, prefix, max_dept
     loss = err.mean() * w * C
     loss.backward()
     return float(loss.detach()), g.grad.numpy(), a.shape[0]
+
+
+# --------------------------------------------------------------------------
+# structure updates (samples/reconstruct.cpp:254-319, geometry_ex_ex.cpp:182-209)
+# --------------------------------------------------------------------------
+def node_lattice(node_min, node_max, nodes, G):
+    """UniformGlobalSamples: [len(nodes), G^3, 3] f32, cells x fastest."""
+    z, y, x = np.meshgrid(np.arange(G), np.arange(G), np.arange(G), indexing="ij")
+    r = np.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], 1).astype(np.float32)
+    l = r / np.float32(G - 1)
+    mn = node_min[nodes].astype(np.float32)[:, None, :]
+    mx = node_max[nodes].astype(np.float32)[:, None, :]
+    return l[None] * (mx - mn) + mn
+
+
+def point_in_any_image(p, intr, rot, trans, w, h):
+    """PointInAnyImage (src/data/SceneBase.cu:13-45), f64, per row of p."""
+    fx, fy, cx, cy = intr.reshape(-1)[:4]
+    p = np.asarray(p, np.float64)
+    out = np.zeros(p.shape[0], bool)
+    for q, t in zip(rot, trans):
+        u, qw = -np.asarray(q[:3]), q[3]
+        v = p - t
+        tt = 2 * np.cross(u, v)
+        c = v + qw * tt + np.cross(u, tt)
+        px = np.round(fx * c[:, 0] / c[:, 2] + cx)
+        py = np.round(fy * c[:, 1] / c[:, 2] + cy)
+        out |= (px >= 0) & (px < w) & (py >= 0) & (py < h)
+    return out
+
+
+def node_max_density_f64(grid, dec, node_min, node_max, active_ids, G, beta=2.0, cam=None):
+    """ComputeMaxDensity: per active node the max f64 density over its lattice
+    (times the PointInAnyImage mask when cam = (intr, rot, trans, w, h))."""
+    import torch
+    A = active_ids.shape[0]
+    P = node_lattice(node_min, node_max, active_ids, G).reshape(-1, 3)
+    node = np.repeat(active_ids, G ** 3)
+    mn = torch.from_numpy(node_min[node].astype(np.float64))
+    mx = torch.from_numpy(node_max[node].astype(np.float64))
+    local = (torch.from_numpy(P.astype(np.float64)) - mn) / (mx - mn) * 2 - 1
+    row = torch.from_numpy(np.repeat(np.arange(A), G ** 3))
+    g = torch.as_tensor(np.asarray(grid, np.float64))
+    rho = decoder_f64(torch, _trilinear_f64(torch, g, row, local), torch.as_tensor(np.asarray(dec, np.float64)),
+                      g.shape[1], beta).numpy()
+    if cam is not None:
+        rho = rho * point_in_any_image(P, *cam)
+    return rho.reshape(A, -1).max(1)
+
+
+def interpolate_grid_f64(old_grid, node_min, node_max, old_active, old_ids, old_prefix, max_depth, new_ids, G):
+    """InterpolateInactiveNodes: the new rows [len(new_ids), C, G, G, G] from the
+    old grid at the new nodes' lattice points, f64."""
+    import torch
+    P = node_lattice(node_min, node_max, new_ids, G).reshape(-1, 3)
+    on = active_node_for_positions(P, old_active, node_min, node_max, max_depth)
+    on = np.where(on >= 0, on, old_ids[0])
+    mn = torch.from_numpy(node_min[on].astype(np.float64))
+    mx = torch.from_numpy(node_max[on].astype(np.float64))
+    local = (torch.from_numpy(P.astype(np.float64)) - mn) / (mx - mn) * 2 - 1
+    g = torch.as_tensor(np.asarray(old_grid, np.float64))
+    f = _trilinear_f64(torch, g, torch.from_numpy(old_prefix[on]), local).numpy()
+    C = g.shape[1]
+    return f.reshape(len(new_ids), G, G, G, C).transpose(0, 4, 1, 2, 3)

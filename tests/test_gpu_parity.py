@@ -663,3 +663,41 @@ def test_step_with_regularisers(neat, oracle, case):
     print("regularised step grid-gradient rel err", err, "reg loss", float(tr.reg_loss.item()), l_tv + l_ed)
     assert err < 1e-4
     assert abs(float(tr.reg_loss.item()) - (l_tv + l_ed)) <= 1e-5 * (l_tv + l_ed)
+
+
+# ---------------------------------------------------------------- structure updates
+def test_max_density_culling_and_interpolation(neat, oracle, adaptive_case):
+    """ComputeMaxDensity (with the in-image mask) against f64; culling on the
+    host; InterpolateInactiveNodes into a refined/coarsened tree against f64;
+    the trainer keeps stepping on the new structure."""
+    c = adaptive_case
+    tr = _trainer(c, "bf16x3")
+    T = c.tree
+    mx = tr.ComputeMaxDensity().cpu().numpy()
+    ref = oracle.node_max_density_f64(c.grid, c.dec, T.node_position_min, T.node_position_max, T.active_node_ids, c.G,
+                                      cam=(c.intr, c.rot, c.trans, c.w, c.h))
+    print("max density rel err", _rel2(mx, ref))
+    assert _rel2(mx, ref) < 1e-5
+    # cull the lowest quarter, then split the densest remaining leaf-level-minus-one node
+    thr = np.quantile(mx, 0.25)
+    new_tree = T.copy()
+    new_tree.node_max_density = T.node_max_density.copy()
+    k = new_tree.NodeCulling(thr)
+    assert k == int((mx < thr).sum()) and new_tree.NumActiveNodes() == T.NumActiveNodes() - k
+    act = set(new_tree.active_node_ids.tolist())
+    split = next(n for n in new_tree.active_node_ids if new_tree.node_depth[n] < new_tree.max_depth)
+    act.discard(int(split))
+    act.update(int(x) for x in new_tree.node_children[split])
+    new_tree.SetActiveNodes(sorted(act))
+    old_ref_grid = tr.grid_reference_layout().cpu().numpy()
+    tr.restructure(new_tree)
+    got = tr.grid_reference_layout().cpu().numpy()
+    want = oracle.interpolate_grid_f64(old_ref_grid, T.node_position_min, T.node_position_max, T.node_active,
+                                       T.active_node_ids, T.node_active_prefix_sum, T.max_depth,
+                                       new_tree.active_node_ids, c.G)
+    print("interpolation rel err", _rel2(got, want))
+    assert got.shape == want.shape and _rel2(got, want) < 1e-6
+    loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target))
+    torch.cuda.synchronize()
+    tr.check_status()
+    assert np.isfinite(float(loss.item()))

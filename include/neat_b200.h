@@ -281,6 +281,32 @@ typedef struct
     float* node_desc;  /* [num_active][6] node descriptors, written by TRAIN calls */
 } neat_proposal;
 
+/* ----------------------------------------------------------------------- */
+/* Photometric calibration fused into the loss (PhotometricCalibration,     */
+/* src/modules/ToneMapper.cpp:139-223, optimised by SGD in                   */
+/* SceneBase::OptimizerStep, src/data/SceneBase.cpp:121-157, 232-263):       */
+/*   y = I * exposure_factor[img] (if exposure_mult) + exposure_bias[img]    */
+/*       + sensor_bias(uv)  (bilinear, border, align_corners false)          */
+/*   y = response(y)  (25-point curve over [0, range], linear interpolation, */
+/*       border; + (y - range) above range while training)                  */
+/* then the loss compares y with the target.  The step adds the response's  */
+/* smoothness loss (CameraResponseNet::ParamLoss) to its gradient, takes one */
+/* SGD step per group and clamps the biases at 0 (ApplyConstraints).         */
+/* params (packed): exposure_factor [num_images] | exposure_bias            */
+/* [num_images] | sensor_bias [bias_h][bias_w] | response [25].             */
+/* ----------------------------------------------------------------------- */
+#define NEAT_RESPONSE_PARAMS 25
+typedef struct
+{
+    int exposure, exposure_mult, sensor_bias, response; /* enables */
+    int num_images, bias_w, bias_h;
+    float response_range;                               /* e.g. 2 */
+    float lr_exposure, lr_sensor_bias, lr_response;     /* SGD learning rates */
+    float* params;                                      /* packed, see above */
+    float* grad;                                        /* same layout: zero on entry, left zero */
+    float* param_loss;                                  /* optional device f32: ParamLoss of the step */
+} neat_tonemap;
+
 typedef struct
 {
     float* grid;       /* [A, G,G,G, C] channel-last */
@@ -306,6 +332,8 @@ typedef struct
      * master after every update; gradients stay FP32.  Requires a tensor-core
      * decoder path. */
     uint16_t* grid_bf16;
+    /* optional photometric calibration between the line integral and the loss; NULL: identity */
+    const neat_tonemap* tonemap;
 } neat_step_state;
 
 typedef struct

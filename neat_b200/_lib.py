@@ -55,10 +55,20 @@ class Proposal(ctypes.Structure):
                 ("beta2", c_float), ("eps", c_float), ("mix", c_float), ("iters", c_int), ("node_desc", c_void_p)]
 
 
+NEAT_RESPONSE_PARAMS = 25
+
+
+class ToneMap(ctypes.Structure):
+    _fields_ = [("exposure", c_int), ("exposure_mult", c_int), ("sensor_bias", c_int), ("response", c_int),
+                ("num_images", c_int), ("bias_w", c_int), ("bias_h", c_int), ("response_range", c_float),
+                ("lr_exposure", c_float), ("lr_sensor_bias", c_float), ("lr_response", c_float),
+                ("params", c_void_p), ("grad", c_void_p), ("param_loss", c_void_p)]
+
+
 class StepState(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("grid", "grid_m", "grid_v", "grid_grad",
                                         "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter",
-                                        "proposal", "grid_bf16")]
+                                        "proposal", "grid_bf16", "tonemap")]
 
 
 class StepBatch(ctypes.Structure):

@@ -207,11 +207,30 @@ __global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restri
     if (t * TT < e && t < tiles_cap) tile_seg[t] = (int)i;
 }
 
+// Photometric calibration of one ray's integral x (PhotometricCalibration::forward,
+// src/modules/ToneMapper.cpp:188-217): returns y and, given dL/dy, accumulates
+// the parameter gradients and returns dL/dx.
+struct ToneMap
+{
+    neat_tonemap t;
+    const float* uv;
+    const int32_t* image_id;
+};
+
+__device__ __forceinline__ int tm_off_bias(const neat_tonemap& t) { return 2 * t.num_images; }
+__device__ __forceinline__ int tm_off_resp(const neat_tonemap& t) { return 2 * t.num_images + t.bias_w * t.bias_h; }
+
 __global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const double* __restrict__ partial,
                            const float* __restrict__ target, float* __restrict__ dpred, float* __restrict__ pred_out,
-                           float* __restrict__ loss_part, float invR, const int64_t* nseg_eff)
+                           float* __restrict__ loss_part, float invR, const int64_t* nseg_eff, ToneMap tm)
 {
     __shared__ float red[256];
+    __shared__ float gresp[NEAT_RESPONSE_PARAMS];
+    const neat_tonemap& T = tm.t;
+    const bool on         = T.params != nullptr;
+    if (on && T.response)
+        for (int i = threadIdx.x; i < NEAT_RESPONSE_PARAMS; i += blockDim.x) gresp[i] = 0.0f;
+    if (on) __syncthreads();
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     float sq        = 0.0f;
     if (r < R)
@@ -224,10 +243,89 @@ __global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const
             for (int k = b; k < e; ++k) acc += partial[k];
             pred = (float)acc;
         }
-        const float diff = pred - target[r];
-        dpred[r]         = 2.0f * diff * invR;
-        sq               = diff * diff;
-        if (pred_out) pred_out[r] = pred;
+        if (!on)
+        {
+            const float diff = pred - target[r];
+            dpred[r]         = 2.0f * diff * invR;
+            sq               = diff * diff;
+            if (pred_out) pred_out[r] = pred;
+        }
+        else
+        {
+            // forward
+            const int img = tm.image_id[r];
+            float ef = 1.0f, y = pred;
+            if (T.exposure)
+            {
+                if (T.exposure_mult) ef = T.params[img];
+                y = y * ef + T.params[T.num_images + img];
+            }
+            int bx0 = 0, bx1 = 0, by0 = 0, by1 = 0;
+            float wx = 0.0f, wy = 0.0f;
+            if (T.sensor_bias)
+            {
+                // grid_sample, align_corners false, border: ix = u W - 0.5 clamped to [0, W-1]
+                const float* sb = T.params + tm_off_bias(T);
+                float ix = fminf(fmaxf(tm.uv[2 * r] * (float)T.bias_w - 0.5f, 0.0f), (float)(T.bias_w - 1));
+                float iy = fminf(fmaxf(tm.uv[2 * r + 1] * (float)T.bias_h - 0.5f, 0.0f), (float)(T.bias_h - 1));
+                bx0 = (int)floorf(ix);
+                by0 = (int)floorf(iy);
+                bx1 = min(bx0 + 1, T.bias_w - 1);
+                by1 = min(by0 + 1, T.bias_h - 1);
+                wx  = ix - (float)bx0;
+                wy  = iy - (float)by0;
+                y += (1.0f - wy) * ((1.0f - wx) * sb[by0 * T.bias_w + bx0] + wx * sb[by0 * T.bias_w + bx1]) +
+                     wy * ((1.0f - wx) * sb[by1 * T.bias_w + bx0] + wx * sb[by1 * T.bias_w + bx1]);
+            }
+            float slope = 1.0f;
+            int r0 = 0;
+            float rf = 0.0f;
+            if (T.response)
+            {
+                // x / range * (P-1), clamped (border), linear interpolation; leak above range
+                const float* rp = T.params + tm_off_resp(T);
+                const float ix  = fminf(fmaxf(y / T.response_range * (float)(NEAT_RESPONSE_PARAMS - 1), 0.0f),
+                                        (float)(NEAT_RESPONSE_PARAMS - 1));
+                r0              = min((int)floorf(ix), NEAT_RESPONSE_PARAMS - 2);
+                rf              = ix - (float)r0;
+                const float in_range = (y > 0.0f && y < T.response_range) ? 1.0f : 0.0f;
+                const float leak     = y > T.response_range ? y - T.response_range : 0.0f;
+                slope = in_range * (rp[r0 + 1] - rp[r0]) * ((float)(NEAT_RESPONSE_PARAMS - 1) / T.response_range) +
+                        (y > T.response_range ? 1.0f : 0.0f);
+                y = (1.0f - rf) * rp[r0] + rf * rp[r0 + 1] + leak;
+            }
+            const float diff = y - target[r];
+            const float dy   = 2.0f * diff * invR;
+            sq               = diff * diff;
+            if (pred_out) pred_out[r] = y;
+            // backward
+            if (T.response)
+            {
+                atomicAdd(&gresp[r0], dy * (1.0f - rf));
+                atomicAdd(&gresp[r0 + 1], dy * rf);
+            }
+            const float d2 = dy * slope;  // dL / d(exposed + bias)
+            if (T.sensor_bias)
+            {
+                float* g = T.grad + tm_off_bias(T);
+                atomicAdd(&g[by0 * T.bias_w + bx0], d2 * (1.0f - wy) * (1.0f - wx));
+                atomicAdd(&g[by0 * T.bias_w + bx1], d2 * (1.0f - wy) * wx);
+                atomicAdd(&g[by1 * T.bias_w + bx0], d2 * wy * (1.0f - wx));
+                atomicAdd(&g[by1 * T.bias_w + bx1], d2 * wy * wx);
+            }
+            if (T.exposure)
+            {
+                atomicAdd(&T.grad[T.num_images + img], d2);
+                if (T.exposure_mult) atomicAdd(&T.grad[img], d2 * pred);
+            }
+            dpred[r] = d2 * ef;
+        }
+    }
+    if (on && T.response)
+    {
+        __syncthreads();
+        for (int i = threadIdx.x; i < NEAT_RESPONSE_PARAMS; i += blockDim.x)
+            atomicAdd(&T.grad[tm_off_resp(T) + i], gresp[i]);
     }
     red[threadIdx.x] = sq;
     __syncthreads();
@@ -292,6 +390,71 @@ __global__ void k_step_begin(int* counter, int host_step, double lr_grid, double
     out->grid_step_size = (float)(lr_grid / bc1);
     out->dec_step_size  = (float)(lr_dec / bc1);
     out->sqrt_bc2       = (float)sqrt(bc2);
+}
+
+// CameraResponseNet::ParamLoss (src/modules/ToneMapper.cpp:100-119): with
+// f = P sqrt(1e-5), L = f^2 [r_0^2 + sum_{i=1..P-2} (r_i - (r_{i-1} + r_{i+1}) / 2)^2];
+// its gradient joins the response's; then SGD per group and the bias clamps
+// (ApplyConstraints), gradients zeroed.
+__global__ void k_tonemap_update(neat_tonemap T)
+{
+    const int P      = NEAT_RESPONSE_PARAMS;
+    const int n_all  = 2 * T.num_images + T.bias_w * T.bias_h + P;
+    const int ro     = 2 * T.num_images + T.bias_w * T.bias_h;
+    const float ff   = (float)P * P * 1e-5f;  // f^2
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_all; i += gridDim.x * blockDim.x)
+    {
+        float g = T.grad[i], lr = 0.0f;
+        bool clamp0 = false;
+        if (i < T.num_images)
+            lr = (T.exposure && T.exposure_mult) ? T.lr_exposure : 0.0f;
+        else if (i < 2 * T.num_images)
+        {
+            lr     = T.exposure ? T.lr_exposure : 0.0f;
+            clamp0 = true;
+        }
+        else if (i < ro)
+        {
+            lr     = T.sensor_bias ? T.lr_sensor_bias : 0.0f;
+            clamp0 = true;
+        }
+        else if (T.response)
+        {
+            lr           = T.lr_response;
+            const int k  = i - ro;
+            const float* r = T.params + ro;
+            auto e = [&](int j) { return r[j] - 0.5f * (r[j - 1] + r[j + 1]); };  // 1 <= j <= P-2
+            float gl = 0.0f;
+            if (k == 0) gl += 2.0f * r[0];
+            if (k >= 1 && k <= P - 2) gl += 2.0f * e(k);
+            if (k - 1 >= 1 && k - 1 <= P - 2) gl -= e(k - 1);
+            if (k + 1 >= 1 && k + 1 <= P - 2) gl -= e(k + 1);
+            g += ff * gl;
+        }
+        float v = T.params[i] - lr * g;
+        if (clamp0) v = fmaxf(v, 0.0f);
+        T.params[i] = v;
+        T.grad[i]   = 0.0f;
+    }
+}
+
+__global__ void k_tonemap_param_loss(neat_tonemap T)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !T.param_loss) return;
+    const int P    = NEAT_RESPONSE_PARAMS;
+    const float* r = T.params + 2 * T.num_images + T.bias_w * T.bias_h;
+    float l        = 0.0f;
+    if (T.response)
+    {
+        l = r[0] * r[0];
+        for (int j = 1; j <= P - 2; ++j)
+        {
+            const float e = r[j] - 0.5f * (r[j - 1] + r[j + 1]);
+            l += e * e;
+        }
+        l *= (float)P * P * 1e-5f;
+    }
+    *T.param_loss = l;
 }
 
 __global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, int P, float* __restrict__ grad,
@@ -748,6 +911,10 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     if (!proposal_mode(d, s->proposal, pmode)) return NEAT_ERR_BAD_INPUT;
     if (s->grid_bf16 && (d->decoder_path == NEAT_DECODER_SIMT_FP32 || ((uintptr_t)s->grid_bf16 & 15)))
         return NEAT_ERR_BAD_INPUT;
+    if (s->tonemap && (!s->tonemap->params || !s->tonemap->grad || s->tonemap->num_images < 1 ||
+                       (s->tonemap->sensor_bias && (s->tonemap->bias_w < 2 || s->tonemap->bias_h < 2)) ||
+                       !(s->tonemap->response_range > 0.0f)))
+        return NEAT_ERR_BAD_INPUT;
     const int64_t R = b->num_rays;
     StepLayout L;
     if (!step_layout(d, R, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
@@ -783,8 +950,15 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ta.seg_hist = nullptr;
     phase(2);
     const float invR = (float)(1.0 / (double)R);
+    ToneMap tm{};
+    if (s->tonemap)
+    {
+        tm.t        = *s->tonemap;
+        tm.uv       = b->uv;
+        tm.image_id = b->image_id;
+    }
     k_ray_loss<<<L.loss_blocks, 256, 0, st>>>(R, w.ray_seg_off, w.partial, b->target, w.dpred, out->prediction,
-                                               w.loss_part, invR, cnt + 0);
+                                               w.loss_part, invR, cnt + 0, tm);
     k_loss_final<<<1, 1024, 0, st>>>(w.loss_part, L.loss_blocks, out->loss, invR);
     phase(3);
     ok = ok && launch_tiles_path(d, true, ta, st) == cudaSuccess;
@@ -798,6 +972,11 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
                                   0.0f, 1.0f, 1, w.scal, s->grid_bf16);
+    if (s->tonemap)
+    {
+        k_tonemap_param_loss<<<1, 32, 0, st>>>(*s->tonemap);
+        k_tonemap_update<<<8, 256, 0, st>>>(*s->tonemap);
+    }
     if (pmode == NEAT_PROPOSAL_TRAIN)
     {
         ok = ok && launch_node_desc(s->grid, A, d->C, d->G, s->decoder, d->softplus_beta, pr->node_desc, st) ==

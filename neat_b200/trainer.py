@@ -23,7 +23,8 @@ class FusedTrainer:
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
-                 proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001):
+                 proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
+                 tonemap=None):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -82,6 +83,14 @@ class FusedTrainer:
         self.loss_tv, self.loss_edge, self.edge_epsilon = float(loss_tv), float(loss_edge), float(edge_epsilon)
         self.reg_loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
         self.reg_ws = torch.empty(lib.neat_regularizer_workspace_bytes(), dtype=torch.uint8, device=self.dev)
+        # photometric calibration (PhotometricCalibration): tonemap = dict of
+        # PhotometricCalibrationParams fields (response_enable, response_range,
+        # response_lr, exposure_enable, exposure_mult, exposure_lr,
+        # sensor_bias_enable, sensor_bias_size_w, sensor_bias_lr) or None
+        self.tonemap = None
+        if tonemap is not None:
+            self.tonemap = PhotometricCalibration(camera.rotation.shape[0], camera.w, camera.h, self.dev, **tonemap)
+            self.state.tonemap = ctypes.addressof(self.tonemap.struct)
         # precision variant: the sample gathers read a BF16 copy of the grid that
         # Adam refreshes from the FP32 master after every update
         self.grid_bf16 = None
@@ -373,3 +382,36 @@ class FusedTrainer:
         _lib.check(self.lib.neat_grid_from_channel_last(t.data_ptr(), out.data_ptr(), self.A, self.C, self.G,
                                                         self._stream()), "neat_grid_from_channel_last")
         return out
+
+
+class PhotometricCalibration:
+    """Parameters of the photometric calibration the fused step applies between
+    the line integral and the loss (PhotometricCalibrationImpl,
+    src/modules/ToneMapper.cpp:139-223; defaults of PhotometricCalibrationParams,
+    src/modules/ToneMapper.h:36-47).  Packed exposure_factor [n] | exposure_bias
+    [n] | sensor_bias [bias_h][bias_w] | response [25]; the response starts as
+    the identity on [0, range] (a gamma-1 curve normalised to the range)."""
+
+    def __init__(self, num_images, w, h, device, response_enable=True, response_range=2.0, response_lr=0.1,
+                 exposure_enable=True, exposure_mult=False, exposure_lr=0.01, sensor_bias_enable=True,
+                 sensor_bias_size_w=32, sensor_bias_lr=0.05):
+        n = int(num_images)
+        bw = int(sensor_bias_size_w)
+        bh = int(math.ceil(bw * (float(h) / w)))
+        P = _lib.NEAT_RESPONSE_PARAMS
+        self.num_images, self.bias_w, self.bias_h = n, bw, bh
+        self.params = torch.cat([torch.ones(n), torch.zeros(n), torch.zeros(bh * bw),
+                                 torch.arange(P, dtype=torch.float32) / (P - 1) * float(response_range)]).to(device)
+        self.grad = torch.zeros_like(self.params)
+        self.param_loss = torch.zeros(1, dtype=torch.float32, device=device)
+        self.struct = _lib.ToneMap(
+            exposure=int(bool(exposure_enable)), exposure_mult=int(bool(exposure_mult)),
+            sensor_bias=int(bool(sensor_bias_enable)), response=int(bool(response_enable)), num_images=n, bias_w=bw,
+            bias_h=bh, response_range=float(response_range), lr_exposure=float(exposure_lr),
+            lr_sensor_bias=float(sensor_bias_lr), lr_response=float(response_lr), params=self.params.data_ptr(),
+            grad=self.grad.data_ptr(), param_loss=self.param_loss.data_ptr())
+
+    def split(self):
+        n, b = self.num_images, self.bias_w * self.bias_h
+        p = self.params
+        return p[:n], p[n:2 * n], p[2 * n:2 * n + b].reshape(self.bias_h, self.bias_w), p[2 * n + b:]

@@ -686,3 +686,38 @@ def interpolate_grid_f64(old_grid, node_min, node_max, old_active, old_ids, old_
     f = _trilinear_f64(torch, g, torch.from_numpy(old_prefix[on]), local).numpy()
     C = g.shape[1]
     return f.reshape(len(new_ids), G, G, G, C).transpose(0, 4, 1, 2, 3)
+
+
+# --------------------------------------------------------------------------
+# photometric calibration (src/modules/ToneMapper.cpp:14-223), with torch's own
+# grid_sample as the reference calls it
+# --------------------------------------------------------------------------
+def tonemap_f64(torch, x, uv, img, ef, eb, sb, resp, rng, exposure=True, mult=False, sensor=True, response=True,
+                training=True):
+    """PhotometricCalibration::forward on ray integrals x [R] (f64 autograd)."""
+    F = torch.nn.functional
+    y = x
+    if exposure:
+        if mult:
+            y = y * ef[img]
+        y = y + eb[img]
+    if sensor:
+        g = (uv * 2 - 1).unsqueeze(0).unsqueeze(0)
+        s = F.grid_sample(sb.reshape(1, 1, *sb.shape), g, mode="bilinear", padding_mode="border", align_corners=False)
+        y = y + s.reshape(-1)
+    if response:
+        leak = (y - rng) * (y > rng) if training else 0
+        xi = (y * (1.0 / rng)) * 2 - 1
+        grid = torch.stack([xi, torch.zeros_like(xi)], 1).reshape(1, 1, -1, 2)
+        r = F.grid_sample(resp.reshape(1, 1, 1, -1), grid, mode="bilinear", padding_mode="border", align_corners=True)
+        y = r.reshape(-1) + leak
+    return y
+
+
+def response_param_loss_f64(torch, resp):
+    """CameraResponseNet::ParamLoss (src/modules/ToneMapper.cpp:100-119)."""
+    P = resp.shape[0]
+    target = resp.clone()
+    target = torch.cat([torch.zeros(1, dtype=resp.dtype), (resp[2:] + resp[:-2]) * 0.5, resp[-1:]])
+    f = P * np.sqrt(1e-5)
+    return ((resp * f - target * f) ** 2).sum()

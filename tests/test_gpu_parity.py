@@ -701,3 +701,57 @@ def test_max_density_culling_and_interpolation(neat, oracle, adaptive_case):
     torch.cuda.synchronize()
     tr.check_status()
     assert np.isfinite(float(loss.item()))
+
+
+# ---------------------------------------------------------------- photometric calibration
+def test_photometric_calibration_step(neat, oracle, case):
+    """The step with exposure (factor and bias), sensor-bias map and response
+    curve fused into the loss: prediction, grid and decoder gradients, the
+    ParamLoss, and the SGD-updated, clamped calibration parameters against f64
+    autograd through torch's own grid_sample (as the reference calls it)."""
+    c = case
+    from neat_b200.trainer import FusedTrainer
+    tmc = dict(exposure_mult=True, response_range=2.0)
+    tr = FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
+                      grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec), tonemap=tmc)
+    tm = tr.tonemap
+    rng = np.random.default_rng(21)
+    n, b = tm.num_images, tm.bias_w * tm.bias_h
+    p0 = tm.params.cpu().numpy().astype(np.float64)
+    p0[:n] = rng.uniform(0.8, 1.2, n)
+    p0[n:2 * n] = rng.uniform(0.0, 0.05, n)
+    p0[2 * n:2 * n + b] = rng.uniform(0.0, 0.05, b)
+    p0[2 * n + b:] = np.sort(p0[2 * n + b:] + rng.uniform(-0.02, 0.02, 25))
+    p0[2 * n + b] = 0.0
+    tm.params.copy_(torch.from_numpy(p0.astype(np.float32)))
+    p0 = tm.params.cpu().numpy().astype(np.float64)
+    pred = torch.zeros(c.R, device="cuda")
+    loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
+    torch.cuda.synchronize()
+    tr.check_status()
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                              seed=99, step=1)
+    grid = torch.tensor(c.grid.astype(np.float64), requires_grad=True)
+    dec = torch.tensor(c.dec.astype(np.float64), requires_grad=True)
+    P = torch.tensor(p0, requires_grad=True)
+    x = oracle.image_f64(s, grid, dec, T.node_position_min, T.node_position_max, T.node_active_prefix_sum, c.R)
+    y = oracle.tonemap_f64(torch, x, torch.from_numpy(c.uv.astype(np.float64)), torch.from_numpy(c.img.astype(np.int64)),
+                           P[:n], P[n:2 * n], P[2 * n:2 * n + b].reshape(tm.bias_h, tm.bias_w), P[2 * n + b:], 2.0,
+                           mult=True)
+    mse = ((y - torch.from_numpy(c.target.astype(np.float64))) ** 2).mean()
+    pl = oracle.response_param_loss_f64(torch, P[2 * n + b:])
+    (mse + pl).backward()
+    e = dict(pred=_rel2(pred.cpu().numpy(), y.detach().numpy()), loss=abs(float(loss.item()) - float(mse)) / float(mse),
+             dec=_rel2(tr.decoder_grad.cpu().numpy(), dec.grad.numpy()),
+             grid=_rel2(tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1, grid.grad.numpy()),
+             param_loss=abs(float(tm.param_loss.item()) - float(pl)) / float(pl))
+    lr = np.concatenate([np.full(n, 0.01), np.full(n, 0.01), np.full(b, 0.05), np.full(25, 0.1)])
+    want = p0 - lr * P.grad.numpy()
+    want[n:2 * n + b] = np.maximum(want[n:2 * n + b], 0.0)
+    e["params"] = _rel2(tm.params.cpu().numpy() - p0, want - p0)
+    print("photometric calibration errors", {k: f"{v:.2e}" for k, v in e.items()})
+    assert e["pred"] < 1e-5 and e["loss"] < 1e-5 and e["dec"] < 1e-5 and e["grid"] < 1e-5
+    assert e["param_loss"] < 1e-5 and e["params"] < 1e-4
+    assert float(tm.grad.abs().max()) == 0.0

@@ -30,25 +30,39 @@ constexpr int MAX_PLANES = (1 << kMaxDepth) + 1;
 
 constexpr int MAX_FRONT = 256;  // a line meets at most 3 * 2^d - 2 nodes of level d (d <= 6 here)
 
-struct WarpHits
+// Per-warp scratch of one ray: HC hits, FC frontier nodes, planes of depth <= DM.
+template <int HC, int FC, int DM>
+struct WarpHitsT
 {
-    float T[3 * MAX_PLANES];
-    float tmin[kMaxHits];
-    float tmax[kMaxHits];
-    int a[kMaxHits];     // active (local) id
-    int node[kMaxHits];  // global node id
-    int n[kMaxHits];     // samples of the segment
-    int ord[kMaxHits];   // sorted position -> hit index
-    int pre[kMaxHits];   // exclusive prefix of n in sorted order
-    int front[2][MAX_FRONT];
+    static constexpr int kHits  = HC;
+    static constexpr int kFront = FC;
+    static constexpr int kDepth = DM;
+    float T[3 * ((1 << DM) + 1)];
+    float tmin[HC];
+    float tmax[HC];
+    int a[HC];     // active (local) id
+    int node[HC];  // global node id
+    int n[HC];     // samples of the segment
+    int ord[HC];   // sorted position -> hit index
+    int pre[HC];   // exclusive prefix of n in sorted order
+    int front[2][FC];
 };
+// Any tree the library takes (the reference's 256-hit limit, depth 7).
+using WarpHits = WarpHitsT<kMaxHits, MAX_FRONT, kMaxDepth>;
+// The fused step with at most 64 hits kept per ray and depth <= 5: a line
+// meets at most 3 * 2^4 - 2 = 46 nodes of level 4, so 64 frontier entries
+// hold every internal level; 2.7 KB per warp instead of 10.7 KB.
+using WarpHitsStep = WarpHitsT<64, 64, 5>;
 
 // Hits of one ray: active nodes whose slab test passes and whose segment is
 // at least 1e-5 long (HyperTree.cu:274-277).  Returns the raw count (only
 // the first kMaxHits are stored); sets *overflow if a frontier overflowed.
+template <class WH>
 __device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int M, const float o[3], const float d[3],
-                                  WarpHits& ws, int lane, bool& overflow)
+                                  WH& ws, int lane, bool& overflow)
 {
+    constexpr int kMaxHits  = WH::kHits;
+    constexpr int MAX_FRONT = WH::kFront;
     const int P = (1 << D) + 1;
     for (int i = lane; i < 3 * P; i += 32)
     {
@@ -143,7 +157,8 @@ __device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int 
 
 // Rank sort by (tmin, node id) and exclusive prefix of sample counts in that
 // order.  Returns the ray's total sample count.
-__device__ int warp_sort_prefix(WarpHits& ws, int k, int lane)
+template <class WH>
+__device__ int warp_sort_prefix(WH& ws, int k, int lane)
 {
     for (int i = lane; i < k; i += 32)
     {
@@ -358,6 +373,7 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
 // Fused step: one traversal per ray (canonical hit list kept per ray), then
 // the lists are placed node-major.
 // ---------------------------------------------------------------------------
+template <class WH>
 __global__ void __launch_bounds__(32 * RAY_WARPS)
     k_step_rays(const float* __restrict__ uv, const int32_t* __restrict__ image_id, int64_t R, int w, int h,
                 const double* __restrict__ intr, const double* __restrict__ rot, const double* __restrict__ trans,
@@ -365,7 +381,8 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
                 float* __restrict__ direction, SegRec* __restrict__ ray_hits, int* __restrict__ ray_nseg,
                 int* __restrict__ node_nseg, int64_t* counters, int* status)
 {
-    __shared__ WarpHits sh[RAY_WARPS];
+    constexpr int kMaxHits = WH::kHits;
+    __shared__ WH sh[RAY_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t r = (int64_t)blockIdx.x * RAY_WARPS + warp;
     if (r >= R) return;
@@ -377,12 +394,16 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         origin[3 * r + lane]    = o[lane];
         direction[3 * r + lane] = d[lane];
     }
-    WarpHits& ws = sh[warp];
-    bool ovf     = false;
-    int k        = warp_traverse_hits(table, D, M, o, d, ws, lane, ovf);
+    WH& ws   = sh[warp];
+    bool ovf = false;
+    int k    = warp_traverse_hits(table, D, M, o, d, ws, lane, ovf);
     if (k > kMaxHits || ovf)
     {
-        if (lane == 0) raise_status(status, NEAT_ERR_TOO_MANY_HITS);
+        // the reference keeps 256 hits; beyond this scratch's capacity the
+        // step's own per-ray capacity (<= the scratch) is exceeded as well
+        if (lane == 0) raise_status(status, (k > kMaxHits && kMaxHits < NEAT_MAX_HITS_PER_RAY && !ovf)
+                                                ? NEAT_ERR_CAPACITY
+                                                : NEAT_ERR_TOO_MANY_HITS);
         k = min(k, kMaxHits);
     }
     if (k > cap_ray)
@@ -451,9 +472,16 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
 {
     if (R <= 0) return cudaSuccess;
     const unsigned grid = (unsigned)((R + RAY_WARPS - 1) / RAY_WARPS);
-    k_step_rays<<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans, (const NodeEntry*)table, D,
-                                                 M, cap_ray, origin, direction, ray_hits, ray_nseg, node_nseg,
-                                                 counters, status);
+    if (cap_ray <= WarpHitsStep::kHits && D <= WarpHitsStep::kDepth)
+        k_step_rays<WarpHitsStep><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
+                                                                   (const NodeEntry*)table, D, M, cap_ray, origin,
+                                                                   direction, ray_hits, ray_nseg, node_nseg, counters,
+                                                                   status);
+    else
+        k_step_rays<WarpHits><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
+                                                               (const NodeEntry*)table, D, M, cap_ray, origin,
+                                                               direction, ray_hits, ray_nseg, node_nseg, counters,
+                                                               status);
     return cudaGetLastError();
 }
 

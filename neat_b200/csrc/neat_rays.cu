@@ -16,6 +16,7 @@
 // from a shared-memory atomic (src/structure/HyperTree.cu:281) and is not
 // reproducible, its content (hit set, tmin/tmax, sample counts) is matched
 // bit for bit.
+#include <algorithm>
 #include <cstdio>
 
 #include "neat_common.cuh"
@@ -445,24 +446,34 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
 }
 
 // Place every ray's segments into its nodes' buckets (thread per segment).
-__global__ void k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_nseg,
-                             const int* __restrict__ ray_seg_off, int64_t R, int cap_ray,
-                             const int* __restrict__ node_seg_off, int* __restrict__ node_cursor,
-                             SegRec* __restrict__ segs, int* __restrict__ seg_n, const int64_t* nseg_eff,
-                             int64_t cap)
+// Place every ray's segments into its nodes' buckets: one thread per segment
+// (ray-major index rm < counters[0]); its ray by binary search in the ray
+// offsets.
+__global__ void k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_seg_off, int64_t R,
+                             int cap_ray, const int* __restrict__ node_seg_off, int* __restrict__ node_cursor,
+                             SegRec* __restrict__ segs, int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
 {
-    if (*nseg_eff == 0) return;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t r = i / cap_ray;
-    const int p     = (int)(i - r * cap_ray);
-    if (r >= R || p >= ray_nseg[r]) return;
-    SegRec sg    = ray_hits[i];
-    const int rm = ray_seg_off[r] + p;
-    const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
-    if (rm >= cap || nm >= cap) return;  // unreachable: the totals were checked against cap
-    sg.rm     = rm;
-    segs[nm]  = sg;
-    seg_n[nm] = sg.n;
+    const int64_t nseg = *nseg_eff;  // 0 after a capacity overflow
+    for (int64_t rm = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rm < nseg;
+         rm += (int64_t)gridDim.x * blockDim.x)
+    {
+        int64_t lo = 0, hi = R;  // ray_seg_off[lo] <= rm < ray_seg_off[hi]
+        while (hi - lo > 1)
+        {
+            const int64_t mid = (lo + hi) >> 1;
+            if (ray_seg_off[mid] <= rm)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const int p  = (int)(rm - ray_seg_off[lo]);
+        SegRec sg    = ray_hits[lo * cap_ray + p];
+        const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
+        if (rm >= cap || nm >= cap) continue;  // unreachable: the totals were checked against cap
+        sg.rm     = (int32_t)rm;
+        segs[nm]  = sg;
+        seg_n[nm] = sg.n;
+    }
 }
 
 cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R, int w, int h, const double* intr,
@@ -490,9 +501,11 @@ cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const
                               const int64_t* nseg_eff, int64_t cap, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
-    const int64_t n = R * (int64_t)cap_ray;
-    k_step_place<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ray_hits, ray_nseg, ray_seg_off, R, cap_ray,
-                                                              node_seg_off, node_cursor, segs, seg_n, nseg_eff, cap);
+    (void)ray_nseg;
+    const int64_t est = std::min<int64_t>(cap, R * 8);
+    const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((est + 255) / 256, (int64_t)sm_count() * 16));
+    k_step_place<<<nb, 256, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, node_cursor, segs, seg_n,
+                                     nseg_eff, cap);
     return cudaGetLastError();
 }
 

@@ -54,6 +54,11 @@ PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 # x 3 kernels, segment clamp, placement, partial zeroing, sample clamp, tile
 # map, forward tiles, ray loss, loss total, backward tiles, decoder Adam, grid Adam
 STEP_LAUNCHES = 22
+# DRAM bytes per sample of the backward tile kernel from one ncu capture of the
+# same scene at 2^16 rays (dram__bytes_read.sum + dram__bytes_write.sum = 528.0 MB
+# for 2.908 M samples; profiles/step_tiles_tc_bf16x3_65k_rays.md), scaled to a
+# launch by its samples -- an upper bound at larger batches (more grid reuse in L2)
+TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 528.0e6 / 2.908e6}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_step_tiles_tc<C=%d, BF16x3, backward>",
                "bf16": "k_step_tiles_tc<C=%d, BF16, backward>"}
@@ -528,7 +533,10 @@ def main():
                        4 * 4 * tr.grid.numel() / 1e9)},
         "phase_ms": phase_ms,
         "roofline": {"kernel": KERNEL_NAME[args.decoder] % cfg["C"], "bound": "tensor", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": (TRAFFIC_BYTES_PER_SAMPLE[(args.workload, args.decoder)] * S
+                                 if (args.workload, args.decoder) in TRAFFIC_BYTES_PER_SAMPLE else None),
+                     "traffic_source": "ncu capture at 2^16 rays scaled by samples (upper bound)",
                      "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                      "fp32_simt_peak_tflops": simt_peak,
                      "frac_of_fp32_simt": achieved / simt_peak},

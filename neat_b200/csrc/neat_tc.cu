@@ -94,10 +94,11 @@ struct TcThreads
     static constexpr int min_blocks = (PREC == BF16X3) ? (BWD ? 1 : 2) : (BWD ? 2 : 4);
 };
 
-// Shared-memory plan of a tile CTA.  HB rows hold [h1 | x | 1 0 ..] (the
-// weight-gradient B operand).  NX1 separate [x | 1] buffers (0 or 2): with
-// two, the backward issues the next tile's layer-1 GEMM from its own buffer
-// before the current tile's weight-gradient GEMM has finished reading HB.
+// Shared-memory plan of a tile CTA.  Backward HB rows hold [h1 | x | 1 0 ..]
+// (the weight-gradient B operand), forward HB rows h1.  NX1 separate [x | 1]
+// buffers (0 or 2): with two, the next tile's layer-1 GEMM is issued from its
+// own buffer while the current tile is still in flight (backward: behind the
+// weight-gradient GEMM; forward: behind layer 2).
 template <int C, int PREC, bool BWD, int NX1_>
 struct CfgPlan
 {
@@ -106,8 +107,8 @@ struct CfgPlan
     static constexpr int XW     = ((C + 7) / 8) * 8;          // x columns (C padded)
     static constexpr int K1     = ((XW + 1 + 15) / 16) * 16;  // layer-1 K: [x | 1 | 0 ..]
     static constexpr int ONE    = XW;                         // column of the 1 in [x | 1]
-    static constexpr int NW     = HH + K1;                    // HB columns
-    using HB                    = Buf<PREC, 128, NW>;
+    static constexpr int NW     = HH + K1;                    // weight-gradient N: [h1 | x | 1 ..]
+    using HB                    = Buf<PREC, 128, BWD ? NW : HH>;  // the forward keeps h1 only
     using X1                    = Buf<PREC, 128, K1>;         // [x | 1 | 0 ..] rows
     using AB                    = Buf<PREC, 128, 2 * HH>;     // [dz2 | dz1] rows
     using W2                    = Buf<PREC, HH, HH>;
@@ -132,9 +133,9 @@ struct CfgPlan
 };
 
 template <int C, int PREC, bool BWD>
-struct Cfg : CfgPlan<C, PREC, BWD, (BWD && CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
+struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
 {
-    using Base = CfgPlan<C, PREC, BWD, (BWD && CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
+    using Base = CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
     // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 [128, 192 + K1)
     // weight gradients (h1 columns, then [x | 1] columns), D3 [192 + K1, 192 + 2 K1) dX
     static constexpr uint32_t TMEM_COLS = BWD ? 256 : 128;
@@ -292,7 +293,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     constexpr int TC_THREADS = TcThreads<PREC, BWD>::value;
     constexpr int NH         = K::NH;     // threads per sample
     constexpr int HALF       = HH / NH;   // hidden units per thread
-    constexpr bool PIPE      = BWD && K::NX1 == 2;
+    constexpr bool PIPE      = BWD && K::NX1 == 2;   // pipelined backward
+    constexpr bool FPIPE     = !BWD && K::NX1 == 2;  // pipelined forward
     extern __shared__ __align__(128) unsigned char sm[];
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
@@ -468,14 +470,16 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         }
     };
     // layer 1 from the separate buffer b (pipelined) or from HB's [x | 1] columns
+    // (the pipelined forward signals layer 1 on mbar_wg: its layer 2 is still
+    // pending on mbar, and one barrier must never run two phases ahead of its waiter)
     auto issue_l1 = [&](int b) {
-        if constexpr (PIPE)
+        if constexpr (PIPE || FPIPE)
             gemm<PREC, KS1, X1::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(x1_addr(b), 128, X1::RG),
                                                             sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
         else
             gemm<PREC, KS1, HB::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(s_base + K::OFF_HB + (HH / 8) * 128, 128, HB::RG),
                                                             sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
-        mma_commit(mbar);
+        mma_commit(FPIPE ? mbar_wg : mbar);
     };
     // dX of the previous tile (TMEM D3), scattered with the trilinear weights;
     // each thread of a sample takes 8 / NH corners.
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     {
         stage_a(blockIdx.x, 0);
         if (h == 0) cur = stage_b(blockIdx.x, 0);
-        if constexpr (PIPE)
+        if constexpr (PIPE || FPIPE)
         {
             if (h == 0)
             {
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             scatter_prev(buf ^ 1);
         }
         // ---- Z1 = [x | 1] . [W1 | b1]^T (already in flight when pipelined)
-        if constexpr (!PIPE)
+        if constexpr (!PIPE && !FPIPE)
         {
             if (h == 0)
             {
@@ -589,7 +593,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
         }
         if (has_next) stage_a(nxt, buf ^ 1);
-        if (!wait_on(mbar, phase))
+        if (!(FPIPE ? wait_on(mbar_wg, phase_wg) : wait_on(mbar, phase)))
         {
             ok = false;
             break;
@@ -618,6 +622,23 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             mma_commit(mbar);
         }
         if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1);
+        if constexpr (FPIPE)
+        {
+            // the next tile's layer 1, queued behind this tile's layer 2 (its
+            // [x | 1] buffer was last read by the layer 1 of two tiles ago)
+            if (has_next)
+            {
+                if (h == 0) put_x1(nx.x, xb ^ 1);
+                fence_smem_async();
+                fence_before();
+                __syncthreads();
+                if (t == 0)
+                {
+                    fence_after();
+                    issue_l1(xb ^ 1);
+                }
+            }
+        }
         if (!wait_on(mbar, phase))
         {
             ok = false;

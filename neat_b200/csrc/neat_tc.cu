@@ -122,8 +122,8 @@ struct CfgPlan
     static constexpr int OFF_AB = OFF_X1 + NX1 * X1SZ;
     static constexpr int OFF_F  = OFF_AB + (BWD ? P::PIECES * AB::BYTES : 0);
     static constexpr int NF     = 2 * HH + 4;                 // b2, w3, b3
-    static constexpr int OFF_I  = OFF_F + NF * 4;
-    static constexpr int OFF_V  = OFF_I + (2 * 128 + 128 + 2 * 132) * 4;
+    static constexpr int OFF_I  = OFF_F + NF * 4;             // [2][132] segment starts, then 4 f64 + 8 int
+    static constexpr int OFF_V  = OFF_I + 2 * 132 * 4 + 4 * 8 + 8 * 4;
     static constexpr int OFF_Q  = OFF_V + 2 * 128 * 4;        // [2][6][128] slot data for the second thread
     static constexpr int NQ     = (BWD && NH == 2) ? 2 * 6 * 128 : 0;
     static constexpr int OFF_R  = OFF_Q + NQ * 4;
@@ -145,6 +145,7 @@ struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 
     static constexpr int BYTES     = Base::NEED > MIN_BYTES ? Base::NEED : MIN_BYTES;
     static_assert(!BWD || 192 + 2 * Base::K1 <= 256, "D4 and D3 must fit in the allocation");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
+    static_assert((Base::OFF_I + 2 * 132 * 4) % 8 == 0, "f64 reduction scratch must be 8-byte aligned");
 };
 
 // ---------------------------------------------------------------------------
@@ -302,9 +303,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     float* sb2    = reinterpret_cast<float*>(sm + K::OFF_F);
     float* sw3    = sb2 + HH;
     float* sb3    = sw3 + HH;
-    int* marks    = reinterpret_cast<int*>(sm + K::OFF_I);  // [2][128] slot -> segment, double buffered
-    int* slot_seg = marks + 2 * 128;                           // scan scratch
-    int* starts   = slot_seg + 128;                            // [2][132] first sample of the tile's segments
+    int* starts   = reinterpret_cast<int*>(sm + K::OFF_I);  // [2][132] first sample of the tile's segments
+    double* wsum  = reinterpret_cast<double*>(starts + 2 * 132);  // forward: per warp, its first run's sum
+    int* wseg     = reinterpret_cast<int*>(wsum + 4);              // .. that run's segment
+    int* wlast    = wseg + 4;                                      // .. and the segment of its last slot
     float* sval   = reinterpret_cast<float*>(sm + K::OFF_V);  // [2][128]: y halves / contributions
     float* sq     = reinterpret_cast<float*>(sm + K::OFF_Q);  // [2][6][128]: lu, lv, lw, weight, ray, row
     float* sred   = reinterpret_cast<float*>(sm + K::OFF_R);  // end-of-kernel reductions
@@ -403,27 +405,46 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     constexpr int KS128     = 128 / P::KI;
     auto x1_addr = [&](int b) -> uint32_t { return s_base + K::OFF_X1 + b * K::X1SZ; };
 
-    // Tile set-up in two stages, run one tile ahead inside the MMA waits:
-    // A: slot -> segment map (tile_seg, segment starts, block scan) into buffer b;
-    // B: the slot's segment record, its sample and the grid gather (first
-    //    thread of a sample only).
-    auto stage_a = [&](int64_t tl, int b) {
-        tile_slot_segments(tl * 128, a.tile_seg[tl], nseg, a.samp_off, marks + 128 * b, slot_seg, starts + 132 * b);
+    // Tile set-up, run one tile ahead inside the MMA waits.  The sample
+    // offsets of the 129 segments from tile_seg[tile] on (the segments that
+    // can own one of the tile's 128 slots) are fetched into registers a tile
+    // ahead of use (fetch_starts) and put into the starts buffer of that tile
+    // before a barrier (put_starts); stage_b then finds each slot's segment by
+    // a binary search over them, loads its segment record, draws its sample
+    // and gathers its grid features (first thread of a sample only).
+    auto fetch_starts = [&](int lo, int& oa, int& ob) {
+        oa = INT_MAX;
+        ob = INT_MAX;
+        if (t <= 128 && lo + t < nseg) oa = a.samp_off[lo + t];
+        if (TC_THREADS == 128 && t == 0 && lo + 128 < nseg) ob = a.samp_off[lo + 128];
+    };
+    auto put_starts = [&](int b, int oa, int ob) {
+        if (t <= 128) starts[132 * b + t] = oa;
+        if (TC_THREADS == 128 && t == 0) starts[132 * b + 128] = ob;
     };
     struct Slot
     {
         SlotSample q;
         float x[C];
         float dvw;  // backward: dL/dpred of the sample's ray times its weight (0 when invalid)
+        int seg;    // the slot's segment (-1 when the slot is past the last sample)
     };
-    auto stage_b = [&](int64_t tl, int b) -> Slot {
+    auto stage_b = [&](int64_t tl, int b, int lo) -> Slot {
         Slot o;
-        const int* mk    = marks + 128 * b;
-        const int seg    = mk[s];
+        const int* st    = starts + 132 * b;
         const int64_t gs = tl * 128 + s;
         const bool valid = gs < S;
+        // last segment starting at or before the slot: st[0] <= tl * 128 by
+        // construction of tile_seg, the segments past the last hold INT_MAX, and
+        // an empty segment shares its start with the next one
+        int i = 0;
+#pragma unroll
+        for (int d = 128; d > 0; d >>= 1)
+            if (i + d <= 128 && (int64_t)st[i + d] <= gs) i += d;
+        const int seg    = lo + i;
         const SegRec r   = a.segs[seg];
-        const int j      = valid ? (int)(gs - starts[132 * b + (seg - mk[0])]) : 0;
+        const int j      = valid ? (int)(gs - st[i]) : 0;
+        o.seg            = valid ? seg : -1;
         o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no,
                                             a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr);
         Corners kc;
@@ -529,12 +550,19 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     Slot cur;
     cur.q.valid = false;
     cur.dvw     = 0.0f;
+    cur.seg     = -1;
 #pragma unroll
     for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
+    int lo_next = 0;  // tile_seg of the next tile, loaded a tile ahead
     if (blockIdx.x < ntiles)
     {
-        stage_a(blockIdx.x, 0);
-        if (h == 0) cur = stage_b(blockIdx.x, 0);
+        const int lo0 = a.tile_seg[blockIdx.x];
+        int oa, ob;
+        fetch_starts(lo0, oa, ob);
+        put_starts(0, oa, ob);
+        __syncthreads();
+        if (h == 0) cur = stage_b(blockIdx.x, 0, lo0);
+        if (blockIdx.x + gridDim.x < ntiles) lo_next = a.tile_seg[blockIdx.x + gridDim.x];
         if constexpr (PIPE || FPIPE)
         {
             if (h == 0)
@@ -557,13 +585,18 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     {
         const int64_t nxt   = tile + gridDim.x;
         const bool has_next = nxt < ntiles;
-        const int buf       = it & 1;                 // slot map and slot data of this tile
+        const int buf       = it & 1;                 // segment starts and slot data of this tile
         const int xb        = it & 1;                 // [x | 1] buffer of this tile (pipelined)
-        const int* mark     = marks + 128 * buf;
         const SlotSample& q = cur.q;
         Slot nx;
         nx.q.valid = false;
         nx.dvw     = 0.0f;
+        nx.seg     = -1;
+        // the next tile's segment starts (stored before the barrier ahead of
+        // its stage_b) and the tile_seg of the one after it
+        int oa_nx = INT_MAX, ob_nx = INT_MAX;
+        if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
+        const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
         // ---- previous tile: dX and weight gradients done -> scatter dX
         if (BWD && wg_pending)
         {
@@ -592,7 +625,6 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 issue_l1(0);
             }
         }
-        if (has_next) stage_a(nxt, buf ^ 1);
         if (!(FPIPE ? wait_on(mbar_wg, phase_wg) : wait_on(mbar, phase)))
         {
             ok = false;
@@ -610,6 +642,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j + 8), z + 8);
         }
         if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
+        if (!BWD && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
         fence_smem_async();
         fence_before();
         __syncthreads();
@@ -621,7 +654,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                                                              sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
             mma_commit(mbar);
         }
-        if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1);
+        if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
         if constexpr (FPIPE)
         {
             // the next tile's layer 1, queued behind this tile's layer 2 (its
@@ -663,26 +696,41 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const float y = sb3[0] + sval[s] + (NH == 2 ? sval[128 + s] : 0.0f);
         if constexpr (!BWD)
         {
-            __syncthreads();  // both halves read the y parts before they are overwritten
+            // Per-segment sums of the contributions in f64, in a fixed order:
+            // a segmented suffix scan inside each warp (a segment's slots are
+            // consecutive), then a run's first slot adds the first runs of the
+            // following warps that continue it.  One f64 atomic per segment
+            // and tile (a segment spans at most two tiles: its two partials
+            // commute), so the projection is reproducible.
             if (h == 0)
             {
-                sval[s] = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
+                const float c = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
                 // proposal targets: contribution mass per eighth of the segment
-                if (a.seg_hist && q.valid)
-                    atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), sval[s]);
-            }
-            __syncthreads();
-            if (h == 0 && q.valid)
-            {
-                const int seg = mark[s];
-                if (s == 0 || mark[s - 1] != seg)
+                if (a.seg_hist && q.valid) atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), c);
+                const int seg = cur.seg;
+                double v      = (double)c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
                 {
-                    double sum = 0.0;  // f64: independent of where the tile boundary splits the segment
-                    for (int u = s; u < 128 && mark[u] == seg; ++u) sum += (double)sval[u];
-                    atomicAdd(a.partial + q.rm, sum);
+                    const double vn = __shfl_down_sync(0xffffffffu, v, o);
+                    const int sn    = __shfl_down_sync(0xffffffffu, seg, o);
+                    if (l + o < 32 && sn == seg) v += vn;
+                }
+                const int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+                if (l == 0)
+                {
+                    wsum[w] = v;
+                    wseg[w] = seg;
+                }
+                if (l == 31) wlast[w] = seg;
+                asm volatile("bar.sync 1, 128;" ::: "memory");  // the 128 first threads of the samples
+                const bool head = l == 0 ? (w == 0 || wlast[w - 1] != seg) : sp != seg;
+                if (head && q.valid)
+                {
+                    for (int ww = w + 1; ww < 4 && wseg[ww] == seg; ++ww) v += wsum[ww];
+                    atomicAdd(a.partial + q.rm, v);
                 }
             }
-            __syncthreads();
         }
         else
         {
@@ -708,6 +756,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
             }
+            if (has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -721,7 +770,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             if (has_next && h == 0)
             {
-                nx = stage_b(nxt, buf ^ 1);
+                nx = stage_b(nxt, buf ^ 1, lo_next);
                 // the next tile's [x | 1] buffer was last read by this CTA's
                 // previous tile, whose GEMMs have completed
                 if constexpr (PIPE)
@@ -770,6 +819,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             prev       = cur.q;
         }
         if (has_next && h == 0) cur = nx;
+        lo_next = lo_nx2;
     }
     // ---- drain: the last tile's dX and weight gradients
     if (BWD && wg_pending)

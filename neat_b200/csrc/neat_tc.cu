@@ -129,7 +129,7 @@ struct CfgPlan
     static constexpr int OFF_R  = OFF_Q + NQ * 4;
     static constexpr int NRED   = BWD ? 8 * HH : 0;
     static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
-    static constexpr int NEED   = OFF_M + 32;                 // two mbarriers + TMEM slot
+    static constexpr int NEED   = OFF_M + 32;                 // mbarriers at +0, +8, +24; TMEM slot at +16
 };
 
 template <int C, int PREC, bool BWD>
@@ -300,6 +300,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
     const int c0 = h * HALF;  // first hidden column of this thread
+    // The thread that issues every MMA.  A tcgen05.mma of these shapes holds
+    // its issuing thread for about its execution time (44-60 cycles), so with
+    // two threads per sample the issuer sits in the second half (warp 4),
+    // which has no slot set-up to do while the layer-2 and dH1 GEMMs run.
+    const bool issuer = t == (NH == 2 ? 128 : 0);
     float* sb2    = reinterpret_cast<float*>(sm + K::OFF_F);
     float* sw3    = sb2 + HH;
     float* sb3    = sw3 + HH;
@@ -318,7 +323,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     unsigned char* pAB = sm + K::OFF_AB;
     const uint32_t s_base  = smem_u32(sm);
     const uint32_t mbar    = smem_u32(mbar_p);      // layer GEMMs
-    const uint32_t mbar_wg = smem_u32(mbar_p + 1);  // dX and weight-gradient GEMMs
+    const uint32_t mbar_wg = smem_u32(mbar_p + 1);  // forward: layer 1 of the next tile (pipelined)
+    const uint32_t mbar_dx = smem_u32(mbar_p + 3);  // backward: dX
 
     // ---- decoder parameters: b2 / w3 / b3 in fp32, [W1 | b1] and W2 as MMA operand pieces
     using O = DecOff<C>;
@@ -361,6 +367,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     {
         mbar_init(mbar, 1);
         mbar_init(mbar_wg, 1);
+        mbar_init(mbar_dx, 1);
     }
     if (w == 0)
     {
@@ -383,6 +390,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     const uint32_t step_no = a.step_dev ? (uint32_t)*a.step_dev : a.step;
     uint32_t phase         = 0;
     uint32_t phase_wg      = 0;
+    uint32_t phase_dx      = 0;
     bool ok              = true;
     bool wg_pending      = false;
     bool wg_started      = false;
@@ -573,7 +581,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             fence_smem_async();
             fence_before();
             __syncthreads();
-            if (t == 0)
+            if (issuer)
             {
                 fence_after();
                 issue_l1(0);
@@ -597,16 +605,26 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         int oa_nx = INT_MAX, ob_nx = INT_MAX;
         if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
         const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
-        // ---- previous tile: dX and weight gradients done -> scatter dX
+        // ---- previous tile: dX done -> scatter it while its weight-gradient
+        //      GEMM runs (without the pipelined layer 1, also wait for that GEMM:
+        //      HB's [x | 1] columns are rewritten next)
         if (BWD && wg_pending)
         {
             wg_pending = false;
-            if (!wait_on(mbar_wg, phase_wg))
+            if (!wait_on(mbar_dx, phase_dx))
             {
                 ok = false;
                 break;
             }
             scatter_prev(buf ^ 1);
+            if constexpr (!PIPE)
+            {
+                if (!wait_on(mbar, phase))
+                {
+                    ok = false;
+                    break;
+                }
+            }
         }
         // ---- Z1 = [x | 1] . [W1 | b1]^T (already in flight when pipelined)
         if constexpr (!PIPE && !FPIPE)
@@ -619,7 +637,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             fence_smem_async();
             fence_before();
             __syncthreads();
-            if (t == 0)
+            if (issuer)
             {
                 fence_after();
                 issue_l1(0);
@@ -647,7 +665,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         fence_before();
         __syncthreads();
         // ---- Z2 = h1 . W2^T
-        if (t == 0)
+        if (issuer)
         {
             fence_after();
             gemm<PREC, KS64, HB::BYTES, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
@@ -665,7 +683,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 fence_smem_async();
                 fence_before();
                 __syncthreads();
-                if (t == 0)
+                if (issuer)
                 {
                     fence_after();
                     issue_l1(xb ^ 1);
@@ -761,7 +779,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             fence_before();
             __syncthreads();
             // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h) -> D2
-            if (t == 0)
+            if (issuer)
             {
                 fence_after();
                 gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
@@ -800,19 +818,23 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- dX = dz1 . [W1 | b1] -> D3;  [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4;
-            //      then (pipelined) the next tile's layer 1 -> D1
-            if (t == 0)
+            // ---- dX = dz1 . [W1 | b1] -> D3 (signals mbar_dx);
+            //      [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4, then (pipelined) the
+            //      next tile's layer 1 -> D1 (one signal on mbar for both)
+            if (issuer)
             {
                 fence_after();
                 gemm<PREC, KS64, AB::BYTES, 256, W1::BYTES, (P::KI / 8) * W1::RG>(
                     tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
                     idX, false);
+                mma_commit(mbar_dx);
                 gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, HB::BYTES, (P::KI / 8) * HB::RG>(
                     tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
                     wg_started);
-                mma_commit(mbar_wg);
-                if (PIPE && has_next) issue_l1(xb ^ 1);
+                if (PIPE && has_next)
+                    issue_l1(xb ^ 1);
+                else
+                    mma_commit(mbar);
             }
             wg_started = true;
             wg_pending = true;
@@ -824,10 +846,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     // ---- drain: the last tile's dX and weight gradients
     if (BWD && wg_pending)
     {
-        if (wait_on(mbar_wg, phase_wg))
+        if (wait_on(mbar_dx, phase_dx))
             scatter_prev((it - 1) & 1);
         else
             ok = false;
+        if (!wait_on(mbar, phase)) ok = false;
     }
     if (!ok) raise_status(a.status, NEAT_ERR_TIMEOUT);
     if constexpr (BWD)

@@ -510,22 +510,15 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                                                             sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
         mma_commit(FPIPE ? mbar_wg : mbar);
     };
-    // dX of the previous tile (TMEM D3), scattered with the trilinear weights;
-    // each thread of a sample takes 8 / NH corners.
-    SlotSample prev;
-    prev.valid = false;
-    auto scatter_prev = [&](int qb) {
-        float dxv[16];
-        tmem_ld16(tD3 + lane, dxv);
-        float dx[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) dx[c] = dxv[c];
+    // dX of this tile (registers), scattered with the trilinear weights; each
+    // thread of a sample takes 8 / NH corners.
+    auto scatter_dx = [&](const float (&dx)[C], const SlotSample& q, int qb) {
         float lu, lv, lw;
         int row;
         bool valid;
         if (h == 0)
         {
-            lu = prev.lu; lv = prev.lv; lw = prev.lw; row = prev.row; valid = prev.valid;
+            lu = q.lu; lv = q.lv; lw = q.lw; row = q.row; valid = q.valid;
         }
         else
         {
@@ -605,18 +598,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         int oa_nx = INT_MAX, ob_nx = INT_MAX;
         if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
         const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
-        // ---- previous tile: dX done -> scatter it while its weight-gradient
-        //      GEMM runs (without the pipelined layer 1, also wait for that GEMM:
-        //      HB's [x | 1] columns are rewritten next)
+        // ---- without the pipelined layer 1: the previous tile's weight-gradient
+        //      GEMM reads HB's [x | 1] columns, rewritten next
         if (BWD && wg_pending)
         {
             wg_pending = false;
-            if (!wait_on(mbar_dx, phase_dx))
-            {
-                ok = false;
-                break;
-            }
-            scatter_prev(buf ^ 1);
             if constexpr (!PIPE)
             {
                 if (!wait_on(mbar, phase))
@@ -818,9 +804,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- dX = dz1 . [W1 | b1] -> D3 (signals mbar_dx);
-            //      [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4, then (pipelined) the
-            //      next tile's layer 1 -> D1 (one signal on mbar for both)
+            // ---- dX = dz1 . [W1 | b1] -> D3, read into registers before the next
+            //      GEMM is issued (a TMEM load waits while the tensor core
+            //      accumulates into TMEM)
             if (issuer)
             {
                 fence_after();
@@ -828,6 +814,26 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
                     idX, false);
                 mma_commit(mbar_dx);
+            }
+            if (!wait_on(mbar_dx, phase_dx))
+            {
+                ok = false;
+                break;
+            }
+            float dx[C];
+            {
+                float dxv[16];
+                tmem_ld16(tD3 + lane, dxv);
+#pragma unroll
+                for (int c = 0; c < C; ++c) dx[c] = dxv[c];
+            }
+            fence_before();
+            __syncthreads();
+            // ---- [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4, then (pipelined) the
+            //      next tile's layer 1 -> D1 (one signal on mbar for both)
+            if (issuer)
+            {
+                fence_after();
                 gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, HB::BYTES, (P::KI / 8) * HB::RG>(
                     tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
                     wg_started);
@@ -838,18 +844,15 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             wg_started = true;
             wg_pending = true;
-            prev       = cur.q;
+            // ---- this tile's dX scattered while the weight-gradient GEMM runs
+            scatter_dx(dx, cur.q, buf);
         }
         if (has_next && h == 0) cur = nx;
         lo_next = lo_nx2;
     }
-    // ---- drain: the last tile's dX and weight gradients
+    // ---- drain: the last tile's weight gradients
     if (BWD && wg_pending)
     {
-        if (wait_on(mbar_dx, phase_dx))
-            scatter_prev((it - 1) & 1);
-        else
-            ok = false;
         if (!wait_on(mbar, phase)) ok = false;
     }
     if (!ok) raise_status(a.status, NEAT_ERR_TIMEOUT);

@@ -136,14 +136,19 @@ template <int C, int PREC, bool BWD>
 struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
 {
     using Base = CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
-    // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 [128, 192 + K1)
-    // weight gradients (h1 columns, then [x | 1] columns), D3 [192 + K1, 192 + 2 K1) dX
-    static constexpr uint32_t TMEM_COLS = BWD ? 256 : 128;
+    // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 [D4, D4 + 64 + K1)
+    // weight gradients (h1 columns, then [x | 1] columns), D3 [D4 + 64 + K1, D4 + 64 + 2 K1)
+    // dX.  The three-piece backward (one CTA per SM) also caches activations:
+    // [128,192) h2 = silu(z2 + b2), [192,256) sigmoid(z1), and D2 holds
+    // w3 silu'(z2 + b2) between the y and dz2 epilogues; its D4 starts at 256.
+    static constexpr bool CACHE         = BWD && PREC == BF16X3;
+    static constexpr int D4             = CACHE ? 256 : 128;
+    static constexpr uint32_t TMEM_COLS = CACHE ? 512 : (BWD ? 256 : 128);
     // pad so that no more CTAs share an SM than its 512 TMEM columns hold
     // (233472 B of shared memory per SM, 1 KB reserved per CTA)
     static constexpr int MIN_BYTES = 233472 / (512 / (int)TMEM_COLS + 1) - 1024 + 16;
     static constexpr int BYTES     = Base::NEED > MIN_BYTES ? Base::NEED : MIN_BYTES;
-    static_assert(!BWD || 192 + 2 * Base::K1 <= 256, "D4 and D3 must fit in the allocation");
+    static_assert(!BWD || D4 + 64 + 2 * Base::K1 <= (int)TMEM_COLS, "D4 and D3 must fit in the allocation");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
     static_assert((Base::OFF_I + 2 * 132 * 4) % 8 == 0, "f64 reduction scratch must be 8-byte aligned");
 };
@@ -232,6 +237,33 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
         if (clock64() - t0 > (1ll << 32)) return false;  // ~2 s at 2 GHz
     }
 }
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float v[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 32 lanes x 16 columns into registers without waiting; tmem_wait_ld()
+// before the values are used.
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t r[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
 {
@@ -382,7 +414,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + 128, tD3 = tmem + 192 + K::K1;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + K::D4, tD3 = tD4 + HH + K::K1;
+    const uint32_t tH2 = tmem + 128, tS1 = tmem + 192;  // activation cache (K::CACHE)
+    constexpr bool CACHE = K::CACHE;
 
     const int nseg         = (int)a.counters[0];
     const int64_t S        = a.counters[1];
@@ -640,11 +674,26 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         {
             float z[16];
             tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+            if constexpr (CACHE)
+            {
+                float sg[16];  // sigmoid(z1), kept for the dz1 epilogue
 #pragma unroll
-            for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+                for (int i = 0; i < 16; ++i)
+                {
+                    sg[i] = sigmoidf_(z[i]);
+                    z[i]  = z[i] * sg[i];
+                }
+                tmem_st16(tS1 + lane + c0 + 16 * j, sg);
+            }
+            else
+            {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+            }
             store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j), z);
             store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j + 8), z + 8);
         }
+        if constexpr (CACHE) tmem_wait_st();
         if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
         if (!BWD && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
         fence_smem_async();
@@ -689,10 +738,31 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             {
                 float z[16];
                 tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+                if constexpr (CACHE)
+                {
+                    // h2 and w3 silu'(z2 + b2), kept for the dz2 epilogue
+                    float g[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
-                    yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+                    for (int i = 0; i < 16; ++i)
+                    {
+                        const int col  = c0 + 16 * j + i;
+                        const float zz = z[i] + sb2[col];
+                        const float sg = sigmoidf_(zz);
+                        z[i]           = zz * sg;
+                        yp             = fmaf(z[i], sw3[col], yp);
+                        g[i]           = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                    }
+                    tmem_st16(tD2 + lane + c0 + 16 * j, g);
+                    tmem_st16(tH2 + lane + c0 + 16 * j, z);
+                }
+                else
+                {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+                }
             }
+            if constexpr (CACHE) tmem_wait_st();
             sval[h * 128 + s] = yp;
         }
         fence_before();
@@ -745,17 +815,33 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
-                float z[16];
-                tmem_ld16(tD2 + lane + c0 + 16 * j, z);
                 float d[16];
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
+                if constexpr (CACHE)
                 {
-                    const int col   = c0 + 16 * j + i;
-                    const float zz  = z[i] + sb2[col];
-                    const float sg  = sigmoidf_(zz);
-                    d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
-                    dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
+                    uint32_t g[16], h2[16];
+                    tmem_ld16_async(tD2 + lane + c0 + 16 * j, g);
+                    tmem_ld16_async(tH2 + lane + c0 + 16 * j, h2);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                    {
+                        d[i]            = dy * __uint_as_float(g[i]);
+                        dw3[16 * j + i] = fmaf(__uint_as_float(h2[i]), dy, dw3[16 * j + i]);
+                    }
+                }
+                else
+                {
+                    float z[16];
+                    tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                    {
+                        const int col   = c0 + 16 * j + i;
+                        const float zz  = z[i] + sb2[col];
+                        const float sg  = sigmoidf_(zz);
+                        d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                        dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
@@ -792,11 +878,29 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll 1
             for (int j = 0; j < HALF / 16; ++j)
             {
-                float g[16], z[16];
-                tmem_ld16(tD2 + lane + c0 + 16 * j, g);
-                tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+                float g[16];
+                if constexpr (CACHE)
+                {
+                    uint32_t gr[16], zr[16], sr[16];
+                    tmem_ld16_async(tD2 + lane + c0 + 16 * j, gr);
+                    tmem_ld16_async(tD1 + lane + c0 + 16 * j, zr);
+                    tmem_ld16_async(tS1 + lane + c0 + 16 * j, sr);
+                    tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
+                    for (int i = 0; i < 16; ++i)
+                    {
+                        const float z = __uint_as_float(zr[i]), sg = __uint_as_float(sr[i]);
+                        g[i]          = __uint_as_float(gr[i]) * (sg * (1.0f + z * (1.0f - sg)));
+                    }
+                }
+                else
+                {
+                    float z[16];
+                    tmem_ld16(tD2 + lane + c0 + 16 * j, g);
+                    tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
+                }
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E)
                     store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);

@@ -328,6 +328,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     constexpr int HALF       = HH / NH;   // hidden units per thread
     constexpr bool PIPE      = BWD && K::NX1 == 2;   // pipelined backward
     constexpr bool FPIPE     = !BWD && K::NX1 == 2;  // pipelined forward
+    // backward with two threads per sample: the next tile's placement runs in
+    // the layer-2 window, its gather in the dH1 window (one thread per sample:
+    // both in the dH1 window)
+    constexpr bool SPLIT_B   = BWD && TcThreads<PREC, BWD>::value == 256;
     extern __shared__ __align__(128) unsigned char sm[];
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
@@ -471,8 +475,16 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         float dvw;  // backward: dL/dpred of the sample's ray times its weight (0 when invalid)
         int seg;    // the slot's segment (-1 when the slot is past the last sample)
     };
-    auto stage_b = [&](int64_t tl, int b, int lo) -> Slot {
-        Slot o;
+    // stage_b in two parts: place_b (segment, record, sample position) and
+    // gather_b (grid features, dL/dpred); the backward runs them in different
+    // MMA windows.
+    struct Place
+    {
+        SlotSample q;
+        int seg;
+    };
+    auto place_b = [&](int64_t tl, int b, int lo) -> Place {
+        Place o;
         const int* st    = starts + 132 * b;
         const int64_t gs = tl * 128 + s;
         const bool valid = gs < S;
@@ -489,6 +501,13 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         o.seg            = valid ? seg : -1;
         o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no,
                                             a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr);
+        return o;
+    };
+    auto gather_b = [&](const Place& pl) -> Slot {
+        Slot o;
+        o.q              = pl.q;
+        o.seg            = pl.seg;
+        const bool valid = pl.q.valid;
         Corners kc;
         igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
         if (a.grid_bf16)
@@ -501,6 +520,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         o.dvw = (BWD && valid) ? a.dpred[o.q.ray] * o.q.weight : 0.0f;
         return o;
     };
+    auto stage_b = [&](int64_t tl, int b, int lo) -> Slot { return gather_b(place_b(tl, b, lo)); };
     // Row s of an [x | 1 | 0 ..] block: the separate buffer b (b >= 0) or the
     // columns [64, 64 + K1) of HB (b < 0).
     auto put_x1 = [&](const float (&xv)[C], int b) {
@@ -695,7 +715,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         }
         if constexpr (CACHE) tmem_wait_st();
         if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
-        if (!BWD && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+        if ((!BWD || SPLIT_B) && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
         fence_smem_async();
         fence_before();
         __syncthreads();
@@ -708,6 +728,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             mma_commit(mbar);
         }
         if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
+        // backward: the next tile's placement while layer 2 runs, its gather in the dH1 window
+        Place pl_nx;
+        if (SPLIT_B && has_next && h == 0) pl_nx = place_b(nxt, buf ^ 1, lo_next);
         if constexpr (FPIPE)
         {
             // the next tile's layer 1, queued behind this tile's layer 2 (its
@@ -846,7 +869,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
             }
-            if (has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+            if (!SPLIT_B && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -860,7 +883,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             if (has_next && h == 0)
             {
-                nx = stage_b(nxt, buf ^ 1, lo_next);
+                if constexpr (SPLIT_B)
+                    nx = gather_b(pl_nx);
+                else
+                    nx = stage_b(nxt, buf ^ 1, lo_next);
                 // the next tile's [x | 1] buffer was last read by this CTA's
                 // previous tile, whose GEMMs have completed
                 if constexpr (PIPE)

@@ -95,7 +95,11 @@ struct TcThreads
 };
 
 // Shared-memory plan of a tile CTA.  Backward HB rows hold [h1 | x | 1 0 ..]
-// (the weight-gradient B operand), forward HB rows h1.  NX1 separate [x | 1]
+// (the weight-gradient B operand), forward HB rows h1.  HB and [W1 | b1] keep
+// their BF16 pieces side by side along the columns (piece p at column
+// p * width), so that one MMA multiplies an A piece by several B pieces at
+// once (the weight-gradient and dX GEMMs; piece offsets HB_PC, W1_PC bytes);
+// W2, AB and the [x | 1] buffers keep whole pieces one after the other.  NX1 separate [x | 1]
 // buffers (0 or 2): with two, the next tile's layer-1 GEMM is issued from its
 // own buffer while the current tile is still in flight (backward: behind the
 // weight-gradient GEMM; forward: behind layer 2).
@@ -108,16 +112,19 @@ struct CfgPlan
     static constexpr int K1     = ((XW + 1 + 15) / 16) * 16;  // layer-1 K: [x | 1 | 0 ..]
     static constexpr int ONE    = XW;                         // column of the 1 in [x | 1]
     static constexpr int NW     = HH + K1;                    // weight-gradient N: [h1 | x | 1 ..]
-    using HB                    = Buf<PREC, 128, BWD ? NW : HH>;  // the forward keeps h1 only
+    static constexpr int HBW    = BWD ? NW : HH;              // HB columns of one piece (forward: h1 only)
+    using HB                    = Buf<PREC, 128, P::PIECES * HBW>;
     using X1                    = Buf<PREC, 128, K1>;         // [x | 1 | 0 ..] rows
     using AB                    = Buf<PREC, 128, 2 * HH>;     // [dz2 | dz1] rows
     using W2                    = Buf<PREC, HH, HH>;
-    using W1                    = Buf<PREC, HH, K1>;          // [h][x | 1]: W1 | b1
+    using W1                    = Buf<PREC, HH, P::PIECES * K1>;  // [h][x | 1]: W1 | b1
+    static constexpr int HB_PC  = HBW * 16;                   // byte offset of the next piece's columns
+    static constexpr int W1_PC  = K1 * 16;
     static constexpr int NH     = TcThreads<PREC, BWD>::value / 128;
     static constexpr int OFF_W2 = 0;
     static constexpr int OFF_W1 = OFF_W2 + P::PIECES * W2::BYTES;
-    static constexpr int OFF_HB = OFF_W1 + P::PIECES * W1::BYTES;
-    static constexpr int OFF_X1 = OFF_HB + P::PIECES * HB::BYTES;
+    static constexpr int OFF_HB = OFF_W1 + W1::BYTES;
+    static constexpr int OFF_X1 = OFF_HB + HB::BYTES;
     static constexpr int X1SZ   = P::PIECES * X1::BYTES;      // one [x | 1] buffer, all pieces
     static constexpr int OFF_AB = OFF_X1 + NX1 * X1SZ;
     static constexpr int OFF_F  = OFF_AB + (BWD ? P::PIECES * AB::BYTES : 0);
@@ -136,19 +143,27 @@ template <int C, int PREC, bool BWD>
 struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
 {
     using Base = CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
-    // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 [D4, D4 + 64 + K1)
-    // weight gradients (h1 columns, then [x | 1] columns), D3 [D4 + 64 + K1, D4 + 64 + 2 K1)
-    // dX.  The three-piece backward (one CTA per SM) also caches activations:
+    // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 weight
+    // gradients (h1 columns, then [x | 1] columns; with WCAT one such block per B
+    // piece, summed at the end), D3 dX (one block of K1 columns per B piece).
+    // The three-piece backward (one CTA per SM) also caches activations:
     // [128,192) h2 = silu(z2 + b2), [192,256) sigmoid(z1), and D2 holds
-    // w3 silu'(z2 + b2) between the y and dz2 epilogues; its D4 starts at 256.
+    // w3 silu'(z2 + b2) between the y and dz2 epilogues; its D4 starts at 256
+    // and its dX reuses the sigmoid(z1) columns when they fit (read before dX).
+    using PP                            = Prec<PREC>;
     static constexpr bool CACHE         = BWD && PREC == BF16X3;
+    static constexpr bool WCAT          = PP::PIECES * Base::NW <= 256;  // one MMA per A piece
     static constexpr int D4             = CACHE ? 256 : 128;
+    static constexpr int D4W            = WCAT ? PP::PIECES * Base::NW : Base::NW;
+    static constexpr int D3W            = PP::PIECES * Base::K1;
+    static constexpr int D3             = (CACHE && D3W <= 64) ? 192 : D4 + D4W;
     static constexpr uint32_t TMEM_COLS = CACHE ? 512 : (BWD ? 256 : 128);
     // pad so that no more CTAs share an SM than its 512 TMEM columns hold
     // (233472 B of shared memory per SM, 1 KB reserved per CTA)
     static constexpr int MIN_BYTES = 233472 / (512 / (int)TMEM_COLS + 1) - 1024 + 16;
     static constexpr int BYTES     = Base::NEED > MIN_BYTES ? Base::NEED : MIN_BYTES;
-    static_assert(!BWD || D4 + 64 + 2 * Base::K1 <= (int)TMEM_COLS, "D4 and D3 must fit in the allocation");
+    static_assert(!BWD || (D4 + D4W <= (int)TMEM_COLS && D3 + D3W <= (int)TMEM_COLS), "D4 and D3 must fit");
+    static_assert(!BWD || D3 + D3W <= D4 || D3 >= D4 + D4W, "dX must not overlap the weight gradients");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
     static_assert((Base::OFF_I + 2 * 132 * 4) % 8 == 0, "f64 reduction scratch must be 8-byte aligned");
 };
@@ -207,6 +222,26 @@ __device__ __forceinline__ void gemm(uint32_t d, uint64_t da, uint64_t db, uint3
             const uint64_t a = da + (uint64_t)((prod_a(p) * A_PIECE + kk * A_K) >> 4);
             const uint64_t b = db + (uint64_t)((prod_b(p) * B_PIECE + kk * B_K) >> 4);
             mma<1>(d, a, b, idesc, (acc0 || p || kk) ? 1u : 0u);
+        }
+}
+
+// A GEMM whose B operand holds its pieces side by side along N (NB columns
+// each): per A piece p one MMA against B pieces 0 .. PIECES-1-p (N = (PIECES -
+// p) NB), which puts the products of piece orders <= 2 into PIECES column
+// blocks of D (block q: the products with B piece q; the reader sums them).
+// Half the MMAs of gemm(), and each A piece is read once per K step.
+template <int PREC, int KS, int A_PIECE, int A_K, int B_K, int NB, int A_MN, int B_MN>
+__device__ __forceinline__ void gemm_cat(uint32_t d, uint64_t da, uint64_t db, bool acc0)
+{
+    constexpr int NP = Prec<PREC>::PIECES;
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+        for (int kk = 0; kk < KS; ++kk)
+        {
+            const uint64_t a = da + (uint64_t)((p * A_PIECE + kk * A_K) >> 4);
+            const uint64_t b = db + (uint64_t)((kk * B_K) >> 4);
+            mma<1>(d, a, b, make_idesc(Prec<PREC>::FMT, A_MN, B_MN, 128, (NP - p) * NB), (acc0 || p || kk) ? 1u : 0u);
         }
 }
 
@@ -389,7 +424,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             r           = col < C ? a.decoder[O::W1 + hr * C + col] : (col == K::ONE ? a.decoder[O::b1 + hr] : 0.0f);
             off         = W1::off(hr, col);
             dst         = pW1;
-            piece_bytes = W1::BYTES;
+            piece_bytes = K::W1_PC;
         }
 #pragma unroll
         for (int p = 0; p < P::PIECES; ++p)
@@ -418,7 +453,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + K::D4, tD3 = tD4 + HH + K::K1;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + K::D4, tD3 = tmem + K::D3;
     const uint32_t tH2 = tmem + 128, tS1 = tmem + 192;  // activation cache (K::CACHE)
     constexpr bool CACHE = K::CACHE;
 
@@ -444,7 +479,6 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     };
     constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);       // layers 1 and 2
     constexpr uint32_t idH  = make_idesc(P::FMT, 0, 1, 128, HH);       // dH1
-    constexpr uint32_t idX  = make_idesc(P::FMT, 0, 1, 128, K::K1);    // dX
     constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);    // weight gradients
     constexpr int KS1       = K::K1 / P::KI;
     constexpr int KS64      = HH / P::KI;
@@ -525,7 +559,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     // columns [64, 64 + K1) of HB (b < 0).
     auto put_x1 = [&](const float (&xv)[C], int b) {
         unsigned char* base = b >= 0 ? sm + K::OFF_X1 + b * K::X1SZ : pHB;
-        const int pbytes    = b >= 0 ? X1::BYTES : HB::BYTES;
+        const int pbytes    = b >= 0 ? X1::BYTES : K::HB_PC;
 #pragma unroll
         for (int cc = 0; cc < K::K1; cc += P::E)
         {
@@ -557,11 +591,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     // pending on mbar, and one barrier must never run two phases ahead of its waiter)
     auto issue_l1 = [&](int b) {
         if constexpr (PIPE || FPIPE)
-            gemm<PREC, KS1, X1::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(x1_addr(b), 128, X1::RG),
-                                                            sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
+            gemm<PREC, KS1, X1::BYTES, 256, K::W1_PC, 256>(tD1, sdesc(x1_addr(b), 128, X1::RG),
+                                                           sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
         else
-            gemm<PREC, KS1, HB::BYTES, 256, W1::BYTES, 256>(tD1, sdesc(s_base + K::OFF_HB + (HH / 8) * 128, 128, HB::RG),
-                                                            sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
+            gemm<PREC, KS1, K::HB_PC, 256, K::W1_PC, 256>(tD1, sdesc(s_base + K::OFF_HB + (HH / 8) * 128, 128, HB::RG),
+                                                          sdesc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
         mma_commit(FPIPE ? mbar_wg : mbar);
     };
     // dX of this tile (registers), scattered with the trilinear weights; each
@@ -710,8 +744,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
             }
-            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j), z);
-            store_chunk<PREC>(pHB, HB::BYTES, HB::off(s, c0 + 16 * j + 8), z + 8);
+            store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
+            store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
         }
         if constexpr (CACHE) tmem_wait_st();
         if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
@@ -723,7 +757,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         if (issuer)
         {
             fence_after();
-            gemm<PREC, KS64, HB::BYTES, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+            gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
                                                              sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
             mma_commit(mbar);
         }
@@ -940,9 +974,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (issuer)
             {
                 fence_after();
-                gemm<PREC, KS64, AB::BYTES, 256, W1::BYTES, (P::KI / 8) * W1::RG>(
+                gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W1::RG, K::K1, 0, 1>(
                     tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
-                    idX, false);
+                    false);
                 mma_commit(mbar_dx);
             }
             if (!wait_on(mbar_dx, phase_dx))
@@ -952,10 +986,18 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             float dx[C];
             {
-                float dxv[16];
-                tmem_ld16(tD3 + lane, dxv);
+                uint32_t dxv[P::PIECES][16];  // one column block per [W1 | b1] piece
 #pragma unroll
-                for (int c = 0; c < C; ++c) dx[c] = dxv[c];
+                for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD3 + lane + p * K::K1, dxv[p]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                {
+                    float v = __uint_as_float(dxv[0][c]);
+#pragma unroll
+                    for (int p = 1; p < P::PIECES; ++p) v += __uint_as_float(dxv[p][c]);
+                    dx[c] = v;
+                }
             }
             fence_before();
             __syncthreads();
@@ -964,9 +1006,13 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (issuer)
             {
                 fence_after();
-                gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, HB::BYTES, (P::KI / 8) * HB::RG>(
-                    tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
-                    wg_started);
+                if constexpr (K::WCAT)
+                    gemm_cat<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, (P::KI / 8) * HB::RG, K::NW, 1, 1>(
+                        tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), wg_started);
+                else
+                    gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, K::HB_PC, (P::KI / 8) * HB::RG>(
+                        tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
+                        wg_started);
                 if (PIPE && has_next)
                     issue_l1(xb ^ 1);
                 else
@@ -998,7 +1044,18 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         {
             float v[16];
             if (wg_started && ok)
+            {
                 tmem_ld16(tD4 + lane + 16 * j, v);
+                if constexpr (K::WCAT)  // one column block per HB piece
+#pragma unroll
+                    for (int p = 1; p < P::PIECES; ++p)
+                    {
+                        float u[16];
+                        tmem_ld16(tD4 + lane + p * K::NW + 16 * j, u);
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) v[i] += u[i];
+                    }
+            }
             else
 #pragma unroll
                 for (int i = 0; i < 16; ++i) v[i] = 0.0f;

@@ -131,8 +131,8 @@ struct CfgPlan
     static constexpr int NF     = 2 * HH + 4;                 // b2, w3, b3
     static constexpr int OFF_I  = OFF_F + NF * 4;             // [2][132] segment starts, then 4 f64 + 8 int
     static constexpr int OFF_V  = OFF_I + 2 * 132 * 4 + 4 * 8 + 8 * 4;
-    static constexpr int OFF_Q  = OFF_V + 2 * 128 * 4;        // [2][6][128] slot data for the second thread
-    static constexpr int NQ     = (BWD && NH == 2) ? 2 * 6 * 128 : 0;
+    static constexpr int OFF_Q  = OFF_V + 2 * 128 * 4;        // [2][6][128] slot data for the second thread (both directions)
+    static constexpr int NQ     = (NH == 2) ? 2 * 6 * 128 : 0;
     static constexpr int OFF_R  = OFF_Q + NQ * 4;
     static constexpr int NRED   = BWD ? 8 * HH : 0;
     static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
@@ -367,6 +367,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     // the layer-2 window, its gather in the dH1 window (one thread per sample:
     // both in the dH1 window)
     constexpr bool SPLIT_B   = BWD && TcThreads<PREC, BWD>::value == 256;
+    // forward with two threads per sample: its own loop (below)
+    constexpr bool FSPLIT    = FPIPE && TcThreads<PREC, BWD>::value == 256;
     extern __shared__ __align__(128) unsigned char sm[];
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
@@ -636,77 +638,46 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         }
     };
 
-    Slot cur;
-    cur.q.valid = false;
-    cur.dvw     = 0.0f;
-    cur.seg     = -1;
-#pragma unroll
-    for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
-    int lo_next = 0;  // tile_seg of the next tile, loaded a tile ahead
-    if (blockIdx.x < ntiles)
-    {
-        const int lo0 = a.tile_seg[blockIdx.x];
-        int oa, ob;
-        fetch_starts(lo0, oa, ob);
-        put_starts(0, oa, ob);
-        __syncthreads();
-        if (h == 0) cur = stage_b(blockIdx.x, 0, lo0);
-        if (blockIdx.x + gridDim.x < ntiles) lo_next = a.tile_seg[blockIdx.x + gridDim.x];
-        if constexpr (PIPE || FPIPE)
-        {
-            if (h == 0)
-            {
-                put_x1(cur.x, 0);
-                put_q(cur, 0);
-            }
-            fence_smem_async();
-            fence_before();
-            __syncthreads();
-            if (issuer)
-            {
-                fence_after();
-                issue_l1(0);
-            }
-        }
-    }
     int it = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it)
+    if constexpr (FSPLIT)
     {
-        const int64_t nxt   = tile + gridDim.x;
-        const bool has_next = nxt < ntiles;
-        const int buf       = it & 1;                 // segment starts and slot data of this tile
-        const int xb        = it & 1;                 // [x | 1] buffer of this tile (pipelined)
-        const SlotSample& q = cur.q;
-        Slot nx;
-        nx.q.valid = false;
-        nx.dvw     = 0.0f;
-        nx.seg     = -1;
-        // the next tile's segment starts (stored before the barrier ahead of
-        // its stage_b) and the tile_seg of the one after it
-        int oa_nx = INT_MAX, ob_nx = INT_MAX;
-        if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
-        const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
-        // ---- without the pipelined layer 1: the previous tile's weight-gradient
-        //      GEMM reads HB's [x | 1] columns, rewritten next
-        if (BWD && wg_pending)
+        // Forward with two threads per sample.  Per tile: layer 1 (issued a
+        // tile ahead) -> h1 epilogue -> layer 2, while the first half gathers
+        // the next tile's grid features (placed a tile earlier) and queues its
+        // layer 1 -> y epilogue -> the second half sums the contributions per
+        // segment (slot records of the first half, in sq) while the first half
+        // places the tile after next.
+        auto put_sr = [&](const Slot& sl, int qb) {
+            float* qd       = sq + qb * 6 * 128;
+            qd[0 * 128 + s] = sl.q.weight;
+            qd[1 * 128 + s] = sl.q.u;
+            qd[2 * 128 + s] = __int_as_float(sl.q.rm);
+            qd[3 * 128 + s] = __int_as_float(sl.seg);
+        };
+        const int64_t T0 = blockIdx.x, G = gridDim.x;
+        Place pl_next;  // first half: placement of the next tile
+        pl_next.q.valid = false;
+        pl_next.seg     = -1;
+        int lo_n2       = 0;  // tile_seg two tiles ahead
+        if (T0 < ntiles)
         {
-            wg_pending = false;
-            if constexpr (!PIPE)
+            const int lo0 = a.tile_seg[T0];
+            int oa, ob;
+            fetch_starts(lo0, oa, ob);
+            put_starts(0, oa, ob);
+            const bool has1 = T0 + G < ntiles;
+            const int lo1   = has1 ? a.tile_seg[T0 + G] : 0;
+            if (has1)
             {
-                if (!wait_on(mbar, phase))
-                {
-                    ok = false;
-                    break;
-                }
+                fetch_starts(lo1, oa, ob);
+                put_starts(1, oa, ob);
             }
-        }
-        // ---- Z1 = [x | 1] . [W1 | b1]^T (already in flight when pipelined)
-        if constexpr (!PIPE && !FPIPE)
-        {
+            __syncthreads();
             if (h == 0)
             {
-                put_x1(cur.x, -1);
-                put_q(cur, buf);
+                const Slot c0s = gather_b(place_b(T0, 0, lo0));
+                put_x1(c0s.x, 0);
+                put_sr(c0s, 0);
             }
             fence_smem_async();
             fence_before();
@@ -716,130 +687,103 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 fence_after();
                 issue_l1(0);
             }
+            if (has1 && h == 0) pl_next = place_b(T0 + G, 1, lo1);
+            if (T0 + 2 * G < ntiles) lo_n2 = a.tile_seg[T0 + 2 * G];
         }
-        if (!(FPIPE ? wait_on(mbar_wg, phase_wg) : wait_on(mbar, phase)))
+        for (int64_t tile = T0; tile < ntiles; tile += G, ++it)
         {
-            ok = false;
-            break;
-        }
-        // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
-#pragma unroll 1
-        for (int j = 0; j < HALF / 16; ++j)
-        {
-            float z[16];
-            tmem_ld16(tD1 + lane + c0 + 16 * j, z);
-            if constexpr (CACHE)
+            const int64_t nxt = tile + G, nxt2 = nxt + G;
+            const bool has_next = nxt < ntiles, has_next2 = nxt2 < ntiles;
+            const int buf       = it & 1;  // [x | 1] buffer and slot records of this tile
+            // segment starts of the tile after next (stored before the barrier
+            // ahead of its placement) and the tile_seg of the one after that
+            int oa2 = INT_MAX, ob2 = INT_MAX;
+            if (has_next2) fetch_starts(lo_n2, oa2, ob2);
+            const int lo_n3 = nxt2 + G < ntiles ? a.tile_seg[nxt2 + G] : 0;
+            if (!wait_on(mbar_wg, phase_wg))
             {
-                float sg[16];  // sigmoid(z1), kept for the dz1 epilogue
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
-                {
-                    sg[i] = sigmoidf_(z[i]);
-                    z[i]  = z[i] * sg[i];
-                }
-                tmem_st16(tS1 + lane + c0 + 16 * j, sg);
+                ok = false;
+                break;
             }
-            else
+            // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
+#pragma unroll 1
+            for (int j = 0; j < HALF / 16; ++j)
             {
+                float z[16];
+                tmem_ld16(tD1 + lane + c0 + 16 * j, z);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
+                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
             }
-            store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
-            store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
-        }
-        if constexpr (CACHE) tmem_wait_st();
-        if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
-        if ((!BWD || SPLIT_B) && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
-        fence_smem_async();
-        fence_before();
-        __syncthreads();
-        // ---- Z2 = h1 . W2^T
-        if (issuer)
-        {
-            fence_after();
-            gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
-                                                             sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
-            mma_commit(mbar);
-        }
-        if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
-        // backward: the next tile's placement while layer 2 runs, its gather in the dH1 window
-        Place pl_nx;
-        if (SPLIT_B && has_next && h == 0) pl_nx = place_b(nxt, buf ^ 1, lo_next);
-        if constexpr (FPIPE)
-        {
-            // the next tile's layer 1, queued behind this tile's layer 2 (its
-            // [x | 1] buffer was last read by the layer 1 of two tiles ago)
+            fence_smem_async();
+            fence_before();
+            __syncthreads();
+            // ---- Z2 = h1 . W2^T
+            if (issuer)
+            {
+                fence_after();
+                gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                                                                sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
+                mma_commit(mbar);
+            }
+            // ---- the next tile: grid gather, slot records, layer 1 (queued behind layer 2)
             if (has_next)
             {
-                if (h == 0) put_x1(nx.x, xb ^ 1);
+                if (h == 0)
+                {
+                    const Slot nx = gather_b(pl_next);
+                    put_x1(nx.x, buf ^ 1);
+                    put_sr(nx, buf ^ 1);
+                }
                 fence_smem_async();
                 fence_before();
                 __syncthreads();
                 if (issuer)
                 {
                     fence_after();
-                    issue_l1(xb ^ 1);
+                    issue_l1(buf ^ 1);
                 }
             }
-        }
-        if (!wait_on(mbar, phase))
-        {
-            ok = false;
-            break;
-        }
-        // ---- epilogue 1: y = b3 + sum over both halves
-        {
-            float yp = 0.0f;
-#pragma unroll 1
-            for (int j = 0; j < HALF / 16; ++j)
+            if (!wait_on(mbar, phase))
             {
-                float z[16];
-                tmem_ld16(tD2 + lane + c0 + 16 * j, z);
-                if constexpr (CACHE)
+                ok = false;
+                break;
+            }
+            // ---- epilogue 1: this thread's part of y
+            {
+                float yp = 0.0f;
+#pragma unroll 1
+                for (int j = 0; j < HALF / 16; ++j)
                 {
-                    // h2 and w3 silu'(z2 + b2), kept for the dz2 epilogue
-                    float g[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                    {
-                        const int col  = c0 + 16 * j + i;
-                        const float zz = z[i] + sb2[col];
-                        const float sg = sigmoidf_(zz);
-                        z[i]           = zz * sg;
-                        yp             = fmaf(z[i], sw3[col], yp);
-                        g[i]           = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
-                    }
-                    tmem_st16(tD2 + lane + c0 + 16 * j, g);
-                    tmem_st16(tH2 + lane + c0 + 16 * j, z);
-                }
-                else
-                {
+                    float z[16];
+                    tmem_ld16(tD2 + lane + c0 + 16 * j, z);
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                         yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
                 }
+                sval[h * 128 + s] = yp;
             }
-            if constexpr (CACHE) tmem_wait_st();
-            sval[h * 128 + s] = yp;
-        }
-        fence_before();
-        __syncthreads();
-        const float y = sb3[0] + sval[s] + (NH == 2 ? sval[128 + s] : 0.0f);
-        if constexpr (!BWD)
-        {
-            // Per-segment sums of the contributions in f64, in a fixed order:
-            // a segmented suffix scan inside each warp (a segment's slots are
-            // consecutive), then a run's first slot adds the first runs of the
-            // following warps that continue it.  One f64 atomic per segment
-            // and tile (a segment spans at most two tiles: its two partials
-            // commute), so the projection is reproducible.
-            if (h == 0)
+            if (has_next2) put_starts(buf, oa2, ob2);
+            fence_before();
+            __syncthreads();
+            if (h == 1)
             {
-                const float c = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
+                // Per-segment sums of the contributions in f64, in a fixed order:
+                // a segmented suffix scan inside each warp (a segment's slots are
+                // consecutive), then a run's first slot adds the first runs of the
+                // following warps that continue it.  One f64 atomic per segment
+                // and tile (a segment spans at most two tiles: its two partials
+                // commute), so the projection is reproducible.
+                const float* qd = sq + buf * 6 * 128;
+                const int seg   = __float_as_int(qd[3 * 128 + s]);
+                const bool vld  = seg >= 0;
+                const int rm    = __float_as_int(qd[2 * 128 + s]);
+                const float y   = sb3[0] + sval[s] + sval[128 + s];
+                const float c   = vld ? softplusf_(y, a.beta) * qd[s] : 0.0f;
                 // proposal targets: contribution mass per eighth of the segment
-                if (a.seg_hist && q.valid) atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), c);
-                const int seg = cur.seg;
-                double v      = (double)c;
+                if (a.seg_hist && vld) atomicAdd(a.seg_hist + 8 * (int64_t)rm + min(7, (int)(qd[128 + s] * 8.0f)), c);
+                double v = (double)c;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1)
                 {
@@ -848,85 +792,173 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     if (l + o < 32 && sn == seg) v += vn;
                 }
                 const int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+                const int wq = w & 3;
                 if (l == 0)
                 {
-                    wsum[w] = v;
-                    wseg[w] = seg;
+                    wsum[wq] = v;
+                    wseg[wq] = seg;
                 }
-                if (l == 31) wlast[w] = seg;
-                asm volatile("bar.sync 1, 128;" ::: "memory");  // the 128 first threads of the samples
-                const bool head = l == 0 ? (w == 0 || wlast[w - 1] != seg) : sp != seg;
-                if (head && q.valid)
+                if (l == 31) wlast[wq] = seg;
+                asm volatile("bar.sync 1, 128;" ::: "memory");  // the 128 second threads of the samples
+                const bool head = l == 0 ? (wq == 0 || wlast[wq - 1] != seg) : sp != seg;
+                if (head && vld)
                 {
-                    for (int ww = w + 1; ww < 4 && wseg[ww] == seg; ++ww) v += wsum[ww];
-                    atomicAdd(a.partial + q.rm, v);
+                    for (int ww = wq + 1; ww < 4 && wseg[ww] == seg; ++ww) v += wsum[ww];
+                    atomicAdd(a.partial + rm, v);
+                }
+            }
+            else if (has_next2)
+            {
+                pl_next = place_b(nxt2, buf, lo_n2);
+            }
+            lo_n2 = lo_n3;
+        }
+    }
+    else
+    {
+        Slot cur;
+        cur.q.valid = false;
+        cur.dvw     = 0.0f;
+        cur.seg     = -1;
+    #pragma unroll
+        for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
+        int lo_next = 0;  // tile_seg of the next tile, loaded a tile ahead
+        if (blockIdx.x < ntiles)
+        {
+            const int lo0 = a.tile_seg[blockIdx.x];
+            int oa, ob;
+            fetch_starts(lo0, oa, ob);
+            put_starts(0, oa, ob);
+            __syncthreads();
+            if (h == 0) cur = stage_b(blockIdx.x, 0, lo0);
+            if (blockIdx.x + gridDim.x < ntiles) lo_next = a.tile_seg[blockIdx.x + gridDim.x];
+            if constexpr (PIPE || FPIPE)
+            {
+                if (h == 0)
+                {
+                    put_x1(cur.x, 0);
+                    put_q(cur, 0);
+                }
+                fence_smem_async();
+                fence_before();
+                __syncthreads();
+                if (issuer)
+                {
+                    fence_after();
+                    issue_l1(0);
                 }
             }
         }
-        else
+        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it)
         {
-            const float dvw = h == 0 ? cur.dvw : sq[buf * 6 * 128 + 3 * 128 + s];
-            const float dy  = dvw * softplus_grad(y, a.beta);
-            if (h == 0) db3 += dy;
-            // dz2 (this thread's columns) -> AB[:, c0 ..]; dW3 += h2 dy
-#pragma unroll
+            const int64_t nxt   = tile + gridDim.x;
+            const bool has_next = nxt < ntiles;
+            const int buf       = it & 1;                 // segment starts and slot data of this tile
+            const int xb        = it & 1;                 // [x | 1] buffer of this tile (pipelined)
+            const SlotSample& q = cur.q;
+            Slot nx;
+            nx.q.valid = false;
+            nx.dvw     = 0.0f;
+            nx.seg     = -1;
+            // the next tile's segment starts (stored before the barrier ahead of
+            // its stage_b) and the tile_seg of the one after it
+            int oa_nx = INT_MAX, ob_nx = INT_MAX;
+            if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
+            const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
+            // ---- without the pipelined layer 1: the previous tile's weight-gradient
+            //      GEMM reads HB's [x | 1] columns, rewritten next
+            if (BWD && wg_pending)
+            {
+                wg_pending = false;
+                if constexpr (!PIPE)
+                {
+                    if (!wait_on(mbar, phase))
+                    {
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+            // ---- Z1 = [x | 1] . [W1 | b1]^T (already in flight when pipelined)
+            if constexpr (!PIPE && !FPIPE)
+            {
+                if (h == 0)
+                {
+                    put_x1(cur.x, -1);
+                    put_q(cur, buf);
+                }
+                fence_smem_async();
+                fence_before();
+                __syncthreads();
+                if (issuer)
+                {
+                    fence_after();
+                    issue_l1(0);
+                }
+            }
+            if (!(FPIPE ? wait_on(mbar_wg, phase_wg) : wait_on(mbar, phase)))
+            {
+                ok = false;
+                break;
+            }
+            // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
+    #pragma unroll 1
             for (int j = 0; j < HALF / 16; ++j)
             {
-                float d[16];
+                float z[16];
+                tmem_ld16(tD1 + lane + c0 + 16 * j, z);
                 if constexpr (CACHE)
                 {
-                    uint32_t g[16], h2[16];
-                    tmem_ld16_async(tD2 + lane + c0 + 16 * j, g);
-                    tmem_ld16_async(tH2 + lane + c0 + 16 * j, h2);
-                    tmem_wait_ld();
-#pragma unroll
+                    float sg[16];  // sigmoid(z1), kept for the dz1 epilogue
+    #pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
-                        d[i]            = dy * __uint_as_float(g[i]);
-                        dw3[16 * j + i] = fmaf(__uint_as_float(h2[i]), dy, dw3[16 * j + i]);
+                        sg[i] = sigmoidf_(z[i]);
+                        z[i]  = z[i] * sg[i];
                     }
+                    tmem_st16(tS1 + lane + c0 + 16 * j, sg);
                 }
                 else
                 {
-                    float z[16];
-                    tmem_ld16(tD2 + lane + c0 + 16 * j, z);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                    {
-                        const int col   = c0 + 16 * j + i;
-                        const float zz  = z[i] + sb2[col];
-                        const float sg  = sigmoidf_(zz);
-                        d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
-                        dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
-                    }
+    #pragma unroll
+                    for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
                 }
-#pragma unroll
-                for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
+                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
+                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
             }
-            if (!SPLIT_B && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+            if constexpr (CACHE) tmem_wait_st();
+            if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
+            if ((!BWD || SPLIT_B) && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
             fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h) -> D2
+            // ---- Z2 = h1 . W2^T
             if (issuer)
             {
                 fence_after();
-                gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
-                    tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), idH, false);
+                gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                                                                 sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 mma_commit(mbar);
             }
-            if (has_next && h == 0)
+            if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
+            // backward: the next tile's placement while layer 2 runs, its gather in the dH1 window
+            Place pl_nx;
+            if (SPLIT_B && has_next && h == 0) pl_nx = place_b(nxt, buf ^ 1, lo_next);
+            if constexpr (FPIPE)
             {
-                if constexpr (SPLIT_B)
-                    nx = gather_b(pl_nx);
-                else
-                    nx = stage_b(nxt, buf ^ 1, lo_next);
-                // the next tile's [x | 1] buffer was last read by this CTA's
-                // previous tile, whose GEMMs have completed
-                if constexpr (PIPE)
+                // the next tile's layer 1, queued behind this tile's layer 2 (its
+                // [x | 1] buffer was last read by the layer 1 of two tiles ago)
+                if (has_next)
                 {
-                    put_x1(nx.x, xb ^ 1);
-                    put_q(nx, buf ^ 1);
+                    if (h == 0) put_x1(nx.x, xb ^ 1);
+                    fence_smem_async();
+                    fence_before();
+                    __syncthreads();
+                    if (issuer)
+                    {
+                        fence_after();
+                        issue_l1(xb ^ 1);
+                    }
                 }
             }
             if (!wait_on(mbar, phase))
@@ -934,97 +966,245 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 ok = false;
                 break;
             }
-            // ---- epilogue 2: dz1 = dH1 silu'(Z1) (this thread's columns) -> AB[:, 64 + c0 ..]
-#pragma unroll 1
-            for (int j = 0; j < HALF / 16; ++j)
+            // ---- epilogue 1: y = b3 + sum over both halves
             {
-                float g[16];
-                if constexpr (CACHE)
-                {
-                    uint32_t gr[16], zr[16], sr[16];
-                    tmem_ld16_async(tD2 + lane + c0 + 16 * j, gr);
-                    tmem_ld16_async(tD1 + lane + c0 + 16 * j, zr);
-                    tmem_ld16_async(tS1 + lane + c0 + 16 * j, sr);
-                    tmem_wait_ld();
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                    {
-                        const float z = __uint_as_float(zr[i]), sg = __uint_as_float(sr[i]);
-                        g[i]          = __uint_as_float(gr[i]) * (sg * (1.0f + z * (1.0f - sg)));
-                    }
-                }
-                else
+                float yp = 0.0f;
+    #pragma unroll 1
+                for (int j = 0; j < HALF / 16; ++j)
                 {
                     float z[16];
-                    tmem_ld16(tD2 + lane + c0 + 16 * j, g);
-                    tmem_ld16(tD1 + lane + c0 + 16 * j, z);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
+                    tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+                    if constexpr (CACHE)
+                    {
+                        // h2 and w3 silu'(z2 + b2), kept for the dz2 epilogue
+                        float g[16];
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                        {
+                            const int col  = c0 + 16 * j + i;
+                            const float zz = z[i] + sb2[col];
+                            const float sg = sigmoidf_(zz);
+                            z[i]           = zz * sg;
+                            yp             = fmaf(z[i], sw3[col], yp);
+                            g[i]           = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                        }
+                        tmem_st16(tD2 + lane + c0 + 16 * j, g);
+                        tmem_st16(tH2 + lane + c0 + 16 * j, z);
+                    }
+                    else
+                    {
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                            yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+                    }
                 }
-#pragma unroll
-                for (int i = 0; i < 16; i += P::E)
-                    store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
+                if constexpr (CACHE) tmem_wait_st();
+                sval[h * 128 + s] = yp;
             }
-            fence_smem_async();
             fence_before();
             __syncthreads();
-            // ---- dX = dz1 . [W1 | b1] -> D3, read into registers before the next
-            //      GEMM is issued (a TMEM load waits while the tensor core
-            //      accumulates into TMEM)
-            if (issuer)
+            const float y = sb3[0] + sval[s] + (NH == 2 ? sval[128 + s] : 0.0f);
+            if constexpr (!BWD)
             {
-                fence_after();
-                gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W1::RG, K::K1, 0, 1>(
-                    tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
-                    false);
-                mma_commit(mbar_dx);
-            }
-            if (!wait_on(mbar_dx, phase_dx))
-            {
-                ok = false;
-                break;
-            }
-            float dx[C];
-            {
-                uint32_t dxv[P::PIECES][16];  // one column block per [W1 | b1] piece
-#pragma unroll
-                for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD3 + lane + p * K::K1, dxv[p]);
-                tmem_wait_ld();
-#pragma unroll
-                for (int c = 0; c < C; ++c)
+                // Per-segment sums of the contributions in f64, in a fixed order:
+                // a segmented suffix scan inside each warp (a segment's slots are
+                // consecutive), then a run's first slot adds the first runs of the
+                // following warps that continue it.  One f64 atomic per segment
+                // and tile (a segment spans at most two tiles: its two partials
+                // commute), so the projection is reproducible.
+                if (h == 0)
                 {
-                    float v = __uint_as_float(dxv[0][c]);
-#pragma unroll
-                    for (int p = 1; p < P::PIECES; ++p) v += __uint_as_float(dxv[p][c]);
-                    dx[c] = v;
+                    const float c = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
+                    // proposal targets: contribution mass per eighth of the segment
+                    if (a.seg_hist && q.valid) atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), c);
+                    const int seg = cur.seg;
+                    double v      = (double)c;
+    #pragma unroll
+                    for (int o = 1; o < 32; o <<= 1)
+                    {
+                        const double vn = __shfl_down_sync(0xffffffffu, v, o);
+                        const int sn    = __shfl_down_sync(0xffffffffu, seg, o);
+                        if (l + o < 32 && sn == seg) v += vn;
+                    }
+                    const int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+                    if (l == 0)
+                    {
+                        wsum[w] = v;
+                        wseg[w] = seg;
+                    }
+                    if (l == 31) wlast[w] = seg;
+                    asm volatile("bar.sync 1, 128;" ::: "memory");  // the 128 first threads of the samples
+                    const bool head = l == 0 ? (w == 0 || wlast[w - 1] != seg) : sp != seg;
+                    if (head && q.valid)
+                    {
+                        for (int ww = w + 1; ww < 4 && wseg[ww] == seg; ++ww) v += wsum[ww];
+                        atomicAdd(a.partial + q.rm, v);
+                    }
                 }
             }
-            fence_before();
-            __syncthreads();
-            // ---- [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4, then (pipelined) the
-            //      next tile's layer 1 -> D1 (one signal on mbar for both)
-            if (issuer)
+            else
             {
-                fence_after();
-                if constexpr (K::WCAT)
-                    gemm_cat<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, (P::KI / 8) * HB::RG, K::NW, 1, 1>(
-                        tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), wg_started);
-                else
-                    gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, K::HB_PC, (P::KI / 8) * HB::RG>(
-                        tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
-                        wg_started);
-                if (PIPE && has_next)
-                    issue_l1(xb ^ 1);
-                else
+                const float dvw = h == 0 ? cur.dvw : sq[buf * 6 * 128 + 3 * 128 + s];
+                const float dy  = dvw * softplus_grad(y, a.beta);
+                if (h == 0) db3 += dy;
+                // dz2 (this thread's columns) -> AB[:, c0 ..]; dW3 += h2 dy
+    #pragma unroll
+                for (int j = 0; j < HALF / 16; ++j)
+                {
+                    float d[16];
+                    if constexpr (CACHE)
+                    {
+                        uint32_t g[16], h2[16];
+                        tmem_ld16_async(tD2 + lane + c0 + 16 * j, g);
+                        tmem_ld16_async(tH2 + lane + c0 + 16 * j, h2);
+                        tmem_wait_ld();
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                        {
+                            d[i]            = dy * __uint_as_float(g[i]);
+                            dw3[16 * j + i] = fmaf(__uint_as_float(h2[i]), dy, dw3[16 * j + i]);
+                        }
+                    }
+                    else
+                    {
+                        float z[16];
+                        tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                        {
+                            const int col   = c0 + 16 * j + i;
+                            const float zz  = z[i] + sb2[col];
+                            const float sg  = sigmoidf_(zz);
+                            d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                            dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
+                        }
+                    }
+    #pragma unroll
+                    for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
+                }
+                if (!SPLIT_B && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+                fence_smem_async();
+                fence_before();
+                __syncthreads();
+                // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h) -> D2
+                if (issuer)
+                {
+                    fence_after();
+                    gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
+                        tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), idH, false);
                     mma_commit(mbar);
+                }
+                if (has_next && h == 0)
+                {
+                    if constexpr (SPLIT_B)
+                        nx = gather_b(pl_nx);
+                    else
+                        nx = stage_b(nxt, buf ^ 1, lo_next);
+                    // the next tile's [x | 1] buffer was last read by this CTA's
+                    // previous tile, whose GEMMs have completed
+                    if constexpr (PIPE)
+                    {
+                        put_x1(nx.x, xb ^ 1);
+                        put_q(nx, buf ^ 1);
+                    }
+                }
+                if (!wait_on(mbar, phase))
+                {
+                    ok = false;
+                    break;
+                }
+                // ---- epilogue 2: dz1 = dH1 silu'(Z1) (this thread's columns) -> AB[:, 64 + c0 ..]
+    #pragma unroll 1
+                for (int j = 0; j < HALF / 16; ++j)
+                {
+                    float g[16];
+                    if constexpr (CACHE)
+                    {
+                        uint32_t gr[16], zr[16], sr[16];
+                        tmem_ld16_async(tD2 + lane + c0 + 16 * j, gr);
+                        tmem_ld16_async(tD1 + lane + c0 + 16 * j, zr);
+                        tmem_ld16_async(tS1 + lane + c0 + 16 * j, sr);
+                        tmem_wait_ld();
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                        {
+                            const float z = __uint_as_float(zr[i]), sg = __uint_as_float(sr[i]);
+                            g[i]          = __uint_as_float(gr[i]) * (sg * (1.0f + z * (1.0f - sg)));
+                        }
+                    }
+                    else
+                    {
+                        float z[16];
+                        tmem_ld16(tD2 + lane + c0 + 16 * j, g);
+                        tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+    #pragma unroll
+                        for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
+                    }
+    #pragma unroll
+                    for (int i = 0; i < 16; i += P::E)
+                        store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
+                }
+                fence_smem_async();
+                fence_before();
+                __syncthreads();
+                // ---- dX = dz1 . [W1 | b1] -> D3, read into registers before the next
+                //      GEMM is issued (a TMEM load waits while the tensor core
+                //      accumulates into TMEM)
+                if (issuer)
+                {
+                    fence_after();
+                    gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W1::RG, K::K1, 0, 1>(
+                        tD3, sdesc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG), sdesc(s_base + K::OFF_W1, W1::RG, 128),
+                        false);
+                    mma_commit(mbar_dx);
+                }
+                if (!wait_on(mbar_dx, phase_dx))
+                {
+                    ok = false;
+                    break;
+                }
+                float dx[C];
+                {
+                    uint32_t dxv[P::PIECES][16];  // one column block per [W1 | b1] piece
+    #pragma unroll
+                    for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD3 + lane + p * K::K1, dxv[p]);
+                    tmem_wait_ld();
+    #pragma unroll
+                    for (int c = 0; c < C; ++c)
+                    {
+                        float v = __uint_as_float(dxv[0][c]);
+    #pragma unroll
+                        for (int p = 1; p < P::PIECES; ++p) v += __uint_as_float(dxv[p][c]);
+                        dx[c] = v;
+                    }
+                }
+                fence_before();
+                __syncthreads();
+                // ---- [dW2 ; dW1 | db] += AB^T . [h1 | x 1] -> D4, then (pipelined) the
+                //      next tile's layer 1 -> D1 (one signal on mbar for both)
+                if (issuer)
+                {
+                    fence_after();
+                    if constexpr (K::WCAT)
+                        gemm_cat<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, (P::KI / 8) * HB::RG, K::NW, 1, 1>(
+                            tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), wg_started);
+                    else
+                        gemm<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, K::HB_PC, (P::KI / 8) * HB::RG>(
+                            tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
+                            wg_started);
+                    if (PIPE && has_next)
+                        issue_l1(xb ^ 1);
+                    else
+                        mma_commit(mbar);
+                }
+                wg_started = true;
+                wg_pending = true;
+                // ---- this tile's dX scattered while the weight-gradient GEMM runs
+                scatter_dx(dx, cur.q, buf);
             }
-            wg_started = true;
-            wg_pending = true;
-            // ---- this tile's dX scattered while the weight-gradient GEMM runs
-            scatter_dx(dx, cur.q, buf);
+            if (has_next && h == 0) cur = nx;
+            lo_next = lo_nx2;
         }
-        if (has_next && h == 0) cur = nx;
-        lo_next = lo_nx2;
     }
     // ---- drain: the last tile's weight gradients
     if (BWD && wg_pending)

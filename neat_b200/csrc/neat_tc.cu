@@ -820,7 +820,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         cur.q.valid = false;
         cur.dvw     = 0.0f;
         cur.seg     = -1;
-    #pragma unroll
+#pragma unroll
         for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
         int lo_next = 0;  // tile_seg of the next tile, loaded a tile ahead
         if (blockIdx.x < ntiles)
@@ -902,7 +902,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 break;
             }
             // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
-    #pragma unroll 1
+#pragma unroll 1
             for (int j = 0; j < HALF / 16; ++j)
             {
                 float z[16];
@@ -910,7 +910,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 if constexpr (CACHE)
                 {
                     float sg[16];  // sigmoid(z1), kept for the dz1 epilogue
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
                         sg[i] = sigmoidf_(z[i]);
@@ -920,7 +920,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 }
                 else
                 {
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
                 }
                 store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
@@ -969,7 +969,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             // ---- epilogue 1: y = b3 + sum over both halves
             {
                 float yp = 0.0f;
-    #pragma unroll 1
+#pragma unroll 1
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float z[16];
@@ -978,7 +978,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     {
                         // h2 and w3 silu'(z2 + b2), kept for the dz2 epilogue
                         float g[16];
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i)
                         {
                             const int col  = c0 + 16 * j + i;
@@ -993,7 +993,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     }
                     else
                     {
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i)
                             yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
                     }
@@ -1019,7 +1019,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     if (a.seg_hist && q.valid) atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), c);
                     const int seg = cur.seg;
                     double v      = (double)c;
-    #pragma unroll
+#pragma unroll
                     for (int o = 1; o < 32; o <<= 1)
                     {
                         const double vn = __shfl_down_sync(0xffffffffu, v, o);
@@ -1048,7 +1048,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 const float dy  = dvw * softplus_grad(y, a.beta);
                 if (h == 0) db3 += dy;
                 // dz2 (this thread's columns) -> AB[:, c0 ..]; dW3 += h2 dy
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float d[16];
@@ -1058,7 +1058,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         tmem_ld16_async(tD2 + lane + c0 + 16 * j, g);
                         tmem_ld16_async(tH2 + lane + c0 + 16 * j, h2);
                         tmem_wait_ld();
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i)
                         {
                             d[i]            = dy * __uint_as_float(g[i]);
@@ -1069,7 +1069,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     {
                         float z[16];
                         tmem_ld16(tD2 + lane + c0 + 16 * j, z);
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i)
                         {
                             const int col   = c0 + 16 * j + i;
@@ -1079,7 +1079,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                             dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
                         }
                     }
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
                 }
                 if (!SPLIT_B && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
@@ -1114,7 +1114,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     break;
                 }
                 // ---- epilogue 2: dz1 = dH1 silu'(Z1) (this thread's columns) -> AB[:, 64 + c0 ..]
-    #pragma unroll 1
+#pragma unroll 1
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float g[16];
@@ -1125,7 +1125,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         tmem_ld16_async(tD1 + lane + c0 + 16 * j, zr);
                         tmem_ld16_async(tS1 + lane + c0 + 16 * j, sr);
                         tmem_wait_ld();
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i)
                         {
                             const float z = __uint_as_float(zr[i]), sg = __uint_as_float(sr[i]);
@@ -1137,10 +1137,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         float z[16];
                         tmem_ld16(tD2 + lane + c0 + 16 * j, g);
                         tmem_ld16(tD1 + lane + c0 + 16 * j, z);
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
                     }
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 16; i += P::E)
                         store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
                 }
@@ -1166,14 +1166,14 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 float dx[C];
                 {
                     uint32_t dxv[P::PIECES][16];  // one column block per [W1 | b1] piece
-    #pragma unroll
+#pragma unroll
                     for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD3 + lane + p * K::K1, dxv[p]);
                     tmem_wait_ld();
-    #pragma unroll
+#pragma unroll
                     for (int c = 0; c < C; ++c)
                     {
                         float v = __uint_as_float(dxv[0][c]);
-    #pragma unroll
+#pragma unroll
                         for (int p = 1; p < P::PIECES; ++p) v += __uint_as_float(dxv[p][c]);
                         dx[c] = v;
                     }

@@ -369,6 +369,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     constexpr bool SPLIT_B   = BWD && TcThreads<PREC, BWD>::value == 256;
     // forward with two threads per sample: its own loop (below)
     constexpr bool FSPLIT    = FPIPE && TcThreads<PREC, BWD>::value == 256;
+    // epilogue chunk loops unrolled where the registers allow (two threads per sample, backward)
+    constexpr int UNR        = SPLIT_B ? HALF / 16 : 1;
     extern __shared__ __align__(128) unsigned char sm[];
     // thread t: sample (TMEM lane) s = t & 127, hidden part h = t >> 7
     const int t = threadIdx.x, w = t >> 5, l = t & 31, s = t & 127, h = t >> 7;
@@ -902,7 +904,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 break;
             }
             // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
-#pragma unroll 1
+#pragma unroll UNR
             for (int j = 0; j < HALF / 16; ++j)
             {
                 float z[16];
@@ -969,7 +971,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             // ---- epilogue 1: y = b3 + sum over both halves
             {
                 float yp = 0.0f;
-#pragma unroll 1
+#pragma unroll UNR
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float z[16];
@@ -1114,7 +1116,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     break;
                 }
                 // ---- epilogue 2: dz1 = dH1 silu'(Z1) (this thread's columns) -> AB[:, 64 + c0 ..]
-#pragma unroll 1
+#pragma unroll UNR
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float g[16];

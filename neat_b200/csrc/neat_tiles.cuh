@@ -395,29 +395,44 @@ __device__ __forceinline__ void gather_cl(const float* __restrict__ grid, int64_
                                           float x[C])
 {
     const int64_t base = row * (int64_t)G * G * G;
-#pragma unroll
-    for (int c = 0; c < C; ++c) x[c] = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
+    if constexpr (C % 4 == 0)
     {
-        const float* p = grid + (base + corner_cell(k, q, G, G)) * C;
-        const float wq = k.w[q];
-        if constexpr (C % 4 == 0)
-        {
+        // one round of 8 loads (one per corner) per 4 channels; each channel
+        // still accumulates its corners in order 0..7
+        const float* pq[8];
 #pragma unroll
-            for (int c4 = 0; c4 < C / 4; ++c4)
+        for (int q = 0; q < 8; ++q) pq[q] = grid + (base + corner_cell(k, q, G, G)) * C;
+#pragma unroll
+        for (int c4 = 0; c4 < C / 4; ++c4)
+        {
+            float4 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = __ldg(reinterpret_cast<const float4*>(pq[q]) + c4);
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
             {
-                const float4 v = __ldg(reinterpret_cast<const float4*>(p) + c4);
-                x[4 * c4 + 0]  = fmaf(v.x, wq, x[4 * c4 + 0]);
-                x[4 * c4 + 1]  = fmaf(v.y, wq, x[4 * c4 + 1]);
-                x[4 * c4 + 2]  = fmaf(v.z, wq, x[4 * c4 + 2]);
-                x[4 * c4 + 3]  = fmaf(v.w, wq, x[4 * c4 + 3]);
+                a0 = fmaf(v[q].x, k.w[q], a0);
+                a1 = fmaf(v[q].y, k.w[q], a1);
+                a2 = fmaf(v[q].z, k.w[q], a2);
+                a3 = fmaf(v[q].w, k.w[q], a3);
             }
+            x[4 * c4]     = a0;
+            x[4 * c4 + 1] = a1;
+            x[4 * c4 + 2] = a2;
+            x[4 * c4 + 3] = a3;
         }
-        else
-        {
+    }
+    else
+    {
 #pragma unroll
-            for (int c = 0; c < C; ++c) x[c] = fmaf(__ldg(p + c), wq, x[c]);
+        for (int c = 0; c < C; ++c) x[c] = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            const float* p = grid + (base + corner_cell(k, q, G, G)) * C;
+#pragma unroll
+            for (int c = 0; c < C; ++c) x[c] = fmaf(__ldg(p + c), k.w[q], x[c]);
         }
     }
 }

@@ -88,14 +88,16 @@ __device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool v
 }
 
 // slot_sample for a full warp of consecutive slots: each lane draws the
-// jitter of its own sample only and takes t of samples j-1 and j+1 from its
+// jitter of its own sample and takes t of samples j-1 and j+1 from its
 // neighbour lanes (consecutive slots of one segment are consecutive samples);
-// lanes 0 and 31 draw the one neighbour outside the warp when they need it.
-// Same values as slot_sample when cdf is null; with a proposal CDF (8 bin
-// ends of this slot's segment) the positions come from its inverse.  All 32
-// lanes must call it.
+// lanes 0 and 31 need the one neighbour outside the warp, which every lane
+// draws alongside its own (two independent Philox chains that interleave,
+// instead of a second chain on two diverged lanes).  Same values as
+// slot_sample when cdf is null; with a proposal CDF (8 bin ends of this slot's
+// segment) the positions come from its inverse.  u (the stratified CDF
+// position) only when want_u.  All 32 lanes must call it.
 __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, bool valid, bool jitter, uint64_t seed,
-                                                       uint32_t step, const float* cdf = nullptr)
+                                                       uint32_t step, const float* cdf = nullptr, bool want_u = true)
 {
     SlotSample q;
     q.valid = valid;
@@ -108,32 +110,23 @@ __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, b
         c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
         c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
     }
-    auto t_of = [&](int jj) -> float {
-        const float a = jitter_a(jitter, seed, step, r.ray, r.local_base + jj);
-        return cdf ? proposal_t(r.tmin, r.tmax, r.n, jj, a, c) : seg_t(r.tmin, r.step, jj, a);
-    };
-    const float a = jitter_a(jitter, seed, step, r.ray, r.local_base + j);
-    const float t = cdf ? proposal_t(r.tmin, r.tmax, r.n, j, a, c) : seg_t(r.tmin, r.step, j, a);
     const int lane = threadIdx.x & 31;
+    const int jx   = lane == 0 ? j - 1 : j + 1;  // the neighbour a warp edge lane cannot shuffle in
+    const float a  = jitter_a(jitter, seed, step, r.ray, r.local_base + j);
+    const float ax = jitter_a(jitter, seed, step, r.ray, r.local_base + jx);
+    const float t  = cdf ? proposal_t(r.tmin, r.tmax, r.n, j, a, c) : seg_t(r.tmin, r.step, j, a);
+    const float tx = cdf ? proposal_t(r.tmin, r.tmax, r.n, jx, ax, c) : seg_t(r.tmin, r.step, jx, ax);
     float tp       = __shfl_up_sync(0xffffffffu, t, 1);
     float tn       = __shfl_down_sync(0xffffffffu, t, 1);
-    const bool np  = j > 0 && lane == 0;
-    const bool nn  = j < r.n - 1 && lane == 31;
-    if (np || nn)
-    {
-        const float tx = t_of(np ? j - 1 : j + 1);
-        if (np)
-            tp = tx;
-        else
-            tn = tx;
-    }
+    if (j > 0 && lane == 0) tp = tx;
+    if (j < r.n - 1 && lane == 31) tn = tx;
     const float lo = j == 0 ? r.tmin : __fmul_rn(__fadd_rn(tp, t), 0.5f);
     const float hi = j == r.n - 1 ? r.tmax : __fmul_rn(__fadd_rn(tn, t), 0.5f);
     q.lu           = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], t)), r.mn[0], r.mx[0]);
     q.lv           = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], t)), r.mn[1], r.mx[1]);
     q.lw           = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], t)), r.mn[2], r.mx[2]);
     q.weight       = q.valid ? __fsub_rn(hi, lo) : 0.0f;
-    q.u            = __fdiv_rn(__fadd_rn((float)j, a), (float)r.n);
+    q.u            = want_u ? __fdiv_rn(__fadd_rn((float)j, a), (float)r.n) : 0.0f;
     q.ray          = r.ray;
     q.rm           = r.rm;
     q.row          = r.row;

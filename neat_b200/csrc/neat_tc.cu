@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         const int j      = valid ? (int)(gs - st[i]) : 0;
         o.seg            = valid ? seg : -1;
         o.q              = slot_sample_warp(r, j, valid, a.jitter != 0, a.seed, step_no,
-                                            a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr);
+                                            a.seg_cdf ? a.seg_cdf + 8 * (int64_t)seg : nullptr, a.seg_hist != nullptr);
         return o;
     };
     auto gather_b = [&](const Place& pl) -> Slot {

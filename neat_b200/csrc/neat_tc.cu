@@ -99,10 +99,13 @@ struct TcThreads
 // their BF16 pieces side by side along the columns (piece p at column
 // p * width), so that one MMA multiplies an A piece by several B pieces at
 // once (the weight-gradient and dX GEMMs; piece offsets HB_PC, W1_PC bytes);
-// W2, AB and the [x | 1] buffers keep whole pieces one after the other.  NX1 separate [x | 1]
-// buffers (0 or 2): with two, the next tile's layer-1 GEMM is issued from its
-// own buffer while the current tile is still in flight (backward: behind the
-// weight-gradient GEMM; forward: behind layer 2).
+// W2, AB and the [x | 1] buffer keep whole pieces one after the other.  NX1
+// separate [x | 1] buffers (0 or 1): with one, the next tile's layer-1 GEMM is
+// issued from it while the current tile is still in flight (backward: behind
+// the weight-gradient GEMM; forward: behind layer 2); its rows are written
+// after the current tile's layer 1 has completed.  TA (forward, two threads
+// per sample, C <= 8): h1 is the A operand of layer 2 straight from TMEM (no
+// HB; its BF16 pieces are written with tcgen05.st instead of shared stores).
 template <int C, int PREC, bool BWD, int NX1_>
 struct CfgPlan
 {
@@ -112,7 +115,8 @@ struct CfgPlan
     static constexpr int K1     = ((XW + 1 + 15) / 16) * 16;  // layer-1 K: [x | 1 | 0 ..]
     static constexpr int ONE    = XW;                         // column of the 1 in [x | 1]
     static constexpr int NW     = HH + K1;                    // weight-gradient N: [h1 | x | 1 ..]
-    static constexpr int HBW    = BWD ? NW : HH;              // HB columns of one piece (forward: h1 only)
+    static constexpr bool TA    = !BWD && TcThreads<PREC, BWD>::value == 256 && C <= 8;
+    static constexpr int HBW    = BWD ? NW : (TA ? 0 : HH);   // HB columns of one piece (forward: h1 only)
     using HB                    = Buf<PREC, 128, P::PIECES * HBW>;
     using X1                    = Buf<PREC, 128, K1>;         // [x | 1 | 0 ..] rows
     using AB                    = Buf<PREC, 128, 2 * HH>;     // [dz2 | dz1] rows
@@ -140,9 +144,9 @@ struct CfgPlan
 };
 
 template <int C, int PREC, bool BWD>
-struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>
+struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 1>::NEED <= 232448) ? 1 : 0>
 {
-    using Base = CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 2 : 0>;
+    using Base = CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 1>::NEED <= 232448) ? 1 : 0>;
     // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 weight
     // gradients (h1 columns, then [x | 1] columns; with WCAT one such block per B
     // piece, summed at the end), D3 dX (one block of K1 columns per B piece).
@@ -157,7 +161,10 @@ struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 2>::NEED <= 232448) ? 
     static constexpr int D4W            = WCAT ? PP::PIECES * Base::NW : Base::NW;
     static constexpr int D3W            = PP::PIECES * Base::K1;
     static constexpr int D3             = (CACHE && D3W <= 64) ? 192 : D4 + D4W;
-    static constexpr uint32_t TMEM_COLS = CACHE ? 512 : (BWD ? 256 : 128);
+    // forward with TA: h1 pieces as the layer-2 A operand at [128, 128 + 32 PIECES)
+    // (two BF16 per 32-bit column)
+    static constexpr int TA_COL         = 128;
+    static constexpr uint32_t TMEM_COLS = CACHE ? 512 : ((BWD || Base::TA) ? 256 : 128);
     // pad so that no more CTAs share an SM than its 512 TMEM columns hold
     // (233472 B of shared memory per SM, 1 KB reserved per CTA)
     static constexpr int MIN_BYTES = 233472 / (512 / (int)TMEM_COLS + 1) - 1024 + 16;
@@ -201,6 +208,16 @@ __device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t
         "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
+// tcgen05.mma with A in TMEM (K-major, two BF16 per 32-bit column) and B in
+// shared memory.
+__device__ __forceinline__ void mma_ta(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc));
+}
+
 __device__ __forceinline__ void mma_commit(uint32_t mbar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
@@ -222,6 +239,23 @@ __device__ __forceinline__ void gemm(uint32_t d, uint64_t da, uint64_t db, uint3
             const uint64_t a = da + (uint64_t)((prod_a(p) * A_PIECE + kk * A_K) >> 4);
             const uint64_t b = db + (uint64_t)((prod_b(p) * B_PIECE + kk * B_K) >> 4);
             mma<1>(d, a, b, idesc, (acc0 || p || kk) ? 1u : 0u);
+        }
+}
+
+// gemm() with A in TMEM: piece p of A at column offset p * A_PIECE_COLS, K
+// steps of 16 elements = 8 columns.
+template <int PREC, int KS, int A_PIECE_COLS, int B_PIECE, int B_K>
+__device__ __forceinline__ void gemm_ta(uint32_t d, uint32_t a_tmem, uint64_t db, uint32_t idesc, bool acc0)
+{
+    constexpr int NPROD = PREC == 1 ? 6 : 1;
+#pragma unroll
+    for (int p = 0; p < NPROD; ++p)
+#pragma unroll
+        for (int kk = 0; kk < KS; ++kk)
+        {
+            const uint32_t a = a_tmem + (uint32_t)(prod_a(p) * A_PIECE_COLS + kk * 8);
+            const uint64_t b = db + (uint64_t)((prod_b(p) * B_PIECE + kk * B_K) >> 4);
+            mma_ta(d, a, b, idesc, (acc0 || p || kk) ? 1u : 0u);
         }
 }
 
@@ -283,6 +317,12 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float v[16])
         "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
         "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
         : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t v[8])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
@@ -361,8 +401,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     constexpr int TC_THREADS = TcThreads<PREC, BWD>::value;
     constexpr int NH         = K::NH;     // threads per sample
     constexpr int HALF       = HH / NH;   // hidden units per thread
-    constexpr bool PIPE      = BWD && K::NX1 == 2;   // pipelined backward
-    constexpr bool FPIPE     = !BWD && K::NX1 == 2;  // pipelined forward
+    constexpr bool PIPE      = BWD && K::NX1 == 1;   // pipelined backward
+    constexpr bool FPIPE     = !BWD && K::NX1 == 1;  // pipelined forward
     // backward with two threads per sample: the next tile's placement runs in
     // the layer-2 window, its gather in the dH1 window (one thread per sample:
     // both in the dH1 window)
@@ -707,7 +747,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 ok = false;
                 break;
             }
-            // ---- h1 = silu(Z1), this thread's columns -> HB[:, c0 .. c0 + HALF)
+            // ---- h1 = silu(Z1), this thread's columns -> layer-2 A operand: TMEM
+            //      (TA: BF16 pieces, two per column) or HB[:, c0 .. c0 + HALF)
 #pragma unroll 1
             for (int j = 0; j < HALF / 16; ++j)
             {
@@ -715,9 +756,30 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 tmem_ld16(tD1 + lane + c0 + 16 * j, z);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
-                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
-                store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
+                if constexpr (K::TA)
+                {
+#pragma unroll
+                    for (int p = 0; p < P::PIECES; ++p)
+                    {
+                        uint32_t v[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                        {
+                            const __nv_bfloat162 b = __floats2bfloat162_rn(z[2 * i], z[2 * i + 1]);
+                            v[i]                   = *reinterpret_cast<const uint32_t*>(&b);
+                            z[2 * i] -= __low2float(b);  // exact: the remainder of a bf16 rounding
+                            z[2 * i + 1] -= __high2float(b);
+                        }
+                        tmem_st8(tmem + lane + K::TA_COL + 32 * p + (c0 + 16 * j) / 2, v);
+                    }
+                }
+                else
+                {
+                    store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
+                    store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
+                }
             }
+            if constexpr (K::TA) tmem_wait_st();
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -725,8 +787,12 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (issuer)
             {
                 fence_after();
-                gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
-                                                                sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
+                if constexpr (K::TA)
+                    gemm_ta<PREC, KS64, 32, W2::BYTES, 256>(tD2, tmem + K::TA_COL,
+                                                            sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
+                else
+                    gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                                                                    sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 mma_commit(mbar);
             }
             // ---- the next tile: grid gather, slot records, layer 1 (queued behind layer 2)
@@ -735,7 +801,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 if (h == 0)
                 {
                     const Slot nx = gather_b(pl_next);
-                    put_x1(nx.x, buf ^ 1);
+                    put_x1(nx.x, 0);
                     put_sr(nx, buf ^ 1);
                 }
                 fence_smem_async();
@@ -744,7 +810,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 if (issuer)
                 {
                     fence_after();
-                    issue_l1(buf ^ 1);
+                    issue_l1(0);
                 }
             }
             if (!wait_on(mbar, phase))
@@ -856,7 +922,6 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             const int64_t nxt   = tile + gridDim.x;
             const bool has_next = nxt < ntiles;
             const int buf       = it & 1;                 // segment starts and slot data of this tile
-            const int xb        = it & 1;                 // [x | 1] buffer of this tile (pipelined)
             const SlotSample& q = cur.q;
             Slot nx;
             nx.q.valid = false;
@@ -948,18 +1013,18 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (SPLIT_B && has_next && h == 0) pl_nx = place_b(nxt, buf ^ 1, lo_next);
             if constexpr (FPIPE)
             {
-                // the next tile's layer 1, queued behind this tile's layer 2 (its
-                // [x | 1] buffer was last read by the layer 1 of two tiles ago)
+                // the next tile's layer 1, queued behind this tile's layer 2 (the
+                // [x | 1] buffer was last read by this tile's layer 1, completed)
                 if (has_next)
                 {
-                    if (h == 0) put_x1(nx.x, xb ^ 1);
+                    if (h == 0) put_x1(nx.x, 0);
                     fence_smem_async();
                     fence_before();
                     __syncthreads();
                     if (issuer)
                     {
                         fence_after();
-                        issue_l1(xb ^ 1);
+                        issue_l1(0);
                     }
                 }
             }
@@ -1102,11 +1167,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         nx = gather_b(pl_nx);
                     else
                         nx = stage_b(nxt, buf ^ 1, lo_next);
-                    // the next tile's [x | 1] buffer was last read by this CTA's
-                    // previous tile, whose GEMMs have completed
+                    // the [x | 1] buffer was last read by this tile's layer 1,
+                    // which has completed
                     if constexpr (PIPE)
                     {
-                        put_x1(nx.x, xb ^ 1);
+                        put_x1(nx.x, 0);
                         put_q(nx, buf ^ 1);
                     }
                 }
@@ -1195,7 +1260,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                             tD4, sdesc(s_base + K::OFF_AB, AB::RG, 128), sdesc(s_base + K::OFF_HB, HB::RG, 128), idW,
                             wg_started);
                     if (PIPE && has_next)
-                        issue_l1(xb ^ 1);
+                        issue_l1(0);
                     else
                         mma_commit(mbar);
                 }

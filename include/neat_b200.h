@@ -218,6 +218,9 @@ typedef struct
     /* nonzero: the workspace also holds the proposal's per-segment CDFs and
      * bins, so that state->proposal may be used */
     int proposal;
+    /* nonzero: the workspace also holds the per-segment and per-ray pose
+     * gradient accumulators, so that state->pose may be used */
+    int pose_grad;
 } neat_step_desc;
 
 /* Decoder paths of the fused step.
@@ -282,6 +285,38 @@ typedef struct
 } neat_proposal;
 
 /* ----------------------------------------------------------------------- */
+/* Camera pose and intrinsics gradients of the step's loss: the reference's */
+/* autograd through SceneBase::GetRays (src/data/SceneBase.cpp:171-193),    */
+/* RotatePoint (src/modules/CameraPose.cu:37-127, left tangent at 0),       */
+/* CameraModelModuleImpl::Unproject (CameraPose.cu:262-274) and the sample  */
+/* positions o[ray] + d[ray] t with t held constant (HyperTree.cu:426-432),  */
+/* IGS's uv gradient and the local coordinates.  Accumulated (added) into:  */
+/*   grad_tangent     [num_images, 3] f64: rotation tangent                 */
+/*   grad_translation [num_images, 3] f64                                   */
+/*   grad_intrinsics  [5] f64: fx, fy, cx, cy, skew (skew's is 0: unused)   */
+/* Requires a tensor-core decoder path and desc->pose_grad.                 */
+/* ----------------------------------------------------------------------- */
+typedef struct
+{
+    double* grad_tangent;
+    double* grad_translation;
+    double* grad_intrinsics;
+    int num_images;
+} neat_pose_grad;
+
+/* The reference's structure optimizer step (SceneBase::OptimizerStep,      */
+/* src/data/SceneBase.cpp:103-118, 232-240): plain SGD with lr_pose on the  */
+/* rotation tangent and translation (when optimize_pose) and lr_intrinsics  */
+/* on the intrinsics (when optimize_intrinsics), then the tangent applied   */
+/* to the rotation, q <- exp(tangent) * q (CameraPoseModuleImpl::ApplyTangent, */
+/* CameraPose.cu:163-183; the product renormalised), and the gradients      */
+/* zeroed (zero_grad).  rotation [num_images, 4] (x, y, z, w), translation  */
+/* [num_images, 3], intrinsics [5], all f64 device arrays, updated in place. */
+int neat_pose_sgd(double* rotation, double* translation, double* intrinsics, const neat_pose_grad* grad,
+                  double lr_pose, double lr_intrinsics, int optimize_pose, int optimize_intrinsics,
+                  neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
 /* Photometric calibration fused into the loss (PhotometricCalibration,     */
 /* src/modules/ToneMapper.cpp:139-223, optimised by SGD in                   */
 /* SceneBase::OptimizerStep, src/data/SceneBase.cpp:121-157, 232-263):       */
@@ -334,6 +369,8 @@ typedef struct
     uint16_t* grid_bf16;
     /* optional photometric calibration between the line integral and the loss; NULL: identity */
     const neat_tonemap* tonemap;
+    /* optional camera pose / intrinsics gradients (requires desc->pose_grad); NULL: off */
+    const neat_pose_grad* pose;
 } neat_step_state;
 
 typedef struct

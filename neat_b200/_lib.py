@@ -41,7 +41,7 @@ class StepDesc(ctypes.Structure):
         ("intrinsics", c_void_p), ("rotation", c_void_p), ("translation", c_void_p),
         ("C", c_int), ("G", c_int), ("softplus_beta", c_float), ("max_samples_per_node", c_int),
         ("lr_grid", c_float), ("lr_decoder", c_float), ("beta1", c_float), ("beta2", c_float), ("eps", c_float),
-        ("seg_capacity", c_int64), ("decoder_path", c_int), ("proposal", c_int),
+        ("seg_capacity", c_int64), ("decoder_path", c_int), ("proposal", c_int), ("pose_grad", c_int),
     ]
 
 
@@ -65,10 +65,15 @@ class ToneMap(ctypes.Structure):
                 ("params", c_void_p), ("grad", c_void_p), ("param_loss", c_void_p)]
 
 
+class PoseGrad(ctypes.Structure):
+    _fields_ = [("grad_tangent", c_void_p), ("grad_translation", c_void_p), ("grad_intrinsics", c_void_p),
+                ("num_images", c_int)]
+
+
 class StepState(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("grid", "grid_m", "grid_v", "grid_grad",
                                         "decoder", "decoder_m", "decoder_v", "decoder_grad", "step_counter",
-                                        "proposal", "grid_bf16", "tonemap")]
+                                        "proposal", "grid_bf16", "tonemap", "pose")]
 
 
 class StepBatch(ctypes.Structure):
@@ -107,6 +112,8 @@ _SIGS = {
                                  c_void_p, c_void_p]),
     "neat_igs_backward": (c_int, [c_void_p, c_int64, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_int64,
                                   c_void_p, c_void_p, c_void_p, c_void_p]),
+    "neat_pose_sgd": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.POINTER(PoseGrad), ctypes.c_double,
+                              ctypes.c_double, c_int, c_int, c_void_p]),
     "neat_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_float, c_float, c_float, c_float, c_int,
                           c_int, c_void_p]),
     "neat_decoder_params": (c_int64, [c_int]),

@@ -67,11 +67,19 @@ struct StepTileArgs
     const int* step_dev;  // when set, the step number is read here (device-side step counter)
     const float* seg_cdf;  // proposal CDF per node-major segment [8] (null: uniform stratified)
     float* seg_hist;       // per ray-major segment [8]: contribution mass per sub-interval (null: off)
+    float* seg_pgrad;      // per node-major segment [6]: sums of dL/d(ix,iy,iz) and t times it (null: off)
     int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;
 };
 using StepTcArgs = StepTileArgs;
+
+// Camera pose gradients (neat_pose.cu): per-segment sums -> per-ray dL/do,
+// dL/dd -> per-image rotation tangent and translation, camera intrinsics.
+cudaError_t launch_pose_grad(const SegRec* segs, const int64_t* counters, const float* seg_pgrad, int G,
+                             float* ray_pgrad, const float* uv, const int32_t* image_id, int64_t R, int w, int h,
+                             const double* intrinsics, const double* rotation, const neat_pose_grad* pose,
+                             cudaStream_t st);
 
 // Learned proposal (neat_proposal.cu).
 // CDF of every node-major segment (counters[0] of them) from the proposal MLP.

@@ -62,6 +62,7 @@ struct SlotSample
     float weight;
     float lu, lv, lw;  // local coordinates in [-1,1]
     float u;           // stratified CDF position (j + a) / n of the sample
+    float t;           // ray parameter of the sample
     int ray, rm, row;
 };
 
@@ -76,6 +77,7 @@ __device__ __forceinline__ SlotSample slot_sample(const SegRec& r, int j, bool v
     if (!valid) j = 0;
     float ts, ws;
     seg_sample(r.tmin, r.tmax, r.n, j, jitter, seed, step, r.ray, r.local_base, ts, ws);
+    q.t             = ts;
     q.lu            = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], ts)), r.mn[0], r.mx[0]);
     q.lv            = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], ts)), r.mn[1], r.mx[1]);
     q.lw            = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], ts)), r.mn[2], r.mx[2]);
@@ -122,6 +124,7 @@ __device__ __forceinline__ SlotSample slot_sample_warp(const SegRec& r, int j, b
     if (j < r.n - 1 && lane == 31) tn = tx;
     const float lo = j == 0 ? r.tmin : __fmul_rn(__fadd_rn(tp, t), 0.5f);
     const float hi = j == r.n - 1 ? r.tmax : __fmul_rn(__fadd_rn(tn, t), 0.5f);
+    q.t            = t;
     q.lu           = local_coord(__fadd_rn(r.o[0], __fmul_rn(r.d[0], t)), r.mn[0], r.mx[0]);
     q.lv           = local_coord(__fadd_rn(r.o[1], __fmul_rn(r.d[1], t)), r.mn[1], r.mx[1]);
     q.lw           = local_coord(__fadd_rn(r.o[2], __fmul_rn(r.d[2], t)), r.mn[2], r.mx[2]);

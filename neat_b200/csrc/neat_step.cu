@@ -593,7 +593,7 @@ struct StepLayout
     {
         ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
         SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, SEG_CDF, SEG_HIST,
-        PROP_PART, NUM
+        PROP_PART, SEG_PGRAD, RAY_PGRAD, NUM
     };
     size_t off[NUM];
     size_t total;
@@ -624,7 +624,8 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
         (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars),
         d->proposal ? (size_t)cap * 8 * 4 : 0, d->proposal ? (size_t)cap * 8 * 4 : 0,
-        d->proposal ? proposal_part_floats() * 4 : 0};
+        d->proposal ? proposal_part_floats() * 4 : 0, d->pose_grad ? (size_t)cap * 6 * 4 : 0,
+        d->pose_grad ? (size_t)R * 6 * 4 : 0};
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
     {
@@ -708,6 +709,7 @@ struct StepBufs
     int* scratch;
     StepScalars* scal;
     float *seg_cdf, *seg_hist, *prop_part;
+    float *seg_pgrad, *ray_pgrad;
 };
 
 static StepBufs step_bufs(const StepLayout& L, void* workspace)
@@ -736,6 +738,8 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.seg_cdf      = (float*)P_(StepLayout::SEG_CDF);
     w.seg_hist     = (float*)P_(StepLayout::SEG_HIST);
     w.prop_part    = (float*)P_(StepLayout::PROP_PART);
+    w.seg_pgrad    = (float*)P_(StepLayout::SEG_PGRAD);
+    w.ray_pgrad    = (float*)P_(StepLayout::RAY_PGRAD);
     return w;
 }
 
@@ -808,6 +812,7 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.step_dev  = &w.scal->step;
     ta.seg_cdf   = nullptr;
     ta.seg_hist  = nullptr;
+    ta.seg_pgrad = nullptr;
     ta.jitter    = jitter;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;
@@ -911,6 +916,9 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     if (!proposal_mode(d, s->proposal, pmode)) return NEAT_ERR_BAD_INPUT;
     if (s->grid_bf16 && (d->decoder_path == NEAT_DECODER_SIMT_FP32 || ((uintptr_t)s->grid_bf16 & 15)))
         return NEAT_ERR_BAD_INPUT;
+    if (s->pose && (!d->pose_grad || d->decoder_path == NEAT_DECODER_SIMT_FP32 || !s->pose->grad_tangent ||
+                    !s->pose->grad_translation || !s->pose->grad_intrinsics || s->pose->num_images < 1))
+        return NEAT_ERR_BAD_INPUT;
     if (s->tonemap && (!s->tonemap->params || !s->tonemap->grad || s->tonemap->num_images < 1 ||
                        (s->tonemap->sensor_bias && (s->tonemap->bias_w < 2 || s->tonemap->bias_h < 2)) ||
                        !(s->tonemap->response_range > 0.0f)))
@@ -961,7 +969,18 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
                                                w.loss_part, invR, cnt + 0, tm);
     k_loss_final<<<1, 1024, 0, st>>>(w.loss_part, L.loss_blocks, out->loss, invR);
     phase(3);
-    ok = ok && launch_tiles_path(d, true, ta, st) == cudaSuccess;
+    if (s->pose)
+    {
+        // per-segment and per-ray pose-gradient accumulators start at zero
+        k_zero_per_segment<<<sm_count() * 4, 256, 0, st>>>(w.seg_pgrad, cnt, 6);
+        ok           = ok && cudaMemsetAsync(w.ray_pgrad, 0, (size_t)R * 6 * 4, st) == cudaSuccess;
+        ta.seg_pgrad = w.seg_pgrad;
+    }
+    ok           = ok && launch_tiles_path(d, true, ta, st) == cudaSuccess;
+    ta.seg_pgrad = nullptr;
+    if (s->pose)
+        ok = ok && launch_pose_grad(w.segs, cnt, w.seg_pgrad, d->G, w.ray_pgrad, b->uv, b->image_id, R, d->w, d->h,
+                                    d->intrinsics, d->rotation, s->pose, st) == cudaSuccess;
     phase(4);
 
     const int P = (int)decoder_params(d->C);

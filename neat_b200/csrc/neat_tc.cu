@@ -387,7 +387,9 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
-template <int C, int PREC, bool BWD>
+// POSE (backward only): also the camera pose gradient terms of every sample
+// (a.seg_pgrad); a separate instantiation, so the plain step's code is unchanged.
+template <int C, int PREC, bool BWD, bool POSE = false>
 __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, BWD>::min_blocks)
     k_step_tiles_tc(StepTcArgs a)
 {
@@ -678,6 +680,71 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 scatter_cl<C>(a.grid_grad, row, a.G, kc, dx);
             }
         }
+    };
+
+    // Camera pose gradients of one sample (first thread of the sample): with
+    // g_q = sum_c grid_q[c] dX[c] over the 8 corners (re-read: the gather summed
+    // them into x), dL/d(ix, iy, iz) = sum_q g_q dw_q/d(ix, iy, iz) -- the
+    // IGS uv gradient before its (W-1)/2 scale -- and t times it; summed over
+    // the warp's runs of one segment, one atomic per run into seg_pgrad.
+    auto pose_sample = [&](const float (&dx)[C], const SlotSample& q, int seg) {
+        float g[6] = {};
+        if (q.valid)
+        {
+            Corners kc;
+            igs_corners(q.lu, q.lv, q.lw, a.G, a.G, a.G, kc);
+            const float ax0 = __fsub_rn((float)(kc.x0 + 1), kc.ix), ax1 = __fsub_rn(kc.ix, (float)kc.x0);
+            const float ay0 = __fsub_rn((float)(kc.y0 + 1), kc.iy), ay1 = __fsub_rn(kc.iy, (float)kc.y0);
+            const float az0 = __fsub_rn((float)(kc.z0 + 1), kc.iz), az1 = __fsub_rn(kc.iz, (float)kc.z0);
+            const int64_t base = (int64_t)q.row * a.G * a.G * a.G;
+#pragma unroll
+            for (int qq = 0; qq < 8; ++qq)
+            {
+                const int64_t cell = (base + corner_cell(kc, qq, a.G, a.G)) * C;
+                float gq = 0.0f;
+                if (a.grid_bf16)
+                {
+#pragma unroll
+                    for (int c = 0; c < C; ++c)
+                        gq = fmaf(__uint_as_float((uint32_t)__ldg(a.grid_bf16 + cell + c) << 16), dx[c], gq);
+                }
+                else
+                {
+#pragma unroll
+                    for (int c4 = 0; c4 < C / 4; ++c4)
+                    {
+                        const float4 v = __ldg(reinterpret_cast<const float4*>(a.grid + cell) + c4);
+                        gq             = fmaf(v.x, dx[4 * c4], gq);
+                        gq             = fmaf(v.y, dx[4 * c4 + 1], gq);
+                        gq             = fmaf(v.z, dx[4 * c4 + 2], gq);
+                        gq             = fmaf(v.w, dx[4 * c4 + 3], gq);
+                    }
+                }
+                const float fx = (qq & 1) ? ax1 : ax0, fy = (qq & 2) ? ay1 : ay0, fz = (qq & 4) ? az1 : az0;
+                g[0] = fmaf(gq, ((qq & 1) ? 1.0f : -1.0f) * fy * fz, g[0]);
+                g[1] = fmaf(gq, fx * ((qq & 2) ? 1.0f : -1.0f) * fz, g[1]);
+                g[2] = fmaf(gq, fx * fy * ((qq & 4) ? 1.0f : -1.0f), g[2]);
+            }
+            g[3] = g[0] * q.t;
+            g[4] = g[1] * q.t;
+            g[5] = g[2] * q.t;
+        }
+        const int sg = q.valid ? seg : -1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int sn = __shfl_down_sync(0xffffffffu, sg, o);
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+            {
+                const float vn = __shfl_down_sync(0xffffffffu, g[k], o);
+                if (l + o < 32 && sn == sg) g[k] += vn;
+            }
+        }
+        const int sp = __shfl_up_sync(0xffffffffu, sg, 1);
+        if (q.valid && (l == 0 || sp != sg))
+#pragma unroll
+            for (int k = 0; k < 6; ++k) atomicAdd(a.seg_pgrad + 6 * (int64_t)seg + k, g[k]);
     };
 
     int it = 0;
@@ -1268,6 +1335,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 wg_pending = true;
                 // ---- this tile's dX scattered while the weight-gradient GEMM runs
                 scatter_dx(dx, cur.q, buf);
+                if constexpr (POSE)
+                {
+                    if (h == 0) pose_sample(dx, cur.q, cur.seg);
+                }
             }
             if (has_next && h == 0) cur = nx;
             lo_next = lo_nx2;
@@ -1371,7 +1442,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                      : "memory");
 }
 
-template <int C, int PREC, bool BWD>
+template <int C, int PREC, bool BWD, bool POSE = false>
 static int tc_grid(size_t& smem)
 {
     using K = Cfg<C, PREC, BWD>;
@@ -1379,9 +1450,10 @@ static int tc_grid(size_t& smem)
     static int blocks = 0;
     if (blocks == 0)
     {
-        cudaFuncSetAttribute(k_step_tiles_tc<C, PREC, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_step_tiles_tc<C, PREC, BWD, POSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         // TMEM: 512 columns per SM shared by the resident CTAs
-        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD>, TcThreads<PREC, BWD>::value, smem,
+        blocks = resident_ctas((const void*)k_step_tiles_tc<C, PREC, BWD, POSE>, TcThreads<PREC, BWD>::value, smem,
                                (int)(512 / K::TMEM_COLS)) *
                  sm_count();
     }
@@ -1399,8 +1471,17 @@ static cudaError_t launch(bool bwd, const StepTcArgs& args, cudaStream_t st)
     }
     else
     {
+        // the step's decoder partials are sized by the plain backward's grid
         const int g = tc_grid<C, PREC, true>(smem);
-        k_step_tiles_tc<C, PREC, true><<<g, TcThreads<PREC, true>::value, smem, st>>>(args);
+        if (args.seg_pgrad)
+        {
+            tc_grid<C, PREC, true, true>(smem);  // its shared-memory attribute
+            k_step_tiles_tc<C, PREC, true, true><<<g, TcThreads<PREC, true>::value, smem, st>>>(args);
+        }
+        else
+        {
+            k_step_tiles_tc<C, PREC, true><<<g, TcThreads<PREC, true>::value, smem, st>>>(args);
+        }
     }
     return cudaGetLastError();
 }

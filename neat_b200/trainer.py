@@ -24,7 +24,8 @@ class FusedTrainer:
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
                  proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
-                 tonemap=None):
+                 tonemap=None, pose_grad=False, optimize_pose=False, optimize_intrinsics=False, lr_pose=1e-3,
+                 lr_intrinsics=100.0):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -124,6 +125,28 @@ class FusedTrainer:
             self.state.proposal = ctypes.addressof(self.prop_struct)
             self.desc_budget = _lib.StepDesc.from_buffer_copy(self.desc)
             self.desc_budget.max_samples_per_node = int(proposal_budget)
+        # camera pose / intrinsics gradients (the reference's structure
+        # parameters: rotation tangent, translation, intrinsics), accumulated by
+        # every step into pose_grad_*; with optimize_pose / optimize_intrinsics
+        # the step is followed by the reference's SGD on them (lr_pose,
+        # lr_intrinsics; SceneBase::OptimizerStep), which also zeroes them
+        self.optimize_pose, self.optimize_intrinsics = bool(optimize_pose), bool(optimize_intrinsics)
+        self.lr_pose, self.lr_intrinsics = float(lr_pose), float(lr_intrinsics)
+        self.pose = None
+        if pose_grad or self.optimize_pose or self.optimize_intrinsics:
+            if decoder_path == _lib.NEAT_DECODER_SIMT_FP32:
+                raise ValueError("pose gradients run with the tensor-core decoder paths")
+            n_img = camera.rotation.shape[0]
+            self.pose_grad_tangent = torch.zeros((n_img, 3), dtype=torch.float64, device=self.dev)
+            self.pose_grad_translation = torch.zeros((n_img, 3), dtype=torch.float64, device=self.dev)
+            self.pose_grad_intrinsics = torch.zeros(5, dtype=torch.float64, device=self.dev)
+            self.pose = _lib.PoseGrad(grad_tangent=self.pose_grad_tangent.data_ptr(),
+                                      grad_translation=self.pose_grad_translation.data_ptr(),
+                                      grad_intrinsics=self.pose_grad_intrinsics.data_ptr(), num_images=n_img)
+            self.desc.pose_grad = 1
+            if self.proposal:
+                self.desc_budget.pose_grad = 1
+            self.state.pose = ctypes.addressof(self.pose)
 
     def _stream(self):
         return torch.cuda.current_stream(self.dev).cuda_stream
@@ -174,7 +197,18 @@ class FusedTrainer:
                                       self.seed, self.step_id, ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
                                       self._stream())
         _lib.check(rc, "neat_train_step")
+        if self.optimize_pose or self.optimize_intrinsics:
+            self.pose_step()
         return self.loss
+
+    def pose_step(self):
+        """The reference's structure optimizer step on the accumulated pose
+        gradients (SGD, rotation <- exp(tangent) rotation), which zeroes them."""
+        cam = self.camera
+        _lib.check(self.lib.neat_pose_sgd(cam.rotation.data_ptr(), cam.translation.data_ptr(),
+                                          cam.intrinsics.data_ptr(), ctypes.byref(self.pose), self.lr_pose,
+                                          self.lr_intrinsics, int(self.optimize_pose),
+                                          int(self.optimize_intrinsics), self._stream()), "neat_pose_sgd")
 
     def regularize(self):
         """VolumeRegularizer (src/geometry/geometry_ex_ex.cpp:86-156): TV and edge

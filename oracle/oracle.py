@@ -399,6 +399,94 @@ def step_f64(samples, grid_ref, dec, target, node_min, node_max, prefix, beta=2.
 
 
 # --------------------------------------------------------------------------
+# camera pose and intrinsics gradients (f64 autograd)
+# --------------------------------------------------------------------------
+def _quat_rotate_t(torch, q, v):
+    """v rotated by unit quaternions q = (x, y, z, w): v + w t + u x t, t = 2 u x v."""
+    u, w = q[:, :3], q[:, 3:4]
+    t = 2 * torch.cross(u, v, dim=1)
+    return v + w * t + torch.cross(u, t, dim=1)
+
+
+def pose_loss_f64(samples, uv, image_id, w, h, intr, rot, trans, grid, dec, target, node_min, node_max, prefix,
+                  beta=2.0, tangent=None, cells_from_coords=True):
+    """The step's loss in f64 as a function of the camera parameters, the
+    reference's autograd chain (SceneBase::GetRays, src/data/SceneBase.cpp:171-193;
+    Unproject, src/modules/CameraPose.cu:262-274; RotatePoint, CameraPose.cu:37-127
+    with the rotation on a left tangent; positions o + d t with t constant,
+    src/structure/HyperTree.cu:426-432; local coordinates, IGS, decoder,
+    index_add, MSE).  Returns (loss, tangent, translation, intrinsics), the last
+    three leaf tensors with gradients.  cells_from_coords: the trilinear cells
+    from the sampler's f32 coordinates (the f64 positions carry only the
+    gradient), else from the f64 positions themselves.  tangent [N,3] (default
+    0): applied as exp(w) to first order, exact for the gradient at 0."""
+    import torch
+    R = target.shape[0]
+    rot64 = torch.from_numpy(np.asarray(rot, np.float64).reshape(-1, 4))
+    n_img = rot64.shape[0]
+    tg = np.zeros((n_img, 3)) if tangent is None else np.asarray(tangent, np.float64)
+    tangent = torch.from_numpy(tg.copy()).requires_grad_(True)
+    tr = torch.from_numpy(np.asarray(trans, np.float64).reshape(-1, 3).copy()).requires_grad_(True)
+    k = torch.from_numpy(np.asarray(intr, np.float64).reshape(-1)[:5].copy()).requires_grad_(True)
+    uvf = np.asarray(uv, np.float32)
+    px = torch.from_numpy((uvf[:, 0] * np.float32(w - 1)).astype(np.float64))
+    py = torch.from_numpy((uvf[:, 1] * np.float32(h - 1)).astype(np.float64))
+    img = torch.from_numpy(np.asarray(image_id, np.int64))
+    x = (px - k[2]) / k[0]
+    y = (py - k[3]) / k[1]
+    u = torch.stack([x, y, torch.ones_like(x)], 1)
+    n = u / u.norm(dim=1, keepdim=True)
+    Rn = _quat_rotate_t(torch, rot64[img], n)
+    d = Rn + torch.cross(tangent[img], Rn, dim=1)
+    o = tr[img]
+    ray = torch.from_numpy(samples["ray_index"])
+    t = torch.from_numpy(samples["ray_t"].astype(np.float64))
+    pg = o[ray] + d[ray] * t[:, None]
+    p = torch.from_numpy(samples["coords"].astype(np.float64)) + (pg - pg.detach()) if cells_from_coords else pg
+    nid = torch.from_numpy(samples["node_id"])
+    mn = torch.from_numpy(node_min).double()[nid]
+    mx = torch.from_numpy(node_max).double()[nid]
+    local = (p - mn) / (mx - mn) * 2 - 1
+    row = torch.from_numpy(prefix[samples["node_id"]])
+    g = torch.from_numpy(np.asarray(grid, np.float64))
+    feat = _trilinear_f64(torch, g, row, local)
+    dens = decoder_f64(torch, feat, torch.from_numpy(np.asarray(dec, np.float64)), g.shape[1], beta)
+    val = dens * torch.from_numpy(samples["weight"]).double()
+    pred = torch.zeros(R, dtype=torch.float64).index_add(0, ray, val)
+    loss = ((pred - torch.from_numpy(np.asarray(target, np.float64))) ** 2).mean()
+    return loss, tangent, tr, k
+
+
+def pose_grads_f64(samples, uv, image_id, w, h, intr, rot, trans, grid, dec, target, node_min, node_max, prefix,
+                   beta=2.0, cells_from_coords=True):
+    """d loss / d(rotation tangent [N,3] at 0, translation [N,3], intrinsics [5])
+    in f64 (pose_loss_f64's chain)."""
+    loss, tangent, tr, k = pose_loss_f64(samples, uv, image_id, w, h, intr, rot, trans, grid, dec, target, node_min,
+                                         node_max, prefix, beta, cells_from_coords=cells_from_coords)
+    loss.backward()
+    return dict(loss=float(loss.detach()), tangent=tangent.grad.numpy(), translation=tr.grad.numpy(),
+                intrinsics=k.grad.numpy())
+
+
+def quat_exp_mul_f64(tangent, q):
+    """exp(tangent) * q for rotation vectors [N,3] and unit quaternions [N,4]
+    (x, y, z, w), renormalised: the rotation update of the structure step."""
+    tangent = np.asarray(tangent, np.float64)
+    q = np.asarray(q, np.float64)
+    th = np.linalg.norm(tangent, axis=1)
+    small = th < 1e-10
+    ths = np.where(small, 1.0, th)
+    im = np.where(small, 0.5 - th ** 2 / 48, np.sin(0.5 * th) / ths)
+    re = np.where(small, 1 - th ** 2 / 8, np.cos(0.5 * th))
+    a = np.concatenate([im[:, None] * tangent, re[:, None]], 1)
+    ax, ay, az, aw = a.T
+    bx, by, bz, bw = q.T
+    out = np.stack([aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+                    aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz], 1)
+    return out / np.linalg.norm(out, axis=1, keepdims=True)
+
+
+# --------------------------------------------------------------------------
 # learned sample proposal (restatement of neat_b200/csrc/neat_proposal.cuh)
 # --------------------------------------------------------------------------
 PROP_IN, PROP_H, PROP_B = 16, 32, 8

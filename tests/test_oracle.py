@@ -329,3 +329,70 @@ def test_proposal_gradient_matches_finite_differences(oracle):
         lp, _ = oracle.proposal_grad_f64(P + e, f, hist, 0.1)
         lm, _ = oracle.proposal_grad_f64(P - e, f, hist, 0.1)
         assert abs((lp - lm) / 2e-6 - g[k]) <= 1e-6 + 1e-5 * abs(g[k])
+
+
+def test_pose_gradients_match_finite_differences(oracle):
+    """The f64 pose / intrinsics gradient chain (the oracle of the GPU pose
+    gradients) matches central differences of its own loss: rotation tangent,
+    translation and intrinsics, with the samples (t, node, weight) held fixed as
+    in the reference's autograd and the trilinear cells from the f64 positions.
+    Steps are small enough (1e-7, 1e-6 pixels) that no sample changes cell."""
+    c = cfg1_case(R=64, oracle=oracle, n_angles=4, w=32, h=32)
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    T = c.tree
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True, seed=1)
+    args = (s, c.uv, c.img, c.w, c.h)
+    tail = (c.grid, c.dec, c.target, T.node_position_min, T.node_position_max, T.node_active_prefix_sum)
+    g = oracle.pose_grads_f64(*args, c.intr, c.rot, c.trans, *tail, cells_from_coords=False)
+
+    def loss(intr=c.intr, trans=c.trans, tangent=None):
+        return float(oracle.pose_loss_f64(*args, intr, c.rot, trans, *tail, tangent=tangent,
+                                          cells_from_coords=False)[0].detach())
+
+    n_img = np.asarray(c.rot).reshape(-1, 4).shape[0]
+    e = 1e-7
+    for i in np.unique(c.img)[:3]:
+        for k in range(3):
+            tp = np.zeros((n_img, 3))
+            tp[i, k] = e
+            fd = (loss(tangent=tp) - loss(tangent=-tp)) / (2 * e)
+            assert abs(fd - g["tangent"][i, k]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9
+            trp = np.asarray(c.trans, np.float64).reshape(-1, 3).copy()
+            trm = trp.copy()
+            trp[i, k] += e
+            trm[i, k] -= e
+            fd = (loss(trans=trp) - loss(trans=trm)) / (2 * e)
+            assert abs(fd - g["translation"][i, k]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9
+    for k in range(4):
+        ip = np.asarray(c.intr, np.float64).reshape(-1).copy()
+        im = ip.copy()
+        ip[k] += 1e-6
+        im[k] -= 1e-6
+        fd = (loss(intr=ip) - loss(intr=im)) / 2e-6
+        assert abs(fd - g["intrinsics"][k]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9
+    assert g["intrinsics"][4] == 0.0  # the skew does not enter Unproject
+
+
+def test_quat_exp_mul_is_the_rotation_update(oracle):
+    """quat_exp_mul_f64: exp of a rotation vector (axis * angle) times q, as a
+    rotation matrix product (Rodrigues)."""
+    rng = np.random.default_rng(2)
+    q = rng.normal(size=(6, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w = rng.normal(size=(6, 3)) * 0.3
+    w[0] = 0.0
+    w[1] = 1e-12
+
+    def mat(qq):
+        x, y, z, s = qq
+        return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - s * z), 2 * (x * z + s * y)],
+                         [2 * (x * y + s * z), 1 - 2 * (x * x + z * z), 2 * (y * z - s * x)],
+                         [2 * (x * z - s * y), 2 * (y * z + s * x), 1 - 2 * (x * x + y * y)]])
+
+    out = oracle.quat_exp_mul_f64(w, q)
+    for i in range(6):
+        th = np.linalg.norm(w[i])
+        K = np.array([[0, -w[i, 2], w[i, 1]], [w[i, 2], 0, -w[i, 0]], [-w[i, 1], w[i, 0], 0]])
+        a = np.sin(th) / th if th > 0 else 1.0
+        b = (1 - np.cos(th)) / th ** 2 if th > 1e-6 else 0.5
+        np.testing.assert_allclose(mat(out[i]), (np.eye(3) + a * K + b * K @ K) @ mat(q[i]), rtol=0, atol=1e-12)

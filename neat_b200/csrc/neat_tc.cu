@@ -137,7 +137,12 @@ struct CfgPlan
     static constexpr int OFF_V  = OFF_I + 2 * 132 * 4 + 4 * 8 + 8 * 4;
     static constexpr int OFF_Q  = OFF_V + 2 * 128 * 4;        // [2][6][128] slot data for the second thread (both directions)
     static constexpr int NQ     = (NH == 2) ? 2 * 6 * 128 : 0;
-    static constexpr int OFF_R  = OFF_Q + NQ * 4;
+    // backward, two threads per sample: placement records of the next tile
+    // [weight, lu, lv, lw, t, ray, rm, row, seg, u][128], written by the second
+    // half, read by the first half's gather
+    static constexpr int NP     = (BWD && NH == 2) ? 10 * 128 : 0;
+    static constexpr int OFF_P  = OFF_Q + NQ * 4;
+    static constexpr int OFF_R  = OFF_P + NP * 4;
     static constexpr int NRED   = BWD ? 8 * HH : 0;
     static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
     static constexpr int NEED   = OFF_M + 32;                 // mbarriers at +0, +8, +24; TMEM slot at +16
@@ -601,6 +606,41 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         return o;
     };
     auto stage_b = [&](int64_t tl, int b, int lo) -> Slot { return gather_b(place_b(tl, b, lo)); };
+    // placement records in shared memory (slot s), see K::OFF_P
+    float* prec = reinterpret_cast<float*>(sm + K::OFF_P);
+    auto store_p = [&](const Place& pl) {
+        if constexpr (K::NP > 0)
+        {
+            prec[0 * 128 + s] = pl.q.weight;
+            prec[1 * 128 + s] = pl.q.lu;
+            prec[2 * 128 + s] = pl.q.lv;
+            prec[3 * 128 + s] = pl.q.lw;
+            prec[4 * 128 + s] = pl.q.t;
+            prec[5 * 128 + s] = __int_as_float(pl.q.ray);
+            prec[6 * 128 + s] = __int_as_float(pl.q.rm);
+            prec[7 * 128 + s] = __int_as_float(pl.q.row);
+            prec[8 * 128 + s] = __int_as_float(pl.seg);
+            prec[9 * 128 + s] = pl.q.u;
+        }
+    };
+    auto load_p = [&]() -> Place {
+        Place pl;
+        if constexpr (K::NP > 0)
+        {
+            pl.q.weight = prec[0 * 128 + s];
+            pl.q.lu     = prec[1 * 128 + s];
+            pl.q.lv     = prec[2 * 128 + s];
+            pl.q.lw     = prec[3 * 128 + s];
+            pl.q.t      = prec[4 * 128 + s];
+            pl.q.ray    = __float_as_int(prec[5 * 128 + s]);
+            pl.q.rm     = __float_as_int(prec[6 * 128 + s]);
+            pl.q.row    = __float_as_int(prec[7 * 128 + s]);
+            pl.seg      = __float_as_int(prec[8 * 128 + s]);
+            pl.q.u      = prec[9 * 128 + s];
+            pl.q.valid  = pl.seg >= 0;
+        }
+        return pl;
+    };
     // Row s of an [x | 1 | 0 ..] block: the separate buffer b (b >= 0) or the
     // columns [64, 64 + K1) of HB (b < 0).
     auto put_x1 = [&](const float (&xv)[C], int b) {
@@ -958,15 +998,29 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
         for (int c = 0; c < C; ++c) cur.x[c] = 0.0f;
         int lo_next = 0;  // tile_seg of the next tile, loaded a tile ahead
+        int lo_p2   = 0;  // SPLIT_B: tile_seg of the tile after next (placed this iteration)
         if (blockIdx.x < ntiles)
         {
             const int lo0 = a.tile_seg[blockIdx.x];
             int oa, ob;
             fetch_starts(lo0, oa, ob);
             put_starts(0, oa, ob);
+            const bool has1 = blockIdx.x + gridDim.x < ntiles;
+            const int lo1   = has1 ? a.tile_seg[blockIdx.x + gridDim.x] : 0;
+            if (SPLIT_B && has1)
+            {
+                fetch_starts(lo1, oa, ob);
+                put_starts(1, oa, ob);
+            }
             __syncthreads();
             if (h == 0) cur = stage_b(blockIdx.x, 0, lo0);
-            if (blockIdx.x + gridDim.x < ntiles) lo_next = a.tile_seg[blockIdx.x + gridDim.x];
+            if constexpr (SPLIT_B)
+            {
+                // the next tile placed by the second half (its records read in the first layer-2 window)
+                if (has1 && h == 1) store_p(place_b(blockIdx.x + gridDim.x, 1, lo1));
+                if (blockIdx.x + 2 * gridDim.x < ntiles) lo_p2 = a.tile_seg[blockIdx.x + 2 * gridDim.x];
+            }
+            lo_next = lo1;
             if constexpr (PIPE || FPIPE)
             {
                 if (h == 0)
@@ -995,10 +1049,14 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             nx.dvw     = 0.0f;
             nx.seg     = -1;
             // the next tile's segment starts (stored before the barrier ahead of
-            // its stage_b) and the tile_seg of the one after it
+            // its stage_b) and the tile_seg of the one after it; SPLIT_B: the same
+            // one tile further ahead (the tile after next is placed here)
+            const bool has_next2 = nxt + gridDim.x < ntiles;
             int oa_nx = INT_MAX, ob_nx = INT_MAX;
-            if (has_next) fetch_starts(lo_next, oa_nx, ob_nx);
-            const int lo_nx2 = nxt + gridDim.x < ntiles ? a.tile_seg[nxt + gridDim.x] : 0;
+            if (!SPLIT_B && has_next) fetch_starts(lo_next, oa_nx, ob_nx);
+            if (SPLIT_B && has_next2) fetch_starts(lo_p2, oa_nx, ob_nx);
+            const int lo_nx2 = !SPLIT_B ? (has_next2 ? a.tile_seg[nxt + gridDim.x] : 0)
+                                        : (nxt + 2 * gridDim.x < ntiles ? a.tile_seg[nxt + 2 * gridDim.x] : 0);
             // ---- without the pipelined layer 1: the previous tile's weight-gradient
             //      GEMM reads HB's [x | 1] columns, rewritten next
             if (BWD && wg_pending)
@@ -1062,7 +1120,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             if constexpr (CACHE) tmem_wait_st();
             if (PIPE && h == 0) put_x1(cur.x, -1);  // HB's [x | 1] columns for the weight gradients
-            if ((!BWD || SPLIT_B) && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+            if (!BWD && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
             fence_smem_async();
             fence_before();
             __syncthreads();
@@ -1075,9 +1133,20 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 mma_commit(mbar);
             }
             if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
-            // backward: the next tile's placement while layer 2 runs, its gather in the dH1 window
-            Place pl_nx;
-            if (SPLIT_B && has_next && h == 0) pl_nx = place_b(nxt, buf ^ 1, lo_next);
+            // backward, two threads per sample: the next tile's gather (placed a tile
+            // ago by the second half) while layer 2 runs
+            if constexpr (SPLIT_B)
+            {
+                if (has_next && h == 0)
+                {
+                    nx = gather_b(load_p());
+                    if constexpr (PIPE)
+                    {
+                        put_x1(nx.x, 0);  // the [x | 1] buffer's last reader, this tile's layer 1, is done
+                        put_q(nx, buf ^ 1);
+                    }
+                }
+            }
             if constexpr (FPIPE)
             {
                 // the next tile's layer 1, queued behind this tile's layer 2 (the
@@ -1217,23 +1286,29 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     for (int i = 0; i < 16; i += P::E) store_chunk<PREC>(pAB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
                 }
                 if (!SPLIT_B && has_next) put_starts(buf ^ 1, oa_nx, ob_nx);
+            if (SPLIT_B && has_next2) put_starts(buf, oa_nx, ob_nx);  // for the placement below
                 fence_smem_async();
                 fence_before();
                 __syncthreads();
                 // ---- dH1 = dz2 . W2  (B = W2 read MN-major: N = k, K = h) -> D2
-                if (issuer)
+                //      (two threads per sample: issued by warp 0, whose half has no
+                //      work in this window; the second half places a tile meanwhile)
+                if (SPLIT_B ? t == 0 : issuer)
                 {
                     fence_after();
                     gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
                         tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), idH, false);
                     mma_commit(mbar);
                 }
-                if (has_next && h == 0)
+                if constexpr (SPLIT_B)
                 {
-                    if constexpr (SPLIT_B)
-                        nx = gather_b(pl_nx);
-                    else
-                        nx = stage_b(nxt, buf ^ 1, lo_next);
+                    // the tile after next: placement into the records (read by the
+                    // next iteration's gather; this iteration's were read above)
+                    if (has_next2 && h == 1) store_p(place_b(nxt + gridDim.x, buf, lo_p2));
+                }
+                else if (has_next && h == 0)
+                {
+                    nx = stage_b(nxt, buf ^ 1, lo_next);
                     // the [x | 1] buffer was last read by this tile's layer 1,
                     // which has completed
                     if constexpr (PIPE)
@@ -1341,7 +1416,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 }
             }
             if (has_next && h == 0) cur = nx;
-            lo_next = lo_nx2;
+            if constexpr (SPLIT_B)
+                lo_p2 = lo_nx2;
+            else
+                lo_next = lo_nx2;
         }
     }
     // ---- drain: the last tile's weight gradients

@@ -68,6 +68,11 @@ struct StepTileArgs
     const float* seg_cdf;  // proposal CDF per node-major segment [8] (null: uniform stratified)
     float* seg_hist;       // per ray-major segment [8]: contribution mass per sub-interval (null: off)
     float* seg_pgrad;      // per node-major segment [6]: sums of dL/d(ix,iy,iz) and t times it (null: off)
+    // per-sample records the forward writes for the backward (null: off): SoA
+    // [8 + C][rec_cap], fields lu, lv, lw, weight, t (f32), ray, row, seg (i32),
+    // then the gathered features x[C]; used while the step's samples fit rec_cap
+    float* rec;
+    int64_t rec_cap;
     int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;

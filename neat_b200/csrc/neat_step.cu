@@ -593,11 +593,11 @@ struct StepLayout
     {
         ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
         SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, SEG_CDF, SEG_HIST,
-        PROP_PART, SEG_PGRAD, RAY_PGRAD, NUM
+        PROP_PART, SEG_PGRAD, RAY_PGRAD, REC, NUM
     };
     size_t off[NUM];
     size_t total;
-    int64_t tiles_cap, sample_cap;
+    int64_t tiles_cap, sample_cap, rec_cap;
     int loss_blocks, bwd_grid, cap_ray;
 };
 
@@ -609,6 +609,9 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
     L.cap_ray         = (int)std::max<int64_t>(1, std::min<int64_t>(NEAT_MAX_HITS_PER_RAY, R > 0 ? cap / R : 1));
     L.sample_cap      = cap * (M + 1);
     L.tiles_cap       = (L.sample_cap + TT - 1) / TT + 1;
+    // per-sample records from the forward to the backward: room for 4 (M + 1)
+    // samples per ray (a step with more recomputes them in the backward)
+    L.rec_cap         = std::min<int64_t>(L.sample_cap, std::max<int64_t>(R, 1) * (M + 1) * 4);
     L.loss_blocks     = (int)((R + 255) / 256);
     size_t smem       = 0;
     L.bwd_grid        = d->decoder_path == NEAT_DECODER_SIMT_FP32
@@ -625,7 +628,8 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars),
         d->proposal ? (size_t)cap * 8 * 4 : 0, d->proposal ? (size_t)cap * 8 * 4 : 0,
         d->proposal ? proposal_part_floats() * 4 : 0, d->pose_grad ? (size_t)cap * 6 * 4 : 0,
-        d->pose_grad ? (size_t)R * 6 * 4 : 0};
+        d->pose_grad ? (size_t)R * 6 * 4 : 0,
+        d->decoder_path != NEAT_DECODER_SIMT_FP32 ? (size_t)L.rec_cap * (8 + d->C) * 4 : 0};
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
     {
@@ -710,6 +714,7 @@ struct StepBufs
     StepScalars* scal;
     float *seg_cdf, *seg_hist, *prop_part;
     float *seg_pgrad, *ray_pgrad;
+    float* rec;
 };
 
 static StepBufs step_bufs(const StepLayout& L, void* workspace)
@@ -740,6 +745,7 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.prop_part    = (float*)P_(StepLayout::PROP_PART);
     w.seg_pgrad    = (float*)P_(StepLayout::SEG_PGRAD);
     w.ray_pgrad    = (float*)P_(StepLayout::RAY_PGRAD);
+    w.rec          = (float*)P_(StepLayout::REC);
     return w;
 }
 
@@ -813,6 +819,8 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.seg_cdf   = nullptr;
     ta.seg_hist  = nullptr;
     ta.seg_pgrad = nullptr;
+    ta.rec       = nullptr;
+    ta.rec_cap   = 0;
     ta.jitter    = jitter;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;
@@ -944,6 +952,11 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
 
     StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
     ta.grid_bf16    = s->grid_bf16;
+    if (d->decoder_path != NEAT_DECODER_SIMT_FP32)
+    {
+        ta.rec     = w.rec;
+        ta.rec_cap = L.rec_cap;
+    }
     if (pmode == NEAT_PROPOSAL_SAMPLE)
     {
         ok         = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;

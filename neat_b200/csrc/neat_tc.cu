@@ -623,6 +623,60 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             prec[9 * 128 + s] = pl.q.u;
         }
     };
+    // Per-sample records (a.rec): the forward stores the slot set-up of every
+    // sample it runs (placement and gathered features), the backward loads it
+    // instead of recomputing it.  Coalesced: field f of sample i at f * rec_cap + i.
+    const bool rec_ok = a.rec != nullptr && S <= a.rec_cap;
+    auto write_rec = [&](const Slot& sl, int64_t tl) {
+        const int64_t i = tl * 128 + s;
+        if (!rec_ok || i >= S) return;
+        const int64_t cp = a.rec_cap;
+        float* r         = a.rec;
+        r[0 * cp + i]    = sl.q.lu;
+        r[1 * cp + i]    = sl.q.lv;
+        r[2 * cp + i]    = sl.q.lw;
+        r[3 * cp + i]    = sl.q.weight;
+        r[4 * cp + i]    = sl.q.t;
+        r[5 * cp + i]    = __int_as_float(sl.q.ray);
+        r[6 * cp + i]    = __int_as_float(sl.q.row);
+        r[7 * cp + i]    = __int_as_float(sl.seg);
+#pragma unroll
+        for (int c = 0; c < C; ++c) r[(8 + c) * cp + i] = sl.x[c];
+    };
+    auto read_rec = [&](int64_t tl) -> Slot {
+        Slot o;
+        const int64_t i = tl * 128 + s;
+        const bool valid = i < S;
+        o.q.valid        = valid;
+        o.q.u            = 0.0f;
+        o.q.rm           = 0;
+        if (valid)
+        {
+            const int64_t cp = a.rec_cap;
+            const float* r   = a.rec;
+            o.q.lu           = __ldcs(r + 0 * cp + i);
+            o.q.lv           = __ldcs(r + 1 * cp + i);
+            o.q.lw           = __ldcs(r + 2 * cp + i);
+            o.q.weight       = __ldcs(r + 3 * cp + i);
+            o.q.t            = __ldcs(r + 4 * cp + i);
+            o.q.ray          = __float_as_int(__ldcs(r + 5 * cp + i));
+            o.q.row          = __float_as_int(__ldcs(r + 6 * cp + i));
+            o.seg            = __float_as_int(__ldcs(r + 7 * cp + i));
+#pragma unroll
+            for (int c = 0; c < C; ++c) o.x[c] = __ldcs(r + (8 + c) * cp + i);
+            o.dvw = a.dpred[o.q.ray] * o.q.weight;
+        }
+        else
+        {
+            o.q.lu = o.q.lv = o.q.lw = o.q.weight = o.q.t = 0.0f;
+            o.q.ray = o.q.row = 0;
+            o.seg             = -1;
+#pragma unroll
+            for (int c = 0; c < C; ++c) o.x[c] = 0.0f;
+            o.dvw = 0.0f;
+        }
+        return o;
+    };
     auto load_p = [&]() -> Place {
         Place pl;
         if constexpr (K::NP > 0)
@@ -827,6 +881,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 const Slot c0s = gather_b(place_b(T0, 0, lo0));
                 put_x1(c0s.x, 0);
                 put_sr(c0s, 0);
+                write_rec(c0s, T0);
             }
             fence_smem_async();
             fence_before();
@@ -910,6 +965,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     const Slot nx = gather_b(pl_next);
                     put_x1(nx.x, 0);
                     put_sr(nx, buf ^ 1);
+                    write_rec(nx, nxt);
                 }
                 fence_smem_async();
                 fence_before();
@@ -1013,11 +1069,15 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 put_starts(1, oa, ob);
             }
             __syncthreads();
-            if (h == 0) cur = stage_b(blockIdx.x, 0, lo0);
+            if (h == 0)
+            {
+                cur = (BWD && rec_ok) ? read_rec(blockIdx.x) : stage_b(blockIdx.x, 0, lo0);
+                if (!BWD) write_rec(cur, blockIdx.x);
+            }
             if constexpr (SPLIT_B)
             {
                 // the next tile placed by the second half (its records read in the first layer-2 window)
-                if (has1 && h == 1) store_p(place_b(blockIdx.x + gridDim.x, 1, lo1));
+                if (has1 && h == 1 && !rec_ok) store_p(place_b(blockIdx.x + gridDim.x, 1, lo1));
                 if (blockIdx.x + 2 * gridDim.x < ntiles) lo_p2 = a.tile_seg[blockIdx.x + 2 * gridDim.x];
             }
             lo_next = lo1;
@@ -1132,14 +1192,18 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                                                                  sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 mma_commit(mbar);
             }
-            if (!BWD && has_next && h == 0) nx = stage_b(nxt, buf ^ 1, lo_next);
+            if (!BWD && has_next && h == 0)
+            {
+                nx = stage_b(nxt, buf ^ 1, lo_next);
+                write_rec(nx, nxt);
+            }
             // backward, two threads per sample: the next tile's gather (placed a tile
             // ago by the second half) while layer 2 runs
             if constexpr (SPLIT_B)
             {
                 if (has_next && h == 0)
                 {
-                    nx = gather_b(load_p());
+                    nx = rec_ok ? read_rec(nxt) : gather_b(load_p());
                     if constexpr (PIPE)
                     {
                         put_x1(nx.x, 0);  // the [x | 1] buffer's last reader, this tile's layer 1, is done
@@ -1304,11 +1368,11 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 {
                     // the tile after next: placement into the records (read by the
                     // next iteration's gather; this iteration's were read above)
-                    if (has_next2 && h == 1) store_p(place_b(nxt + gridDim.x, buf, lo_p2));
+                    if (has_next2 && h == 1 && !rec_ok) store_p(place_b(nxt + gridDim.x, buf, lo_p2));
                 }
                 else if (has_next && h == 0)
                 {
-                    nx = stage_b(nxt, buf ^ 1, lo_next);
+                    nx = rec_ok ? read_rec(nxt) : stage_b(nxt, buf ^ 1, lo_next);
                     // the [x | 1] buffer was last read by this tile's layer 1,
                     // which has completed
                     if constexpr (PIPE)

@@ -221,6 +221,11 @@ typedef struct
     /* nonzero: the workspace also holds the per-segment and per-ray pose
      * gradient accumulators, so that state->pose may be used */
     int pose_grad;
+    /* tensor-core paths: the forward keeps each sample's placement and
+     * gathered features for the backward, with room for this many samples
+     * per ray (0: 4 (max_samples_per_node + 1); negative: no records).  A
+     * step with more samples than the room recomputes them in the backward. */
+    int record_samples_per_ray;
 } neat_step_desc;
 
 /* Decoder paths of the fused step.

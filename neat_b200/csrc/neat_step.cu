@@ -610,8 +610,11 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
     L.sample_cap      = cap * (M + 1);
     L.tiles_cap       = (L.sample_cap + TT - 1) / TT + 1;
     // per-sample records from the forward to the backward: room for 4 (M + 1)
-    // samples per ray (a step with more recomputes them in the backward)
-    L.rec_cap         = std::min<int64_t>(L.sample_cap, std::max<int64_t>(R, 1) * (M + 1) * 4);
+    // samples per ray by default (a step with more recomputes them in the backward)
+    const int64_t rec_per_ray = d->record_samples_per_ray == 0 ? (M + 1) * 4
+                                : d->record_samples_per_ray < 0 ? 0
+                                                                : d->record_samples_per_ray;
+    L.rec_cap = std::min<int64_t>(L.sample_cap, std::max<int64_t>(R, 1) * rec_per_ray);
     L.loss_blocks     = (int)((R + 255) / 256);
     size_t smem       = 0;
     L.bwd_grid        = d->decoder_path == NEAT_DECODER_SIMT_FP32
@@ -954,7 +957,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     ta.grid_bf16    = s->grid_bf16;
     if (d->decoder_path != NEAT_DECODER_SIMT_FP32)
     {
-        ta.rec     = w.rec;
+        ta.rec     = L.rec_cap > 0 ? w.rec : nullptr;
         ta.rec_cap = L.rec_cap;
     }
     if (pmode == NEAT_PROPOSAL_SAMPLE)

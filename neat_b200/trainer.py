@@ -25,7 +25,7 @@ class FusedTrainer:
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
                  proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
                  tonemap=None, pose_grad=False, optimize_pose=False, optimize_intrinsics=False, lr_pose=1e-3,
-                 lr_intrinsics=100.0):
+                 lr_intrinsics=100.0, record_samples_per_ray=0):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -66,7 +66,8 @@ class FusedTrainer:
             intrinsics=camera.intrinsics.data_ptr(), rotation=camera.rotation.data_ptr(),
             translation=camera.translation.data_ptr(), C=self.C, G=self.G, softplus_beta=float(softplus_beta),
             max_samples_per_node=self.M, lr_grid=float(lr_grid), lr_decoder=float(lr_decoder), beta1=0.9,
-            beta2=0.999, eps=1e-8, seg_capacity=0, decoder_path=int(decoder_path))
+            beta2=0.999, eps=1e-8, seg_capacity=0, decoder_path=int(decoder_path),
+            record_samples_per_ray=int(record_samples_per_ray))
         # step number kept on the device: a captured graph of the step advances it on replay
         self.step_counter = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.state = _lib.StepState(

@@ -214,19 +214,33 @@ def test_compute_image_forward_backward(neat, oracle, case):
 PATHS = {"simt": (0, 1e-5, 1e-5, 1e-6), "bf16x3": (1, 1e-5, 1e-5, 1e-6), "bf16": (2, 1e-2, 5e-2, 5e-3)}
 
 
-def _trainer(c, path="bf16x3"):
+def _trainer(c, path="bf16x3", **kw):
     from neat_b200.trainer import FusedTrainer
     return FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, lr_grid=1e-2, lr_decoder=5e-5, seed=99,
                         grid=torch.from_numpy(c.grid), decoder=torch.from_numpy(c.dec),
-                        decoder_path=PATHS[path][0])
+                        decoder_path=PATHS[path][0], **kw)
 
 
 @pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("which", ["cfg1", "adaptive", "c8"])
 def test_fused_step_matches_f64(neat, oracle, case, adaptive_case, c8_case, which, path):
     c = {"cfg1": case, "adaptive": adaptive_case, "c8": c8_case}[which]
+    _check_fused_step(oracle, c, which, path)
+
+
+@pytest.mark.parametrize("path", ["bf16", "bf16x3"])
+@pytest.mark.parametrize("records", [-1, 1])
+@pytest.mark.parametrize("which", ["cfg1", "c8"])
+def test_fused_step_recomputes_without_records(neat, oracle, case, c8_case, which, records, path):
+    """The backward recomputes placement and gather when the forward kept no
+    records (-1) or the step has more samples than their room (1 per ray)."""
+    c = {"cfg1": case, "c8": c8_case}[which]
+    _check_fused_step(oracle, c, which, path, record_samples_per_ray=records)
+
+
+def _check_fused_step(oracle, c, which, path, **kw):
     _, tol_p, tol_g, tol_w = PATHS[path]
-    tr = _trainer(c, path)
+    tr = _trainer(c, path, **kw)
     pred = torch.zeros(c.R, device="cuda")
     loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
     torch.cuda.synchronize()

@@ -99,7 +99,8 @@ struct TcThreads
 // their BF16 pieces side by side along the columns (piece p at column
 // p * width), so that one MMA multiplies an A piece by several B pieces at
 // once (the weight-gradient and dX GEMMs; piece offsets HB_PC, W1_PC bytes);
-// W2, AB and the [x | 1] buffer keep whole pieces one after the other.  NX1
+// W2 [h][k] likewise (W2_PC; dH1 reads it with N = k across its pieces);
+// AB and the [x | 1] buffer keep whole pieces one after the other.  NX1
 // separate [x | 1] buffers (0 or 1): with one, the next tile's layer-1 GEMM is
 // issued from it while the current tile is still in flight (backward: behind
 // the weight-gradient GEMM; forward: behind layer 2); its rows are written
@@ -120,13 +121,14 @@ struct CfgPlan
     using HB                    = Buf<PREC, 128, P::PIECES * HBW>;
     using X1                    = Buf<PREC, 128, K1>;         // [x | 1 | 0 ..] rows
     using AB                    = Buf<PREC, 128, 2 * HH>;     // [dz2 | dz1] rows
-    using W2                    = Buf<PREC, HH, HH>;
+    using W2                    = Buf<PREC, HH, P::PIECES * HH>;  // [h][k]: W2
     using W1                    = Buf<PREC, HH, P::PIECES * K1>;  // [h][x | 1]: W1 | b1
     static constexpr int HB_PC  = HBW * 16;                   // byte offset of the next piece's columns
     static constexpr int W1_PC  = K1 * 16;
+    static constexpr int W2_PC  = HH * 16;
     static constexpr int NH     = TcThreads<PREC, BWD>::value / 128;
     static constexpr int OFF_W2 = 0;
-    static constexpr int OFF_W1 = OFF_W2 + P::PIECES * W2::BYTES;
+    static constexpr int OFF_W1 = OFF_W2 + W2::BYTES;
     static constexpr int OFF_HB = OFF_W1 + W1::BYTES;
     static constexpr int OFF_X1 = OFF_HB + HB::BYTES;
     static constexpr int X1SZ   = P::PIECES * X1::BYTES;      // one [x | 1] buffer, all pieces
@@ -155,10 +157,12 @@ struct Cfg : CfgPlan<C, PREC, BWD, (CfgPlan<C, PREC, BWD, 1>::NEED <= 232448) ? 
     // TMEM columns: D1 [0,64) Z1; D2 [64,128) Z2 / dH1; backward: D4 weight
     // gradients (h1 columns, then [x | 1] columns; with WCAT one such block per B
     // piece, summed at the end), D3 dX (one block of K1 columns per B piece).
-    // The three-piece backward (one CTA per SM) also caches activations:
-    // [128,192) h2 = silu(z2 + b2), [192,256) sigmoid(z1), and D2 holds
-    // w3 silu'(z2 + b2) between the y and dz2 epilogues; its D4 starts at 256
-    // and its dX reuses the sigmoid(z1) columns when they fit (read before dX).
+    // The three-piece backward (one CTA per SM) also caches activations: D1
+    // holds silu'(z1) once Z1 is read, [128,192) h2 = silu(z2 + b2), and D2
+    // w3 silu'(z2 + b2) between the y and dz2 epilogues.  Its dH1 takes one
+    // 64-column block per W2 piece, [64,256), after the dz2 epilogue has read
+    // h2; its D4 starts at 256 and its dX reuses dH1's last block when it fits
+    // (read before dX).
     using PP                            = Prec<PREC>;
     static constexpr bool CACHE         = BWD && PREC == BF16X3;
     static constexpr bool WCAT          = PP::PIECES * Base::NW <= 256;  // one MMA per A piece
@@ -467,7 +471,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             r           = a.decoder[O::W2 + i];
             off         = W2::off(i / HH, i % HH);
             dst         = pW2;
-            piece_bytes = W2::BYTES;
+            piece_bytes = K::W2_PC;
         }
         else
         {
@@ -505,7 +509,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
     const uint32_t tD1 = tmem, tD2 = tmem + 64, tD4 = tmem + K::D4, tD3 = tmem + K::D3;
-    const uint32_t tH2 = tmem + 128, tS1 = tmem + 192;  // activation cache (K::CACHE)
+    const uint32_t tH2 = tmem + 128;  // activation cache (K::CACHE)
     constexpr bool CACHE = K::CACHE;
 
     const int nseg         = (int)a.counters[0];
@@ -529,7 +533,6 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         return all;
     };
     constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);       // layers 1 and 2
-    constexpr uint32_t idH  = make_idesc(P::FMT, 0, 1, 128, HH);       // dH1
     constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);    // weight gradients
     constexpr int KS1       = K::K1 / P::KI;
     constexpr int KS64      = HH / P::KI;
@@ -678,7 +681,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         return o;
     };
     auto load_p = [&]() -> Place {
-        Place pl;
+        Place pl = {};
         if constexpr (K::NP > 0)
         {
             pl.q.weight = prec[0 * 128 + s];
@@ -950,10 +953,10 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             {
                 fence_after();
                 if constexpr (K::TA)
-                    gemm_ta<PREC, KS64, 32, W2::BYTES, 256>(tD2, tmem + K::TA_COL,
+                    gemm_ta<PREC, KS64, 32, K::W2_PC, 256>(tD2, tmem + K::TA_COL,
                                                             sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 else
-                    gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                    gemm<PREC, KS64, K::HB_PC, 256, K::W2_PC, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
                                                                     sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 mma_commit(mbar);
             }
@@ -1161,14 +1164,15 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 tmem_ld16(tD1 + lane + c0 + 16 * j, z);
                 if constexpr (CACHE)
                 {
-                    float sg[16];  // sigmoid(z1), kept for the dz1 epilogue
+                    float d1[16];  // silu'(z1) over z1, kept for the dz1 epilogue
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
-                        sg[i] = sigmoidf_(z[i]);
-                        z[i]  = z[i] * sg[i];
+                        const float sg = sigmoidf_(z[i]);
+                        d1[i]          = sg * (1.0f + z[i] * (1.0f - sg));
+                        z[i]           = z[i] * sg;
                     }
-                    tmem_st16(tS1 + lane + c0 + 16 * j, sg);
+                    tmem_st16(tD1 + lane + c0 + 16 * j, d1);
                 }
                 else
                 {
@@ -1188,7 +1192,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             if (issuer)
             {
                 fence_after();
-                gemm<PREC, KS64, K::HB_PC, 256, W2::BYTES, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
+                gemm<PREC, KS64, K::HB_PC, 256, K::W2_PC, 256>(tD2, sdesc(s_base + K::OFF_HB, 128, HB::RG),
                                                                  sdesc(s_base + K::OFF_W2, 128, W2::RG), idF, false);
                 mma_commit(mbar);
             }
@@ -1360,8 +1364,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 if (SPLIT_B ? t == 0 : issuer)
                 {
                     fence_after();
-                    gemm<PREC, KS64, AB::BYTES, 256, W2::BYTES, (P::KI / 8) * W2::RG>(
-                        tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), idH, false);
+                    gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W2::RG, HH, 0, 1>(
+                        tD2, sdesc(s_base + K::OFF_AB, 128, AB::RG), sdesc(s_base + K::OFF_W2, W2::RG, 128), false);
                     mma_commit(mbar);
                 }
                 if constexpr (SPLIT_B)
@@ -1393,16 +1397,20 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     float g[16];
                     if constexpr (CACHE)
                     {
-                        uint32_t gr[16], zr[16], sr[16];
-                        tmem_ld16_async(tD2 + lane + c0 + 16 * j, gr);
-                        tmem_ld16_async(tD1 + lane + c0 + 16 * j, zr);
-                        tmem_ld16_async(tS1 + lane + c0 + 16 * j, sr);
+                        // dH1: one column block per W2 piece (gemm_cat), summed
+                        // smallest first; times the cached silu'(z1)
+                        uint32_t gr[P::PIECES][16], dr[16];
+#pragma unroll
+                        for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD2 + p * HH + lane + c0 + 16 * j, gr[p]);
+                        tmem_ld16_async(tD1 + lane + c0 + 16 * j, dr);
                         tmem_wait_ld();
 #pragma unroll
                         for (int i = 0; i < 16; ++i)
                         {
-                            const float z = __uint_as_float(zr[i]), sg = __uint_as_float(sr[i]);
-                            g[i]          = __uint_as_float(gr[i]) * (sg * (1.0f + z * (1.0f - sg)));
+                            float v = __uint_as_float(gr[P::PIECES - 1][i]);
+#pragma unroll
+                            for (int p = P::PIECES - 2; p >= 0; --p) v += __uint_as_float(gr[p][i]);
+                            g[i] = v * __uint_as_float(dr[i]);
                         }
                     }
                     else

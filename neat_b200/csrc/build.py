@@ -20,7 +20,7 @@ BUILD = os.path.join(ROOT, "_build", "neat_b200")
 
 SOURCES = ["neat_rays.cu", "neat_step.cu", "neat_tc.cu", "neat_image.cu", "neat_igs.cu", "neat_api.cu", "neat_synth.cu",
            "neat_volume.cu", "neat_proposal.cu", "neat_regularizers.cu",
-           "neat_structure.cu", "neat_pose.cu"]
+           "neat_structure.cu", "neat_pose.cu", "neat_bwd_rec.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),

@@ -73,11 +73,20 @@ struct StepTileArgs
     // then the gathered features x[C]; used while the step's samples fit rec_cap
     float* rec;
     int64_t rec_cap;
+    // backward: nonzero when the records backward (k_bwd_rec) runs the step's
+    // tiles while its samples fit the records; this kernel then returns at once
+    int rec_skip;
     int jitter;  // 0: a = 0.5 (evaluation), else Philox stratified offsets
     int G;
     float beta;
 };
 using StepTcArgs = StepTileArgs;
+
+// Backward tiles from the forward's per-sample records with a warp that only
+// issues the tensor-core work (neat_bwd_rec.cu): three-piece operands, C = 4
+// or 8.  Runs while the step's samples fit the records (else returns at once).
+bool bwd_rec_supported(int C);
+cudaError_t launch_bwd_rec(int C, int grid, const StepTileArgs& args, cudaStream_t st);
 
 // Camera pose gradients (neat_pose.cu): per-segment sums -> per-ray dL/do,
 // dL/dd -> per-image rotation tangent and translation, camera intrinsics.

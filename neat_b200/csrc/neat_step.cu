@@ -824,6 +824,7 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.seg_pgrad = nullptr;
     ta.rec       = nullptr;
     ta.rec_cap   = 0;
+    ta.rec_skip  = 0;
     ta.jitter    = jitter;
     ta.G         = d->G;
     ta.beta      = d->softplus_beta;

@@ -9,11 +9,13 @@
 // CUDA-core work that does not feed the next GEMM runs in the GEMM windows:
 //   wait L1_i -> h1 epilogue: silu'(z1) over Z1, h1's BF16 pieces into TMEM
 //     (the layer-2 A operand); meanwhile WG_{i-1} runs
-//   -> Z2_i, queued behind WG_{i-1}; meanwhile the scatter of tile i-1's dX
+//     (tile i+1's record loads are issued before it and land under it)
+//   -> Z2_i, queued behind WG_{i-1}; meanwhile half of the scatter of tile
+//     i-1's dX, tile i+1's grid features into the [x | 1] buffer and the
+//     dL/dpred of its rays
 //   -> h1 pieces from TMEM into HB (WG_{i-1}, the last reader of HB and AB,
 //     completed with Z2_i) -> y epilogue -> dz2
-//   -> dH1_i; meanwhile tile i+1's record: placement fields (first thread of
-//     a sample) and grid features into the [x | 1] buffer (second thread)
+//   -> dH1_i; meanwhile the rest of tile i-1's scatter, tile i+1's slot data
 //   -> dz1 -> dX_i and right behind it L1_{i+1} (Z1's columns were read by
 //     the dz1 epilogue) -> dX into registers
 //   -> WG_i = [dz2 | dz1]^T [h1 | x | 1], under tile i+1's h1 epilogue.
@@ -206,6 +208,30 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             }
             return o;
         };
+        // The fields alone, issued a tile phase ahead of use: dL/dpred of the
+        // ray (a dependent load) and the slot data come later.
+        struct Raw
+        {
+            float lu, lv, lw, wgt, t;
+            int ray, row, seg;
+            bool valid;
+        };
+        auto load_raw = [&](int64_t tl) -> Raw {
+            Raw o;
+            const int64_t i = tl * 128 + s;
+            o.valid         = i < S;
+            const int64_t cp = a.rec_cap;
+            const float* r   = a.rec;
+            o.lu             = o.valid ? __ldcs(r + 0 * cp + i) : 0.0f;
+            o.lv             = o.valid ? __ldcs(r + 1 * cp + i) : 0.0f;
+            o.lw             = o.valid ? __ldcs(r + 2 * cp + i) : 0.0f;
+            o.wgt            = o.valid ? __ldcs(r + 3 * cp + i) : 0.0f;
+            o.t              = o.valid ? __ldcs(r + 4 * cp + i) : 0.0f;
+            o.ray            = o.valid ? __float_as_int(__ldcs(r + 5 * cp + i)) : 0;
+            o.row            = o.valid ? __float_as_int(__ldcs(r + 6 * cp + i)) : 0;
+            o.seg            = o.valid ? __float_as_int(__ldcs(r + 7 * cp + i)) : -1;
+            return o;
+        };
         auto read_x = [&](int64_t tl, float (&x)[C]) {
             const int64_t i = tl * 128 + s;
 #pragma unroll
@@ -238,15 +264,42 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             qd[4 * 128 + s] = __int_as_float(r.valid ? 1 : -1);
             qd[5 * 128 + s] = __int_as_float(r.row);
         };
-        // dX scattered with the trilinear weights, 4 of the 8 corners per thread
-        auto scatter = [&](const float (&dx)[C], float lu, float lv, float lw, int row, bool valid) {
+        // dX scattered with the trilinear weights: of the 8 corners, this
+        // thread takes 4 h + 2 part and 4 h + 2 part + 1 (parts 0 and 1 run in
+        // different GEMM windows)
+        auto scatter = [&](int part, const float (&dx)[C], float lu, float lv, float lw, int row, bool valid) {
             if (!valid) return;
             Corners kc;
             igs_corners(lu, lv, lw, a.G, a.G, a.G, kc);
             if (h == 0)
-                scatter_cl_half<C>(a.grid_grad, row, a.G, kc, dx, 0);
+            {
+                if (part == 0)
+                    scatter_cl_part<C, 0, 2>(a.grid_grad, row, a.G, kc, dx);
+                else
+                    scatter_cl_part<C, 2, 2>(a.grid_grad, row, a.G, kc, dx);
+            }
             else
-                scatter_cl_half<C>(a.grid_grad, row, a.G, kc, dx, 1);
+            {
+                if (part == 0)
+                    scatter_cl_part<C, 4, 2>(a.grid_grad, row, a.G, kc, dx);
+                else
+                    scatter_cl_part<C, 6, 2>(a.grid_grad, row, a.G, kc, dx);
+            }
+        };
+        // the previous tile's scatter, part 0 or 1 (the first thread of a
+        // sample holds its placement; the second reads it from sq)
+        auto scatter_prev = [&](int part, int pqb, const float (&pdx)[C], float plu, float plv, float plw, int prow,
+                                bool pvalid) {
+            if (h == 0)
+            {
+                scatter(part, pdx, plu, plv, plw, prow, pvalid);
+            }
+            else
+            {
+                const float* qd = sq + pqb * L::QB;
+                scatter(part, pdx, qd[0 * 128 + s], qd[1 * 128 + s], qd[2 * 128 + s], __float_as_int(qd[5 * 128 + s]),
+                        __float_as_int(qd[4 * 128 + s]) >= 0);
+            }
         };
         // camera pose gradient terms of one sample (first thread of the sample):
         // dL/d(ix, iy, iz) = sum over corners of (grid_q . dX) dw_q/d(ix, iy, iz),
@@ -377,6 +430,17 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 ok = false;
                 break;
             }
+            // ---- the next tile's record, in flight during the h1 epilogue:
+            //      placement fields (first thread), grid features (second)
+            Raw nr;
+            float nxx[C];
+            if (has_next)
+            {
+                if (h == 0)
+                    nr = load_raw(nxt);
+                else
+                    read_x(nxt, nxx);
+            }
             // ---- h1 = silu(Z1): silu'(z1) over Z1; h1's pieces -> TMEM (layer-2 A operand)
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
@@ -408,20 +472,18 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             }
             tmem_wait_st();
             cready(r_z2);
-            // ---- while layer 2 runs: the previous tile's scatter
-            if (has_prev)
+            // ---- while layer 2 runs: half of the previous tile's scatter; the
+            //      next tile's grid features into the [x | 1] buffer of its
+            //      layer 1 (issued behind dX; the buffer's last reader, this
+            //      tile's layer 1, has completed); dL/dpred of its rays
+            if (has_prev) scatter_prev(0, pqb, pdx, plu, plv, plw, prow, pvalid);
+            float ndp = 0.0f;
+            if (has_next)
             {
-                if (h == 0)
-                {
-                    scatter(pdx, plu, plv, plw, prow, pvalid);
-                    if constexpr (POSE) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
-                }
-                else
-                {
-                    const float* qd = sq + pqb * L::QB;
-                    scatter(pdx, qd[0 * 128 + s], qd[1 * 128 + s], qd[2 * 128 + s], __float_as_int(qd[5 * 128 + s]),
-                            __float_as_int(qd[4 * 128 + s]) >= 0);
-                }
+                if (h == 1)
+                    put_x1(nxx, 0);
+                else if (nr.valid)
+                    ndp = a.dpred[nr.ray];
             }
             // ---- layer 2 done (and with it the previous tile's weight gradients)
             if (!cwait(m_z2, p_z2))
@@ -501,23 +563,21 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, c0 + 16 * j + i), d + i);
             }
             cready(r_dh1);
-            // ---- while dH1 runs: the next tile's record (its [x | 1] rows for
-            //      layer 1, issued behind dX; the buffer's last reader, this
-            //      tile's layer 1, has completed)
+            // ---- while dH1 runs: the rest of the previous tile's scatter; the
+            //      next tile's slot data
+            if (has_prev) scatter_prev(1, pqb, pdx, plu, plv, plw, prow, pvalid);
             Rec nx;
-            float nxx[C];
-            if (has_next)
+            if (has_next && h == 0)
             {
-                if (h == 0)
-                {
-                    nx = read_fields(nxt);
-                    put_q(nx, nqb);
-                }
-                else
-                {
-                    read_x(nxt, nxx);
-                    put_x1(nxx, 0);
-                }
+                nx.lu    = nr.lu;
+                nx.lv    = nr.lv;
+                nx.lw    = nr.lw;
+                nx.t     = nr.t;
+                nx.dvw   = ndp * nr.wgt;
+                nx.row   = nr.row;
+                nx.seg   = nr.seg;
+                nx.valid = nr.valid;
+                put_q(nx, nqb);
             }
             if (!cwait(m_dh1, p_dh1))
             {
@@ -547,6 +607,11 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
             }
             cready(r_dx);
+            // ---- while dX runs: the previous tile's pose gradient terms
+            if constexpr (POSE)
+            {
+                if (has_prev && h == 0) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
+            }
             if (!cwait(m_dx, p_dx))
             {
                 ok = false;
@@ -590,16 +655,11 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
         // ---- the last tile's scatter
         if (ok && has_prev)
         {
-            if (h == 0)
+            scatter_prev(0, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
+            scatter_prev(1, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
+            if constexpr (POSE)
             {
-                scatter(pdx, plu, plv, plw, prow, pvalid);
-                if constexpr (POSE) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
-            }
-            else
-            {
-                const float* qd = sq + ((it + 2) % 3) * L::QB;
-                scatter(pdx, qd[0 * 128 + s], qd[1 * 128 + s], qd[2 * 128 + s], __float_as_int(qd[5 * 128 + s]),
-                        __float_as_int(qd[4 * 128 + s]) >= 0);
+                if (h == 0) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
             }
         }
         // ---- the last weight-gradient GEMM

@@ -504,6 +504,32 @@ __device__ __forceinline__ void scatter_cl(float* __restrict__ grad, int64_t row
     }
 }
 
+// Corners Q0 .. Q0+NQ-1 only (a sample's scatter split over threads or over
+// phases; compile-time corners keep the corner arrays in registers).
+template <int C, int Q0, int NQ>
+__device__ __forceinline__ void scatter_cl_part(float* __restrict__ grad, int64_t row, int G, const Corners& k,
+                                                const float dx[C])
+{
+    const int64_t base = row * (int64_t)G * G * G;
+#pragma unroll
+    for (int q = Q0; q < Q0 + NQ; ++q)
+    {
+        float* p       = grad + (base + corner_cell(k, q, G, G)) * C;
+        const float wq = k.w[q];
+        if constexpr (C % 4 == 0)
+        {
+#pragma unroll
+            for (int c4 = 0; c4 < C / 4; ++c4)
+                red_add_v4(p + 4 * c4, wq * dx[4 * c4], wq * dx[4 * c4 + 1], wq * dx[4 * c4 + 2], wq * dx[4 * c4 + 3]);
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < C; ++c) atomicAdd(p + c, wq * dx[c]);
+        }
+    }
+}
+
 // Corners 4*half .. 4*half+3 only (two threads share one sample's scatter).
 template <int C>
 __device__ __forceinline__ void scatter_cl_half(float* __restrict__ grad, int64_t row, int G, const Corners& k,

@@ -8,17 +8,18 @@
 // each) hand operands to a ninth warp whose lane 0 issues every MMA, and the
 // CUDA-core work that does not feed the next GEMM runs in the GEMM windows:
 //   wait L1_i -> h1 epilogue: silu'(z1) over Z1, h1's BF16 pieces into TMEM
-//     (the layer-2 A operand); meanwhile WG_{i-1} runs
-//     (tile i+1's record loads are issued before it and land under it)
+//     (the layer-2 A operand); meanwhile WG_{i-1} runs, and tile i+1's
+//     record loads, issued just before, land
+//   -> tile i-1's dX from TMEM
 //   -> Z2_i, queued behind WG_{i-1}; meanwhile half of the scatter of tile
-//     i-1's dX, tile i+1's grid features into the [x | 1] buffer and the
-//     dL/dpred of its rays
-//   -> h1 pieces from TMEM into HB (WG_{i-1}, the last reader of HB and AB,
-//     completed with Z2_i) -> y epilogue -> dz2
-//   -> dH1_i; meanwhile the rest of tile i-1's scatter, tile i+1's slot data
-//   -> dz1 -> dX_i and right behind it L1_{i+1} (Z1's columns were read by
-//     the dz1 epilogue) -> dX into registers
-//   -> WG_i = [dz2 | dz1]^T [h1 | x | 1], under tile i+1's h1 epilogue.
+//     i-1's dX, tile i+1's grid features into the [x | 1] buffer, the
+//     dL/dpred of its rays, and (once WG_{i-1}, the last reader of HB and AB,
+//     is done) h1's pieces from TMEM into HB
+//   -> y epilogue -> dz2 -> dH1_i; meanwhile the rest of tile i-1's scatter
+//     and tile i+1's slot data
+//   -> dz1 -> L1_{i+1}, dX_i (into D2's first columns, read by tile i+1
+//     before its layer 2) and WG_i = [dz2 | dz1]^T [h1 | x | 1], which runs
+//     under tile i+1's h1 epilogue.
 // Same arithmetic as the record path of k_step_tiles_tc<C, BF16X3, true>
 // (operand splits, piece products, TMEM column blocks, f32 epilogues); only
 // the order of the grid-gradient atomics differs.
@@ -61,9 +62,11 @@ struct BwdRecPlan
     static constexpr int QB    = 6 * 128;
     static constexpr int BYTES = K::OFF_M + 96;  // 10 mbarriers, then the TMEM slot at +88
     static_assert(K::OFF_R - K::OFF_Q >= 3 * QB * 4, "three slot-data buffers must fit");
-    static_assert(K::NX1 == 1 && K::WCAT && K::CACHE && K::D3 == 192 && K::TA_COL == 128,
+    static_assert(K::NX1 == 1 && K::WCAT && K::CACHE && K::D4 == 256 && K::TA_COL == 128,
                   "TMEM plan: D1 [0,64) Z1 / silu'(z1); D2 [64,128) Z2 / w3 silu'(z2); dH1 [64,256); "
-                  "h2 [128,192); h1 pieces [128,224); dX [192,240); weight gradients [256,496)");
+                  "h2 [128,192); h1 pieces [128,224); dX [64,112) until the next tile's Z2; "
+                  "weight gradients [256,496)");
+    static_assert(3 * K::K1 <= 64, "dX column blocks must fit below the h1 pieces");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
 };
 
@@ -102,9 +105,10 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     const uint32_t s_base = smem_u32(sm);
     const uint32_t mbase  = smem_u32(sm + K::OFF_M);
     // MMA completion (tcgen05.commit, count 1)
-    const uint32_t m_l1 = mbase, m_z2 = mbase + 8, m_dh1 = mbase + 16, m_dx = mbase + 24, m_end = mbase + 32;
+    const uint32_t m_l1 = mbase, m_z2 = mbase + 8, m_dh1 = mbase + 16, m_wg = mbase + 24, m_end = mbase + 32;
     // operands ready (one arrival per compute warp, count 8)
-    const uint32_t r_x1 = mbase + 40, r_z2 = mbase + 48, r_dh1 = mbase + 56, r_dx = mbase + 64, r_wg = mbase + 72;
+    const uint32_t r_x1 = mbase + 40, r_z2 = mbase + 48, r_dh1 = mbase + 56, r_dz1 = mbase + 64;
+    const uint32_t m_dx = mbase + 72;  // dX (tcgen05.commit, count 1)
 
     // ---- decoder parameters: b2 / w3 / b3 in fp32, [W1 | b1] and W2 as MMA operand pieces
     for (int i = t; i < HH; i += BR_THREADS)
@@ -144,7 +148,8 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     if (t == 0)
     {
         for (int k = 0; k < 5; ++k) mbar_init(mbase + 8 * k, 1);
-        for (int k = 5; k < 10; ++k) mbar_init(mbase + 8 * k, 8);
+        for (int k = 5; k < 9; ++k) mbar_init(mbase + 8 * k, 8);
+        mbar_init(m_dx, 1);
     }
     if (w == 0)
     {
@@ -159,8 +164,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD1 = tmem, tD2 = tmem + 64, tH2 = tmem + 128, tTA = tmem + K::TA_COL, tD3 = tmem + K::D3,
-                   tD4 = tmem + K::D4;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tH2 = tmem + 128, tTA = tmem + K::TA_COL, tD4 = tmem + K::D4;
 
     const int64_t ntiles = (S + 127) / 128, T0 = blockIdx.x, G = gridDim.x;
     constexpr uint32_t idF = make_idesc(P::FMT, 0, 0, 128, HH);  // layers 1 and 2
@@ -376,10 +380,10 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             return r != 0;
         };
         // an MMA completion, all compute threads deciding together
-        auto cwait = [&](uint32_t bar, uint32_t& ph) -> bool {
+        auto cwait = [&](uint32_t bar, uint32_t& ph, bool also = true) -> bool {
             const bool mine = mbar_wait_bounded(bar, ph);
             ph ^= 1u;
-            const bool all = csync_and(mine);
+            const bool all = csync_and(mine && also);
             fence_after();
             return all;
         };
@@ -392,7 +396,22 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             if (l == 0) mbar_arrive(bar);
         };
 
-        uint32_t p_l1 = 0, p_z2 = 0, p_dh1 = 0, p_dx = 0;
+        uint32_t p_l1 = 0, p_z2 = 0, p_dh1 = 0, p_wg = 0, p_dx = 0;
+        // dX of the previous tile, from its column blocks in D2 (summed)
+        auto read_dx = [&](float (&dx)[C]) {
+            uint32_t v[P::PIECES][16];
+#pragma unroll
+            for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD2 + lane + p * K::K1, v[p]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+            {
+                float u = __uint_as_float(v[0][c]);
+#pragma unroll
+                for (int p = 1; p < P::PIECES; ++p) u += __uint_as_float(v[p][c]);
+                dx[c] = u;
+            }
+        };
         float dw3[HALF] = {};  // this thread's columns: sum over its samples of h2 * dy
         float db3       = 0.0f;
         bool wg_started = false;
@@ -471,6 +490,16 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 }
             }
             tmem_wait_st();
+            // ---- the previous tile's dX (issued behind this tile's layer 1),
+            //      read before layer 2 overwrites its columns
+            bool dx_ok = true;
+            if (has_prev)
+            {
+                dx_ok = mbar_wait_bounded(m_dx, p_dx);
+                p_dx ^= 1u;
+                fence_after();
+                read_dx(pdx);
+            }
             cready(r_z2);
             // ---- while layer 2 runs: half of the previous tile's scatter; the
             //      next tile's grid features into the [x | 1] buffer of its
@@ -485,13 +514,16 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 else if (nr.valid)
                     ndp = a.dpred[nr.ray];
             }
-            // ---- layer 2 done (and with it the previous tile's weight gradients)
-            if (!cwait(m_z2, p_z2))
+            // ---- once the previous tile's weight gradients (HB's last reader)
+            //      are done: h1's pieces TMEM -> HB (the weight-gradient B
+            //      operand), x -> HB; layer 2 still reads the pieces in TMEM
+            bool wg_ok = true;
+            if (has_prev)
             {
-                ok = false;
-                break;
+                wg_ok = mbar_wait_bounded(m_wg, p_wg);
+                p_wg ^= 1u;
+                fence_after();
             }
-            // ---- h1's pieces TMEM -> HB (the weight-gradient B operand), x -> HB
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
@@ -510,10 +542,14 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 }
             }
             if (h == 1) put_x1(cx, -1);
-            // h2 (written below) takes columns of the h1 pieces just read
+            // ---- layer 2 done; every thread's reads of the h1 pieces, whose
+            //      columns h2 takes below, are done
             fence_before();
-            csync();
-            fence_after();
+            if (!cwait(m_z2, p_z2, wg_ok && dx_ok))
+            {
+                ok = false;
+                break;
+            }
             // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2) kept in TMEM
             {
                 float yp = 0.0f;
@@ -565,7 +601,14 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             cready(r_dh1);
             // ---- while dH1 runs: the rest of the previous tile's scatter; the
             //      next tile's slot data
-            if (has_prev) scatter_prev(1, pqb, pdx, plu, plv, plw, prow, pvalid);
+            if (has_prev)
+            {
+                scatter_prev(1, pqb, pdx, plu, plv, plw, prow, pvalid);
+                if constexpr (POSE)
+                {
+                    if (h == 0) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
+                }
+            }
             Rec nx;
             if (has_next && h == 0)
             {
@@ -606,33 +649,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 for (int i = 0; i < 16; i += P::E)
                     store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
             }
-            cready(r_dx);
-            // ---- while dX runs: the previous tile's pose gradient terms
-            if constexpr (POSE)
-            {
-                if (has_prev && h == 0) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);
-            }
-            if (!cwait(m_dx, p_dx))
-            {
-                ok = false;
-                break;
-            }
-            // ---- dX: one column block per [W1 | b1] piece, summed
-            {
-                uint32_t dxv[P::PIECES][16];
-#pragma unroll
-                for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD3 + lane + p * K::K1, dxv[p]);
-                tmem_wait_ld();
-#pragma unroll
-                for (int c = 0; c < C; ++c)
-                {
-                    float v = __uint_as_float(dxv[0][c]);
-#pragma unroll
-                    for (int p = 1; p < P::PIECES; ++p) v += __uint_as_float(dxv[p][c]);
-                    pdx[c] = v;
-                }
-            }
-            cready(r_wg);  // this tile's weight gradients
+            cready(r_dz1);  // the next layer 1, this tile's dX and weight gradients
             wg_started = true;
             // this tile's sample, for its scatter during the next tile's layer 2
             plu      = cur.lu;
@@ -652,9 +669,13 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     for (int c = 0; c < C; ++c) cx[c] = nxx[c];
             }
         }
-        // ---- the last tile's scatter
+        // ---- the last tile's dX and scatter
         if (ok && has_prev)
         {
+            const bool e = mbar_wait_bounded(m_dx, p_dx);
+            fence_after();
+            if (!e) ok = false;
+            read_dx(pdx);
             scatter_prev(0, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
             scatter_prev(1, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
             if constexpr (POSE)
@@ -775,7 +796,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                                                                desc(s_base + K::OFF_W1, 128, W1::RG), idF, false);
                 mma_commit(m_l1);
             };
-            uint32_t p_x1 = 0, p_z2 = 0, p_dh1 = 0, p_dx = 0, p_wg = 0;
+            uint32_t p_x1 = 0, p_z2 = 0, p_dh1 = 0, p_dz1 = 0;
             bool iok    = iwait(r_x1, p_x1);
             bool wg_acc = false;
             if (iok) issue_l1();
@@ -790,18 +811,19 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W2::RG, HH, 0, 1>(
                     tD2, desc(s_base + K::OFF_AB, 128, AB::RG), desc(s_base + K::OFF_W2, W2::RG, 128), false);
                 mma_commit(m_dh1);
-                // dX = dz1 . [W1 | b1]
-                if (!(iok = iwait(r_dx, p_dx))) break;
+                // dz1 in AB: the next tile's layer 1 (its Z1 columns were read
+                // by the dz1 epilogue), this tile's dX into D2's first columns
+                // (free until the next tile's layer 2; read before it), then
+                // this tile's weight gradients
+                if (!(iok = iwait(r_dz1, p_dz1))) break;
+                if (tile + G < ntiles) issue_l1();
                 gemm_cat<PREC, KS64, AB::BYTES, 256, (P::KI / 8) * W1::RG, K::K1, 0, 1>(
-                    tD3, desc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG),
+                    tD2, desc(s_base + K::OFF_AB + (HH / 8) * 128, 128, AB::RG),
                     desc(s_base + K::OFF_W1, W1::RG, 128), false);
                 mma_commit(m_dx);
-                // the next tile's layer 1 (its Z1 columns were read by the dz1
-                // epilogue), ahead of this tile's weight gradients
-                if (tile + G < ntiles) issue_l1();
-                if (!(iok = iwait(r_wg, p_wg))) break;
                 gemm_cat<PREC, KS128, AB::BYTES, (P::KI / 8) * AB::RG, (P::KI / 8) * HB::RG, K::NW, 1, 1>(
                     tD4, desc(s_base + K::OFF_AB, AB::RG, 128), desc(s_base + K::OFF_HB, HB::RG, 128), wg_acc);
+                mma_commit(m_wg);
                 wg_acc = true;
             }
             // nothing of this CTA in flight past this point

@@ -15,11 +15,12 @@
 //     i-1's dX, tile i+1's grid features into the [x | 1] buffer, the
 //     dL/dpred of its rays, and (once WG_{i-1}, the last reader of HB and AB,
 //     is done) h1's pieces from TMEM into HB
-//   -> y epilogue -> dz2 -> dH1_i; meanwhile the rest of tile i-1's scatter
-//     and tile i+1's slot data
+//   -> y epilogue -> dz2 -> dH1_i; meanwhile more of tile i-1's scatter and
+//     tile i+1's slot data
 //   -> dz1 -> L1_{i+1}, dX_i (into D2's first columns, read by tile i+1
 //     before its layer 2) and WG_i = [dz2 | dz1]^T [h1 | x | 1], which runs
-//     under tile i+1's h1 epilogue.
+//     under tile i+1's h1 epilogue; until L1_{i+1} is done, the last part of
+//     tile i-1's scatter.
 // Same arithmetic as the record path of k_step_tiles_tc<C, BF16X3, true>
 // (operand splits, piece products, TMEM column blocks, f32 epilogues); only
 // the order of the grid-gradient atomics differs.
@@ -269,8 +270,8 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             qd[5 * 128 + s] = __int_as_float(r.row);
         };
         // dX scattered with the trilinear weights: of the 8 corners, this
-        // thread takes 4 h + 2 part and 4 h + 2 part + 1 (parts 0 and 1 run in
-        // different GEMM windows)
+        // thread takes 4 h .. 4 h + 3, in three parts run in different windows
+        // (part 0: corners 4 h, 4 h + 1; part 1: 4 h + 2; part 2: 4 h + 3)
         auto scatter = [&](int part, const float (&dx)[C], float lu, float lv, float lw, int row, bool valid) {
             if (!valid) return;
             Corners kc;
@@ -279,15 +280,19 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             {
                 if (part == 0)
                     scatter_cl_part<C, 0, 2>(a.grid_grad, row, a.G, kc, dx);
+                else if (part == 1)
+                    scatter_cl_part<C, 2, 1>(a.grid_grad, row, a.G, kc, dx);
                 else
-                    scatter_cl_part<C, 2, 2>(a.grid_grad, row, a.G, kc, dx);
+                    scatter_cl_part<C, 3, 1>(a.grid_grad, row, a.G, kc, dx);
             }
             else
             {
                 if (part == 0)
                     scatter_cl_part<C, 4, 2>(a.grid_grad, row, a.G, kc, dx);
+                else if (part == 1)
+                    scatter_cl_part<C, 6, 1>(a.grid_grad, row, a.G, kc, dx);
                 else
-                    scatter_cl_part<C, 6, 2>(a.grid_grad, row, a.G, kc, dx);
+                    scatter_cl_part<C, 7, 1>(a.grid_grad, row, a.G, kc, dx);
             }
         };
         // the previous tile's scatter, part 0 or 1 (the first thread of a
@@ -461,11 +466,16 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     read_x(nxt, nxx);
             }
             // ---- h1 = silu(Z1): silu'(z1) over Z1; h1's pieces -> TMEM (layer-2 A operand)
+            uint32_t z1r[HALF / 16][16];
+#pragma unroll
+            for (int j = 0; j < HALF / 16; ++j) tmem_ld16_async(tD1 + lane + c0 + 16 * j, z1r[j]);
+            tmem_wait_ld();
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
                 float z[16], d1[16];
-                tmem_ld16(tD1 + lane + c0 + 16 * j, z);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) z[i] = __uint_as_float(z1r[j][i]);
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
                 {
@@ -553,11 +563,16 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2) kept in TMEM
             {
                 float yp = 0.0f;
+                uint32_t z2r[HALF / 16][16];
+#pragma unroll
+                for (int j = 0; j < HALF / 16; ++j) tmem_ld16_async(tD2 + lane + c0 + 16 * j, z2r[j]);
+                tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float z[16], g[16];
-                    tmem_ld16(tD2 + lane + c0 + 16 * j, z);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) z[i] = __uint_as_float(z2r[j][i]);
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
@@ -650,6 +665,8 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
             }
             cready(r_dz1);  // the next layer 1, this tile's dX and weight gradients
+            // ---- while the next layer 1 runs: the last part of the previous tile's scatter
+            if (has_prev) scatter_prev(2, pqb, pdx, plu, plv, plw, prow, pvalid);
             wg_started = true;
             // this tile's sample, for its scatter during the next tile's layer 2
             plu      = cur.lu;
@@ -678,6 +695,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             read_dx(pdx);
             scatter_prev(0, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
             scatter_prev(1, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
+            scatter_prev(2, (it + 2) % 3, pdx, plu, plv, plw, prow, pvalid);
             if constexpr (POSE)
             {
                 if (h == 0) pose_sample(pdx, plu, plv, plw, pt, prow, pseg, pvalid);

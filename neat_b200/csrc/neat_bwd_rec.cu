@@ -64,9 +64,8 @@ struct BwdRecPlan
     static constexpr int BYTES = K::OFF_M + 96;  // 10 mbarriers, then the TMEM slot at +88
     static_assert(K::OFF_R - K::OFF_Q >= 3 * QB * 4, "three slot-data buffers must fit");
     static_assert(K::NX1 == 1 && K::WCAT && K::CACHE && K::D4 == 256 && K::TA_COL == 128,
-                  "TMEM plan: D1 [0,64) Z1 / silu'(z1); D2 [64,128) Z2 / w3 silu'(z2); dH1 [64,256); "
-                  "h2 [128,192); h1 pieces [128,224); dX [64,112) until the next tile's Z2; "
-                  "weight gradients [256,496)");
+                  "TMEM plan: D1 [0,64) Z1 / silu'(z1); D2 [64,128) Z2; dH1 [64,256); "
+                  "h1 pieces [128,224); dX [64,112) until the next tile's Z2; weight gradients [256,496)");
     static_assert(3 * K::K1 <= 64, "dX column blocks must fit below the h1 pieces");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
 };
@@ -165,7 +164,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD1 = tmem, tD2 = tmem + 64, tH2 = tmem + 128, tTA = tmem + K::TA_COL, tD4 = tmem + K::D4;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tTA = tmem + K::TA_COL, tD4 = tmem + K::D4;
 
     const int64_t ntiles = (S + 127) / 128, T0 = blockIdx.x, G = gridDim.x;
     constexpr uint32_t idF = make_idesc(P::FMT, 0, 0, 128, HH);  // layers 1 and 2
@@ -560,7 +559,9 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 ok = false;
                 break;
             }
-            // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2) kept in TMEM
+            // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2)
+            //      kept in registers for the dz2 epilogue
+            float gk[HALF], h2k[HALF];
             {
                 float yp = 0.0f;
                 uint32_t z2r[HALF / 16][16];
@@ -570,23 +571,18 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
 #pragma unroll
                 for (int j = 0; j < HALF / 16; ++j)
                 {
-                    float z[16], g[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) z[i] = __uint_as_float(z2r[j][i]);
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
-                        const int col  = c0 + 16 * j + i;
-                        const float zz = z[i] + sb2[col];
-                        const float sg = sigmoidf_(zz);
-                        z[i]           = zz * sg;
-                        yp             = fmaf(z[i], sw3[col], yp);
-                        g[i]           = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                        const int col   = c0 + 16 * j + i;
+                        const float zz  = __uint_as_float(z2r[j][i]) + sb2[col];
+                        const float sg  = sigmoidf_(zz);
+                        const float h2  = zz * sg;
+                        yp              = fmaf(h2, sw3[col], yp);
+                        h2k[16 * j + i] = h2;
+                        gk[16 * j + i]  = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
                     }
-                    tmem_st16(tD2 + lane + c0 + 16 * j, g);
-                    tmem_st16(tH2 + lane + c0 + 16 * j, z);
                 }
-                tmem_wait_st();
                 sval[h * 128 + s] = yp;
             }
             csync();
@@ -598,16 +594,12 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
-                uint32_t g[16], h2[16];
                 float d[16];
-                tmem_ld16_async(tD2 + lane + c0 + 16 * j, g);
-                tmem_ld16_async(tH2 + lane + c0 + 16 * j, h2);
-                tmem_wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
                 {
-                    d[i]            = dy * __uint_as_float(g[i]);
-                    dw3[16 * j + i] = fmaf(__uint_as_float(h2[i]), dy, dw3[16 * j + i]);
+                    d[i]            = dy * gk[16 * j + i];
+                    dw3[16 * j + i] = fmaf(h2k[16 * j + i], dy, dw3[16 * j + i]);
                 }
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E)
@@ -642,27 +634,36 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 ok = false;
                 break;
             }
-            // ---- dz1 = dH1 silu'(z1) -> AB[:, 64 + c0 ..] (dH1: one column block per W2 piece)
-#pragma unroll
-            for (int j = 0; j < HALF / 16; ++j)
+            // ---- dz1 = dH1 silu'(z1) -> AB[:, 64 + c0 ..] (dH1: one column block per
+            //      W2 piece); the second chunk's loads in flight during the first's work
             {
-                uint32_t gr[P::PIECES][16], dr[16];
-                float g[16];
+                uint32_t gr[HALF / 16][P::PIECES][16], dr[HALF / 16][16];
+                auto load = [&](int j) {
 #pragma unroll
-                for (int p = 0; p < P::PIECES; ++p) tmem_ld16_async(tD2 + p * HH + lane + c0 + 16 * j, gr[p]);
-                tmem_ld16_async(tD1 + lane + c0 + 16 * j, dr);
+                    for (int p = 0; p < P::PIECES; ++p)
+                        tmem_ld16_async(tD2 + p * HH + lane + c0 + 16 * j, gr[j][p]);
+                    tmem_ld16_async(tD1 + lane + c0 + 16 * j, dr[j]);
+                };
+                load(0);
                 tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
+                for (int j = 0; j < HALF / 16; ++j)
                 {
-                    float v = __uint_as_float(gr[P::PIECES - 1][i]);
+                    if (j + 1 < HALF / 16) load(j + 1);
+                    float g[16];
 #pragma unroll
-                    for (int p = P::PIECES - 2; p >= 0; --p) v += __uint_as_float(gr[p][i]);
-                    g[i] = v * __uint_as_float(dr[i]);
+                    for (int i = 0; i < 16; ++i)
+                    {
+                        float v = __uint_as_float(gr[j][P::PIECES - 1][i]);
+#pragma unroll
+                        for (int p = P::PIECES - 2; p >= 0; --p) v += __uint_as_float(gr[j][p][i]);
+                        g[i] = v * __uint_as_float(dr[j][i]);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 16; i += P::E)
+                        store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
+                    if (j + 1 < HALF / 16) tmem_wait_ld();
                 }
-#pragma unroll
-                for (int i = 0; i < 16; i += P::E)
-                    store_chunk<PREC>(sm + K::OFF_AB, AB::BYTES, AB::off(s, HH + c0 + 16 * j + i), g + i);
             }
             cready(r_dz1);  // the next layer 1, this tile's dX and weight gradients
             // ---- while the next layer 1 runs: the last part of the previous tile's scatter

@@ -51,7 +51,7 @@ namespace tc
 // sub-partition's register file); setmaxnreg then moves them to the compute
 // warps: 8 x 32 x 224 + 4 x 32 x 56 = 384 x 168.
 constexpr int BR_THREADS = 384;
-constexpr int BR_REGS_COMPUTE = 208, BR_REGS_MMA = 88;
+constexpr int BR_REGS_COMPUTE = 192, BR_REGS_MMA = 120;
 static_assert(8 * BR_REGS_COMPUTE + 4 * BR_REGS_MMA <= 12 * 168, "register split exceeds the launch's registers");
 
 template <int C>
@@ -416,7 +416,9 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 dx[c] = u;
             }
         };
-        float dw3[HALF] = {};  // this thread's columns: sum over its samples of h2 * dy
+        float2 dw3[HALF / 2];  // this thread's columns (pairs): sum over its samples of h2 * dy
+#pragma unroll
+        for (int i = 0; i < HALF / 2; ++i) dw3[i] = make_float2(0.0f, 0.0f);
         float db3       = 0.0f;
         bool wg_started = false;
         Rec cur         = {};
@@ -472,15 +474,19 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
 #pragma unroll
             for (int j = 0; j < HALF / 16; ++j)
             {
-                float z[16], d1[16];
+                // pairs of columns in f32x2: sg = sigmoid(z), silu'(z) = sg (1 + z (1 - sg)), h1 = z sg
+                float2 hz[8];
+                float d1[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) z[i] = __uint_as_float(z1r[j][i]);
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
+                for (int i = 0; i < 8; ++i)
                 {
-                    const float sg = sigmoidf_(z[i]);
-                    d1[i]          = sg * (1.0f + z[i] * (1.0f - sg));
-                    z[i]           = z[i] * sg;
+                    const float2 z  = make_float2(__uint_as_float(z1r[j][2 * i]), __uint_as_float(z1r[j][2 * i + 1]));
+                    const float2 sg = make_float2(sigmoidf_(z.x), sigmoidf_(z.y));
+                    const float2 u  = __ffma2_rn(z, __ffma2_rn(sg, neg1x2(), one2()), one2());
+                    const float2 dd = __fmul2_rn(sg, u);
+                    d1[2 * i]       = dd.x;
+                    d1[2 * i + 1]   = dd.y;
+                    hz[i]           = __fmul2_rn(z, sg);
                 }
                 tmem_st16(tD1 + lane + c0 + 16 * j, d1);
 #pragma unroll
@@ -488,13 +494,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 {
                     uint32_t v[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                    {
-                        const __nv_bfloat162 b = __floats2bfloat162_rn(z[2 * i], z[2 * i + 1]);
-                        v[i]                   = *reinterpret_cast<const uint32_t*>(&b);
-                        z[2 * i] -= __low2float(b);  // exact: the remainder of a bf16 rounding
-                        z[2 * i + 1] -= __high2float(b);
-                    }
+                    for (int i = 0; i < 8; ++i) v[i] = piece2(hz[i]);
                     tmem_st8(tTA + lane + 32 * p + (c0 + 16 * j) / 2, v);
                 }
             }
@@ -561,9 +561,9 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             }
             // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2)
             //      kept in registers for the dz2 epilogue
-            float gk[HALF], h2k[HALF];
+            float2 gk[HALF / 2], h2k[HALF / 2];
             {
-                float yp = 0.0f;
+                float2 yp2 = make_float2(0.0f, 0.0f);
                 uint32_t z2r[HALF / 16][16];
 #pragma unroll
                 for (int j = 0; j < HALF / 16; ++j) tmem_ld16_async(tD2 + lane + c0 + 16 * j, z2r[j]);
@@ -572,18 +572,22 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 for (int j = 0; j < HALF / 16; ++j)
                 {
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
+                    for (int i = 0; i < 8; ++i)
                     {
-                        const int col   = c0 + 16 * j + i;
-                        const float zz  = __uint_as_float(z2r[j][i]) + sb2[col];
-                        const float sg  = sigmoidf_(zz);
-                        const float h2  = zz * sg;
-                        yp              = fmaf(h2, sw3[col], yp);
-                        h2k[16 * j + i] = h2;
-                        gk[16 * j + i]  = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
+                        const int col   = c0 + 16 * j + 2 * i;
+                        const float2 b2 = *reinterpret_cast<const float2*>(sb2 + col);
+                        const float2 w3 = *reinterpret_cast<const float2*>(sw3 + col);
+                        const float2 zz = __fadd2_rn(
+                            make_float2(__uint_as_float(z2r[j][2 * i]), __uint_as_float(z2r[j][2 * i + 1])), b2);
+                        const float2 sg = make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y));
+                        const float2 h2 = __fmul2_rn(zz, sg);
+                        yp2             = __ffma2_rn(h2, w3, yp2);
+                        h2k[8 * j + i]  = h2;
+                        const float2 u  = __ffma2_rn(zz, __ffma2_rn(sg, neg1x2(), one2()), one2());
+                        gk[8 * j + i]   = __fmul2_rn(w3, __fmul2_rn(sg, u));
                     }
                 }
-                sval[h * 128 + s] = yp;
+                sval[h * 128 + s] = yp2.x + yp2.y;
             }
             csync();
             const float y   = sb3[0] + sval[s] + sval[128 + s];
@@ -595,11 +599,14 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             for (int j = 0; j < HALF / 16; ++j)
             {
                 float d[16];
+                const float2 dy2 = make_float2(dy, dy);
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
+                for (int i = 0; i < 8; ++i)
                 {
-                    d[i]            = dy * gk[16 * j + i];
-                    dw3[16 * j + i] = fmaf(h2k[16 * j + i], dy, dw3[16 * j + i]);
+                    const float2 dd  = __fmul2_rn(dy2, gk[8 * j + i]);
+                    d[2 * i]         = dd.x;
+                    d[2 * i + 1]     = dd.y;
+                    dw3[8 * j + i]   = __ffma2_rn(h2k[8 * j + i], dy2, dw3[8 * j + i]);
                 }
 #pragma unroll
                 for (int i = 0; i < 16; i += P::E)
@@ -652,12 +659,17 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     if (j + 1 < HALF / 16) load(j + 1);
                     float g[16];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
+                    for (int i = 0; i < 8; ++i)
                     {
-                        float v = __uint_as_float(gr[j][P::PIECES - 1][i]);
+                        auto pr = [&](const uint32_t (&r)[16]) {
+                            return make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+                        };
+                        float2 v = pr(gr[j][P::PIECES - 1]);
 #pragma unroll
-                        for (int p = P::PIECES - 2; p >= 0; --p) v += __uint_as_float(gr[j][p][i]);
-                        g[i] = v * __uint_as_float(dr[j][i]);
+                        for (int p = P::PIECES - 2; p >= 0; --p) v = __fadd2_rn(v, pr(gr[j][p]));
+                        const float2 gg = __fmul2_rn(v, pr(dr[j]));
+                        g[2 * i]        = gg.x;
+                        g[2 * i + 1]    = gg.y;
                     }
 #pragma unroll
                     for (int i = 0; i < 16; i += P::E)
@@ -761,7 +773,11 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
         {
             float v[HALF];
 #pragma unroll
-            for (int i = 0; i < HALF; ++i) v[i] = dw3[i];
+            for (int i = 0; i < HALF / 2; ++i)
+            {
+                v[2 * i]     = dw3[i].x;
+                v[2 * i + 1] = dw3[i].y;
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
 #pragma unroll

@@ -571,27 +571,28 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             {
                 float z[16];
                 tmem_ld16(tD1 + lane + c0 + 16 * j, z);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
                 if constexpr (K::TA)
                 {
+                    float2 hz[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                    {
+                        const float2 zz = make_float2(z[2 * i], z[2 * i + 1]);
+                        hz[i]           = __fmul2_rn(zz, make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y)));
+                    }
 #pragma unroll
                     for (int p = 0; p < P::PIECES; ++p)
                     {
                         uint32_t v[8];
 #pragma unroll
-                        for (int i = 0; i < 8; ++i)
-                        {
-                            const __nv_bfloat162 b = __floats2bfloat162_rn(z[2 * i], z[2 * i + 1]);
-                            v[i]                   = *reinterpret_cast<const uint32_t*>(&b);
-                            z[2 * i] -= __low2float(b);  // exact: the remainder of a bf16 rounding
-                            z[2 * i + 1] -= __high2float(b);
-                        }
+                        for (int i = 0; i < 8; ++i) v[i] = piece2(hz[i]);
                         tmem_st8(tmem + lane + K::TA_COL + 32 * p + (c0 + 16 * j) / 2, v);
                     }
                 }
                 else
                 {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
                     store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
                     store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
                 }
@@ -638,17 +639,23 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             }
             // ---- epilogue 1: this thread's part of y
             {
-                float yp = 0.0f;
+                float2 yp2 = make_float2(0.0f, 0.0f);
 #pragma unroll 1
                 for (int j = 0; j < HALF / 16; ++j)
                 {
                     float z[16];
                     tmem_ld16(tD2 + lane + c0 + 16 * j, z);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+                    for (int i = 0; i < 8; ++i)
+                    {
+                        const int col   = c0 + 16 * j + 2 * i;
+                        const float2 zz = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]),
+                                                     *reinterpret_cast<const float2*>(sb2 + col));
+                        const float2 h2 = __fmul2_rn(zz, make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y)));
+                        yp2             = __ffma2_rn(h2, *reinterpret_cast<const float2*>(sw3 + col), yp2);
+                    }
                 }
-                sval[h * 128 + s] = yp;
+                sval[h * 128 + s] = yp2.x + yp2.y;
             }
             if (has_next2) put_starts(buf, oa2, ob2);
             fence_before();

@@ -352,26 +352,36 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
 // ---------------------------------------------------------------------------
 // operand pieces
 // ---------------------------------------------------------------------------
+// Packed pairs of f32 (sm_100 f32x2 arithmetic, round to nearest).
+__device__ __forceinline__ float2 neg1x2() { return make_float2(-1.0f, -1.0f); }
+__device__ __forceinline__ float2 one2() { return make_float2(1.0f, 1.0f); }
+// a - b (exact when the difference is representable, as a bf16 remainder is)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, neg1x2(), a); }
+
+// One BF16 piece of a pair: the packed bits, and the pair minus the piece
+// (exact: the remainder of a bf16 rounding).
+__device__ __forceinline__ uint32_t piece2(float2& r)
+{
+    const __nv_bfloat162 b = __floats2bfloat162_rn(r.x, r.y);
+    r                      = sub2(r, make_float2(__low2float(b), __high2float(b)));
+    return *reinterpret_cast<const uint32_t*>(&b);
+}
+
 // Store E = 8 consecutive values (one 16-byte chunk) as PIECES BF16 pieces,
 // piece p at base + p * piece_bytes + off.
 template <int PREC>
 __device__ __forceinline__ void store_chunk(unsigned char* base, int piece_bytes, int off, const float* v)
 {
-    float r[8];
+    float2 r[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) r[i] = v[i];
+    for (int i = 0; i < 4; ++i) r[i] = make_float2(v[2 * i], v[2 * i + 1]);
 #pragma unroll
     for (int p = 0; p < Prec<PREC>::PIECES; ++p)
     {
-        __nv_bfloat162 b[4];
+        uint32_t b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-            b[i] = __floats2bfloat162_rn(r[2 * i], r[2 * i + 1]);
-            r[2 * i] -= __low2float(b[i]);      // exact: the remainder of a bf16 rounding
-            r[2 * i + 1] -= __high2float(b[i]);
-        }
-        *reinterpret_cast<uint4*>(base + p * piece_bytes + off) = *reinterpret_cast<const uint4*>(b);
+        for (int i = 0; i < 4; ++i) b[i] = piece2(r[i]);
+        *reinterpret_cast<uint4*>(base + p * piece_bytes + off) = make_uint4(b[0], b[1], b[2], b[3]);
     }
 }
 

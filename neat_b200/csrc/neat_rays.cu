@@ -27,7 +27,6 @@ namespace neat
 {
 
 constexpr int RAY_WARPS = 4;  // rays per 128-thread block
-constexpr int MAX_PLANES = (1 << kMaxDepth) + 1;
 
 constexpr int MAX_FRONT = 256;  // a line meets at most 3 * 2^d - 2 nodes of level d (d <= 6 here)
 

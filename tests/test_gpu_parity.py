@@ -49,6 +49,13 @@ def c8_case(oracle):
     return cfg1_case(R=2048, seed=5, depth=3, C=8, G=17, M=32, oracle=oracle, adaptive=200)
 
 
+@pytest.fixture(scope="module")
+def c8_long_case(oracle):
+    # 16 k rays of the C=8 model: ~3.3 k tiles, ~22 per CTA of the backward's
+    # one-CTA-per-SM grid (long tile loops in every kernel)
+    return cfg1_case(R=16384, seed=7, depth=3, C=8, G=17, M=32, oracle=oracle, adaptive=200)
+
+
 def _camera(c):
     from neat_b200.api import CameraModel
     return CameraModel(c.w, c.h, c.intr, c.rot, c.trans)
@@ -236,6 +243,13 @@ def test_fused_step_recomputes_without_records(neat, oracle, case, c8_case, whic
     records (-1) or the step has more samples than their room (1 per ray)."""
     c = {"cfg1": case, "c8": c8_case}[which]
     _check_fused_step(oracle, c, which, path, record_samples_per_ray=records)
+
+
+@pytest.mark.parametrize("path", ["bf16x3", "bf16"])
+def test_fused_step_long_tile_loops(neat, oracle, c8_long_case, path):
+    """~22 tiles per CTA: the pipelined tile loops (records, deferred dX and
+    scatter, weight gradients under the next tile) over many iterations."""
+    _check_fused_step(oracle, c8_long_case, "c8_long", path)
 
 
 def _check_fused_step(oracle, c, which, path, **kw):

@@ -29,9 +29,11 @@
 // per warp on an mbarrier (count 8), after fence.proxy.async for shared
 // stores and tcgen05.wait::st + fence::before_thread_sync for TMEM stores;
 // the MMA warp answers each GEMM with tcgen05.commit on its own mbarrier.
-// Every wait is bounded; compute warps take each decision together
-// (bar.red.and over the 256 of them), the MMA warp gives up on its own, and
-// both drain and free TMEM before returning.
+// Every wait is bounded.  A compute thread whose wait gives up stops waiting
+// but keeps to the loop (so the named barriers of the compute warps always
+// see all 256 threads); the decision is joined (bar.red.and) after the loop.
+// The MMA warp gives up on its own; both drain and free TMEM before
+// returning.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -383,13 +385,12 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 : "memory");
             return r != 0;
         };
-        // an MMA completion, all compute threads deciding together
+        // an MMA completion (this thread's own bounded wait; none after a failure)
         auto cwait = [&](uint32_t bar, uint32_t& ph, bool also = true) -> bool {
-            const bool mine = mbar_wait_bounded(bar, ph);
+            const bool mine = ok && mbar_wait_bounded(bar, ph);
             ph ^= 1u;
-            const bool all = csync_and(mine && also);
             fence_after();
-            return all;
+            return mine && also;
         };
         // this warp's operands are in place (shared stores visible to the
         // tensor core; TMEM stores waited for by the caller)
@@ -450,11 +451,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             const int64_t nxt   = tile + G;
             const bool has_next = nxt < ntiles;
             // ---- layer 1 of this tile
-            if (!cwait(m_l1, p_l1))
-            {
-                ok = false;
-                break;
-            }
+            ok = cwait(m_l1, p_l1) && ok;
             // ---- the next tile's record, in flight during the h1 epilogue:
             //      placement fields (first thread), grid features (second)
             Raw nr;
@@ -504,7 +501,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             bool dx_ok = true;
             if (has_prev)
             {
-                dx_ok = mbar_wait_bounded(m_dx, p_dx);
+                dx_ok = ok && mbar_wait_bounded(m_dx, p_dx);
                 p_dx ^= 1u;
                 fence_after();
                 read_dx(pdx);
@@ -529,7 +526,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             bool wg_ok = true;
             if (has_prev)
             {
-                wg_ok = mbar_wait_bounded(m_wg, p_wg);
+                wg_ok = ok && mbar_wait_bounded(m_wg, p_wg);
                 p_wg ^= 1u;
                 fence_after();
             }
@@ -554,11 +551,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
             // ---- layer 2 done; every thread's reads of the h1 pieces, whose
             //      columns h2 takes below, are done
             fence_before();
-            if (!cwait(m_z2, p_z2, wg_ok && dx_ok))
-            {
-                ok = false;
-                break;
-            }
+            ok = cwait(m_z2, p_z2, wg_ok && dx_ok) && ok;
             // ---- epilogue 1: y = b3 + sum over both halves; h2 and w3 silu'(z2 + b2)
             //      kept in registers for the dz2 epilogue
             float2 gk[HALF / 2], h2k[HALF / 2];
@@ -636,11 +629,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 nx.valid = nr.valid;
                 put_q(nx, nqb);
             }
-            if (!cwait(m_dh1, p_dh1))
-            {
-                ok = false;
-                break;
-            }
+            ok = cwait(m_dh1, p_dh1) && ok;
             // ---- dz1 = dH1 silu'(z1) -> AB[:, 64 + c0 ..] (dH1: one column block per
             //      W2 piece); the second chunk's loads in flight during the first's work
             {
@@ -699,6 +688,9 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                     for (int c = 0; c < C; ++c) cx[c] = nxx[c];
             }
         }
+        // every compute thread takes the same branch below (warp-collective TMEM
+        // loads and shuffles)
+        ok = csync_and(ok);
         // ---- the last tile's dX and scatter
         if (ok && has_prev)
         {

@@ -184,6 +184,14 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         fence_after();
         return all;
     };
+    // this thread's own bounded wait (none after a failure; the loop goes on
+    // so that every barrier sees all threads)
+    auto wait_own = [&](uint32_t bar, uint32_t& ph) -> bool {
+        const bool mine = ok && mbar_wait_bounded(bar, ph);
+        ph ^= 1u;
+        fence_after();
+        return mine;
+    };
     constexpr uint32_t idF  = make_idesc(P::FMT, 0, 0, 128, HH);       // layers 1 and 2
     constexpr uint32_t idW  = make_idesc(P::FMT, 1, 1, 128, K::NW);    // weight gradients
     constexpr int KS1       = K::K1 / P::KI;
@@ -559,11 +567,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             int oa2 = INT_MAX, ob2 = INT_MAX;
             if (has_next2) fetch_starts(lo_n2, oa2, ob2);
             const int lo_n3 = nxt2 + G < ntiles ? a.tile_seg[nxt2 + G] : 0;
-            if (!wait_on(mbar_wg, phase_wg))
-            {
-                ok = false;
-                break;
-            }
+            ok = wait_own(mbar_wg, phase_wg) && ok;
             // ---- h1 = silu(Z1), this thread's columns -> layer-2 A operand: TMEM
             //      (TA: BF16 pieces, two per column) or HB[:, c0 .. c0 + HALF)
 #pragma unroll 1
@@ -632,11 +636,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     issue_l1(0);
                 }
             }
-            if (!wait_on(mbar, phase))
-            {
-                ok = false;
-                break;
-            }
+            ok = wait_own(mbar, phase) && ok;
             // ---- epilogue 1: this thread's part of y
             {
                 float2 yp2 = make_float2(0.0f, 0.0f);

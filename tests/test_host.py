@@ -131,3 +131,36 @@ def test_max_over_ranks_gloo():
         p.join(120)
     res = sorted(q.get(timeout=5) for _ in range(2))
     assert res == [(0, 11.0), (1, 11.0)]
+
+
+def test_ctypes_structs_match_header(tmp_path):
+    """Every ctypes mirror of a C-ABI struct has the header's size and field offsets
+    (a probe compiled with gcc against include/neat_b200.h)."""
+    import shutil
+    import subprocess
+    from neat_b200 import _lib
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    pairs = {"neat_step_desc": _lib.StepDesc, "neat_proposal": _lib.Proposal, "neat_tonemap": _lib.ToneMap,
+             "neat_pose_grad": _lib.PoseGrad, "neat_step_state": _lib.StepState, "neat_step_batch": _lib.StepBatch,
+             "neat_step_out": _lib.StepOut, "neat_project_out": _lib.ProjectOut}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "neat_b200.h"', "int main(void) {"]
+    for cname, cls in pairs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, *_ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0; }"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line.strip():
+            parts = line.split()
+            got[(parts[0], parts[1])] = int(parts[2])
+    for cname, cls in pairs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for fname, *_ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)

@@ -69,6 +69,26 @@ def hidden_flops(C, H=64):
     return C * H + H * H + H  # multiply-adds of one decoder forward
 
 
+def step_roofline(S, R, P, C, ms_step, peaks, simt_peak_tflops, H=64):
+    """Whole-step roofline of the path: T* = max(F / peak flops, B / HBM bandwidth) and
+    achieved = T* / measured step time.  F = 6 (C H + H^2 + H) flops per sample (the decoder
+    forward, its dX and its weight-gradient products); B = 16 R + 36 P bytes (per ray: target,
+    ray key, prediction; per FP32 grid parameter: the step's grid read and gradient write, 8 B,
+    and Adam's reads of p, g, m, v and writes of p, m, v, 28 B).  Reported against the measured
+    tensor-core (BF16, sustained) and the FP32 CUDA-core flop peaks."""
+    F = 6.0 * hidden_flops(C, H) * S
+    B = 16.0 * R + 36.0 * P
+    t_hbm = B / (peaks["hbm_gbs"] * 1e9)
+    t_tc = F / (peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")) * 1e12)
+    t_simt = F / (simt_peak_tflops * 1e12)
+    t = ms_step / 1000.0
+    return {"flops": F, "bytes": B,
+            "t_star_ms_tensor": 1e3 * max(t_tc, t_hbm), "bound_tensor": "hbm" if t_hbm >= t_tc else "tensor",
+            "frac_tensor": max(t_tc, t_hbm) / t,
+            "t_star_ms_fp32_simt": 1e3 * max(t_simt, t_hbm), "bound_fp32_simt": "hbm" if t_hbm >= t_simt else "fp32",
+            "frac_fp32_simt": max(t_simt, t_hbm) / t}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -540,6 +560,7 @@ def main():
                      "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                      "fp32_simt_peak_tflops": simt_peak,
                      "frac_of_fp32_simt": achieved / simt_peak},
+        "step_roofline": step_roofline(S, R, tr.grid.numel(), cfg["C"], ms / K, peaks, simt_peak),
         "e2e": {"value": e2e, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
         # the three-piece backward from records adds one launch (the plain
         # backward kernel then returns at once)

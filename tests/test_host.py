@@ -164,3 +164,18 @@ def test_ctypes_structs_match_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(cls), cname
         for fname, *_ in cls._fields_:
             assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_step_roofline_arithmetic():
+    """The whole-step roofline bench.py reports: F = 6 (C H + H^2 + H) S flops,
+    B = 16 R + 36 P bytes, T* = max of the flop and byte times."""
+    import bench
+    peaks = {"hbm_gbs": 1000.0, "bf16_tflops_sustained": 100.0}
+    r = bench.step_roofline(S=1000, R=10, P=100, C=8, ms_step=1.0, peaks=peaks, simt_peak_tflops=10.0)
+    F = 6.0 * (8 * 64 + 64 * 64 + 64) * 1000
+    assert r["flops"] == F and r["bytes"] == 16 * 10 + 36 * 100
+    assert r["t_star_ms_tensor"] == pytest.approx(1e3 * max(F / 100e12, 3760 / 1000e9))
+    assert r["frac_fp32_simt"] == pytest.approx(1e3 * max(F / 10e12, 3760 / 1000e9) / 1.0)
+    assert r["bound_tensor"] == "tensor" and r["bound_fp32_simt"] == "fp32"
+    r = bench.step_roofline(S=1, R=10, P=10 ** 6, C=8, ms_step=1.0, peaks=peaks, simt_peak_tflops=10.0)
+    assert r["bound_tensor"] == "hbm" and r["bound_fp32_simt"] == "hbm"

@@ -255,9 +255,10 @@ typedef struct
 /* p = (1 - mix) softmax + mix / 8.  In SAMPLE mode the step places its     */
 /* samples by inverting that piecewise-linear CDF at (j + a_j) / n (weights */
 /* by the reference's midpoint rule on the placed positions).  In TRAIN mode */
-/* the step samples uniformly (the fallback and error judge), bins every    */
-/* sample's contribution density * weight into its segment's 8 sub-intervals */
-/* and, after its own update, runs `iters` Adam iterations of the proposal  */
+/* the step samples uniformly (the fallback and the error yardstick), bins */
+/* every sample's contribution density * weight into its segment's 8       */
+/* sub-intervals and, after its own update, runs `iters` Adam iterations of */
+/* the proposal                                                             */
 /* on the cross-entropy between p and where the density changes: bin b's    */
 /* target is |m_b - m_b-1| + |m_b+1 - m_b| of the binned masses m, each     */
 /* segment weighted by its total variation (the midpoint rule is exact on  */

@@ -1,6 +1,6 @@
 """CPU execution of the reference's training step -- baseline only.
 
-TEST/BASELINE INFRASTRUCTURE: used by bench.py's cpu_baseline leg and its
+TEST AND CPU-BASELINE INFRASTRUCTURE: used by bench.py's cpu_baseline leg and its
 --impl reference arm, never by the product.
 
 The reference (darglein/NeAT) has no CPU training path for the whole step:

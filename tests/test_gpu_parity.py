@@ -4,7 +4,7 @@ Bars: bit-exact for rays, hit lists, sample counts, sample positions/weights,
 node indexing (the decisions are integer/ordering work) and for the IGS
 forward and grad_uv (same fma order); FP32 tolerances stated per test for
 everything that sums in a different order than the f64 oracle:
-  projection / loss:  1e-5 relative (north-star FP32 bar)
+  projection / loss:  1e-5 relative (the FP32 bar)
   gradients:          1e-5 relative in the 2-norm (||g - g64|| / ||g64||);
                       elementwise checks would flag cancellation noise.
 """
@@ -476,7 +476,7 @@ def test_proposal_sampling_matches_f64(neat, oracle, case, path):
 
 
 def test_proposal_training_gradient_matches_f64(neat, oracle, case):
-    """A TRAIN step: uniform (judge) sampling, contributions binned per segment,
+    """A TRAIN step: uniform sampling, contributions binned per segment,
     one proposal iteration with lr 0 -> its gradient equals the f64 oracle's
     cross-entropy gradient on the same bins."""
     c = case

@@ -400,6 +400,52 @@ class FusedTrainer:
             self._stream()), "neat_sample_volume")
         return vol, node, valid
 
+    # ---- checkpoint / resume -------------------------------------------------
+    # The reference saves the geometry module, tree and camera per epoch
+    # (samples/reconstruct.cpp:36-62, 153-199) but not the optimizer.  This state
+    # also holds the Adam moments and the step number (the jitter of a step is
+    # keyed on it), so a restored trainer takes the same next step.
+    def _state_tensors(self):
+        names = ["grid", "grid_m", "grid_v", "grid_grad", "decoder", "decoder_m", "decoder_v", "step_counter"]
+        if getattr(self, "grid_bf16", None) is not None:
+            names.append("grid_bf16")
+        if self.proposal:
+            # node descriptors: formed on the proposal's TRAIN steps, read by the SAMPLE steps between
+            names += ["prop", "prop_m", "prop_v", "prop_steps", "prop_node_desc"]
+        t = {n: getattr(self, n) for n in names}
+        if self.tonemap is not None:
+            t["tonemap_params"] = self.tonemap.params
+        if self.optimize_pose or self.optimize_intrinsics:
+            t["camera_rotation"] = self.camera.rotation
+            t["camera_translation"] = self.camera.translation
+            t["camera_intrinsics"] = self.camera.intrinsics
+        return t
+
+    def state_dict(self):
+        """Copies (on the host) of everything a step reads and updates, plus the
+        step number and the seed."""
+        torch.cuda.synchronize(self.dev)
+        sd = {n: v.detach().cpu().clone() for n, v in self._state_tensors().items()}
+        sd["step_id"] = int(self.step_id)
+        sd["seed"] = int(self.seed)
+        return sd
+
+    def load_state_dict(self, sd):
+        """Restores a state_dict() of a trainer built with the same tree, model
+        sizes and options: values are copied into the existing buffers, whose
+        device addresses the step descriptors hold."""
+        if int(sd["seed"]) != self.seed:
+            raise ValueError("state was saved by a trainer with another seed")
+        for n, v in self._state_tensors().items():
+            if n not in sd:
+                raise KeyError(f"state has no {n}")
+            if tuple(sd[n].shape) != tuple(v.shape) or sd[n].dtype != v.dtype:
+                raise ValueError(f"state {n} has shape {tuple(sd[n].shape)} {sd[n].dtype}, "
+                                 f"expected {tuple(v.shape)} {v.dtype}")
+            v.copy_(sd[n].to(v.device))
+        self.step_id = int(sd["step_id"])
+        torch.cuda.synchronize(self.dev)
+
     def check_status(self):
         st = int(self.status.item())
         if st:

@@ -179,3 +179,79 @@ def test_step_roofline_arithmetic():
     assert r["bound_tensor"] == "tensor" and r["bound_fp32_simt"] == "fp32"
     r = bench.step_roofline(S=1, R=10, P=10 ** 6, C=8, ms_step=1.0, peaks=peaks, simt_peak_tflops=10.0)
     assert r["bound_tensor"] == "hbm" and r["bound_fp32_simt"] == "hbm"
+
+
+SETTINGS_TEXT = """
+[TrainParams]
+random_seed = 3746934646
+batch_size = 16000
+lr_exex_grid_adam = 0.0399999991
+exex_op = adam
+train_interval_jitter = true
+loss_tv = 0.0000000000
+loss_edge = 0.001
+optimize_pose = true
+optimize_intrinsics = false
+lr_pose = 0.002
+lr_intrinsics = 50.0
+
+[PhotometricCalibrationParams]
+response_enable = true
+response_range = 2
+exposure_enable = true
+exposure_mult = false
+sensor_bias_enable = false
+sensor_bias_size_w = 32
+
+[Netparams]
+grid_size = 17
+grid_features = 8
+last_activation_function = softplus
+softplus_beta = 2
+decoder_skip = false
+decoder_lr = 4.999999874e-05
+decoder_activation = silu
+decoder_hidden_layers = 1
+decoder_hidden_features = 64
+
+[OctreeParams]
+start_layer = 2
+tree_depth = 4
+max_samples_per_node = 32
+tree_optimizer_params.max_active_nodes = 512
+"""
+
+
+def test_settings_map_to_trainer_arguments():
+    """The reference's INI section and key names map onto FusedTrainer arguments."""
+    from neat_b200 import config
+    st = config.load_settings(text=SETTINGS_TEXT)
+    assert st["OctreeParams"]["tree_optimizer_params.max_active_nodes"] == "512"
+    kw = config.trainer_kwargs(st)
+    assert kw["num_features"] == 8 and kw["grid_size"] == 17 and kw["max_samples_per_node"] == 32
+    assert kw["lr_grid"] == pytest.approx(0.04) and kw["lr_decoder"] == pytest.approx(5e-5)
+    assert kw["softplus_beta"] == 2.0 and kw["seed"] == 3746934646
+    assert kw["loss_edge"] == pytest.approx(0.001) and kw["loss_tv"] == 0.0
+    assert kw["optimize_pose"] is True and kw["optimize_intrinsics"] is False and kw["lr_pose"] == 0.002
+    assert kw["tonemap"] == {"response_enable": True, "response_range": 2.0, "exposure_enable": True,
+                             "exposure_mult": False, "sensor_bias_enable": False, "sensor_bias_size_w": 32}
+    run = config.run_settings(st)
+    assert run == {"batch_size": 16000, "train_interval_jitter": True, "tree_depth": 4, "start_layer": 2}
+    # the signature of FusedTrainer accepts every mapped argument
+    import inspect
+    from neat_b200.trainer import FusedTrainer
+    params = inspect.signature(FusedTrainer.__init__).parameters
+    assert all(k in params for k in kw)
+
+
+@pytest.mark.parametrize("section,key,value", [("Netparams", "decoder_hidden_layers", "2"),
+                                               ("Netparams", "decoder_hidden_features", "128"),
+                                               ("Netparams", "decoder_activation", "relu"),
+                                               ("Netparams", "decoder_skip", "true"),
+                                               ("TrainParams", "exex_op", "rms")])
+def test_settings_the_step_does_not_implement_are_refused(section, key, value):
+    from neat_b200 import config
+    st = config.load_settings(text=SETTINGS_TEXT)
+    st[section][key] = value
+    with pytest.raises(ValueError):
+        config.trainer_kwargs(st)

@@ -56,8 +56,8 @@ PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 STEP_LAUNCHES = 22
 # DRAM bytes per sample of the records backward (k_bwd_rec) from one ncu capture of
 # the same scene at 2^16 rays (dram__bytes_read.sum + dram__bytes_write.sum = 463.2 MB
-# for 2.908 M samples; profiles/bwd_rec_bf16x3_65k_rays.md), scaled to a launch by
-# its samples -- an upper bound at larger batches (more grid reuse in L2)
+# for 2.908 M samples), scaled to a launch by its samples -- an upper bound at
+# larger batches (more grid reuse in L2)
 TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 463.2e6 / 2.908e6}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_bwd_rec<C=%d> (BF16x3 backward from the forward's records, MMA warp)",

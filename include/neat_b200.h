@@ -104,8 +104,10 @@ int neat_create_samples(const void* table, int num_active, int max_depth, const 
  * live in one file-scope device array of the library, sized for at most
  * NEAT_NOALLOC_MAX_RAYS rays (about 3 MB, held on every GPU that loads the
  * library until the process exits); larger batches are rejected with
- * NEAT_ERR_CAPACITY before anything is launched.  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress); make it before
+ * NEAT_ERR_CAPACITY before any kernel is launched (out_count is zeroed
+ * first, as on the other paths).  Each call looks up that array's device
+ * address in the current context (cudaGetSymbolAddress); the first lookup on
+ * a device loads the library's module there, so make the first call before
  * any stream capture.  Every call on a device shares the one array, so calls
  * whose work overlaps on the GPU (different streams or threads without
  * ordering) race and must be serialised by the caller. */

@@ -20,12 +20,25 @@ train_interval_jitter, tree_depth, start_layer).  Settings the fused step does
 not implement raise ValueError rather than being silently ignored: a decoder
 other than Linear(C,64)-SiLU-Linear(64,64)-SiLU-Linear(64,1)-softplus, a
 grid optimizer other than Adam, or decoder skip connections.
+
+A key that is absent takes the reference's default from its struct
+initialisers: Netparams, OctreeParams and MyTrainParams in src/Settings.h
+(e.g. loss_tv 1e-4, loss_edge 1e-3, optimize_pose and optimize_intrinsics on,
+start_layer 3) and PhotometricCalibrationParams in src/modules/ToneMapper.h:36-47
+(response, exposure and sensor bias all enabled, so an absent section still
+calibrates).  batch_size and train_interval_jitter belong to saiga's
+TrainParams base, whose source is not in the reference; their defaults here are
+the values of configs/pepper.ini (16000, true).
 """
 import configparser
 
 SECTIONS = ("TrainParams", "Netparams", "OctreeParams", "PhotometricCalibrationParams")
 TONEMAP_KEYS = ("response_enable", "response_range", "response_lr", "exposure_enable", "exposure_mult",
                 "exposure_lr", "sensor_bias_enable", "sensor_bias_size_w", "sensor_bias_lr")
+# PhotometricCalibrationParams initialisers (src/modules/ToneMapper.h:36-47)
+TONEMAP_DEFAULTS = {"response_enable": True, "response_range": 2.0, "response_lr": 0.1, "exposure_enable": True,
+                    "exposure_mult": False, "exposure_lr": 0.01, "sensor_bias_enable": True,
+                    "sensor_bias_size_w": 32, "sensor_bias_lr": 0.05}
 
 
 def load_settings(path=None, text=None):
@@ -80,28 +93,26 @@ def trainer_kwargs(settings):
         "lr_grid": _get(settings, "TrainParams", "lr_exex_grid_adam", float, 0.04),
         "max_samples_per_node": _get(settings, "OctreeParams", "max_samples_per_node", int, 32),
         "seed": _get(settings, "TrainParams", "random_seed", int, 0) % (1 << 63),
-        "loss_tv": _get(settings, "TrainParams", "loss_tv", float, 0.0),
-        "loss_edge": _get(settings, "TrainParams", "loss_edge", float, 0.0),
-        "optimize_pose": _get(settings, "TrainParams", "optimize_pose", _bool, False),
-        "optimize_intrinsics": _get(settings, "TrainParams", "optimize_intrinsics", _bool, False),
+        "loss_tv": _get(settings, "TrainParams", "loss_tv", float, 1e-4),
+        "loss_edge": _get(settings, "TrainParams", "loss_edge", float, 1e-3),
+        "optimize_pose": _get(settings, "TrainParams", "optimize_pose", _bool, True),
+        "optimize_intrinsics": _get(settings, "TrainParams", "optimize_intrinsics", _bool, True),
         "lr_pose": _get(settings, "TrainParams", "lr_pose", float, 1e-3),
         "lr_intrinsics": _get(settings, "TrainParams", "lr_intrinsics", float, 100.0),
     }
-    pc = settings.get("PhotometricCalibrationParams")
-    if pc:
-        conv = {k: (_bool if k.endswith(("_enable", "_mult")) else (int if k == "sensor_bias_size_w" else float))
-                for k in TONEMAP_KEYS}
-        tm = {k: conv[k](pc[k]) for k in TONEMAP_KEYS if k in pc and str(pc[k]).strip() != ""}
-        if any(tm.get(k, False) for k in ("response_enable", "exposure_enable", "sensor_bias_enable")):
-            kw["tonemap"] = tm
+    conv = {k: (_bool if k.endswith(("_enable", "_mult")) else (int if k == "sensor_bias_size_w" else float))
+            for k in TONEMAP_KEYS}
+    tm = {k: _get(settings, "PhotometricCalibrationParams", k, conv[k], TONEMAP_DEFAULTS[k]) for k in TONEMAP_KEYS}
+    if any(tm[k] for k in ("response_enable", "exposure_enable", "sensor_bias_enable")):
+        kw["tonemap"] = tm
     return kw
 
 
 def run_settings(settings):
     """The settings of the training loop around the step."""
     return {
-        "batch_size": _get(settings, "TrainParams", "batch_size", int, 4096),
+        "batch_size": _get(settings, "TrainParams", "batch_size", int, 16000),
         "train_interval_jitter": _get(settings, "TrainParams", "train_interval_jitter", _bool, True),
         "tree_depth": _get(settings, "OctreeParams", "tree_depth", int, 4),
-        "start_layer": _get(settings, "OctreeParams", "start_layer", int, 2),
+        "start_layer": _get(settings, "OctreeParams", "start_layer", int, 3),
     }

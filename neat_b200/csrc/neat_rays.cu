@@ -611,8 +611,6 @@ extern "C" int neat_create_samples(const void* table, int num_active, int max_de
 // every entry they read before reading it, so nothing needs clearing between
 // calls, but calls that overlap on the GPU race on it.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 namespace neat
 {
 constexpr int64_t kNoAllocRays = NEAT_NOALLOC_MAX_RAYS;
@@ -626,25 +624,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[neat::kNoAllocB
 
 namespace
 {
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device, looked up once
-// per device (the host-side name is only a stand-in, never a device pointer).
+// Device address of g_noalloc_scratch in the current device's context (the
+// host-side name is only a stand-in, never a device pointer).  Looked up on
+// every call rather than cached per device ordinal: after a context is torn
+// down and created again the module is loaded anew and the array may move.
+// Once the module is loaded the lookup is a table read.
 int noalloc_scratch(char** out)
 {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) return NEAT_ERR_CUDA;
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return NEAT_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev])
-    {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return NEAT_ERR_CUDA;
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = (char*)g_noalloc_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return NEAT_ERR_CUDA;
+    *out = (char*)p;
     return NEAT_OK;
 }
 }  // namespace
@@ -659,9 +648,9 @@ extern "C" int neat_create_samples_noalloc(const void* table, int num_active, in
     if (num_rays < 0 || num_active < 0 || max_depth < 1 || max_depth > kMaxDepth || max_samples_per_node < 1 ||
         capacity < 0 || !out_count)
         return NEAT_ERR_BAD_INPUT;
-    if (num_rays > kNoAllocRays) return NEAT_ERR_CAPACITY;  // beyond the static scratch: nothing launched
     cudaStream_t st = (cudaStream_t)stream;
     if (cudaMemsetAsync(out_count, 0, 2 * sizeof(int64_t), st) != cudaSuccess) return NEAT_ERR_CUDA;
+    if (num_rays > kNoAllocRays) return NEAT_ERR_CAPACITY;  // beyond the static scratch: no kernel launched
     if (num_rays == 0) return NEAT_OK;
     if (!table && num_active > 0) return NEAT_ERR_BAD_INPUT;
     if (!origin || !direction) return NEAT_ERR_BAD_INPUT;

@@ -10,6 +10,7 @@ the device until the caller reads it.
 import ctypes
 import math
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -361,6 +362,14 @@ class FusedTrainer:
             new_tables["active"].data_ptr(), A, new_tables["min"].data_ptr(), new_tables["max"].data_ptr(),
             old_tables["table"].data_ptr(), self.tree.max_depth, old_first, old_grid.data_ptr(), self.C, self.G,
             grid.data_ptr(), self._stream()), "neat_interpolate_grid")
+        self._adopt_tree(new_tree, grid)
+
+    def _adopt_tree(self, new_tree, grid):
+        """Point the step at new_tree with `grid` ([A, G, G, G, C]) as its grid:
+        fresh Adam moments and gradient buffers, descriptors and workspace
+        rebuilt for the new active-node count."""
+        new_tables = new_tree.device_tables(self.dev)
+        A = new_tree.NumActiveNodes()
         self.tree, self.tables, self.A, self.grid = new_tree, new_tables, A, grid
         self.grid_m = torch.zeros_like(grid)
         self.grid_v = torch.zeros_like(grid)
@@ -404,7 +413,10 @@ class FusedTrainer:
     # The reference saves the geometry module, tree and camera per epoch
     # (samples/reconstruct.cpp:36-62, 153-199) but not the optimizer.  This state
     # also holds the Adam moments and the step number (the jitter of a step is
-    # keyed on it), so a restored trainer takes the same next step.
+    # keyed on it), so a restored trainer takes the same next step.  The tree is
+    # saved as its depth and active-node ids (the node boxes follow from the
+    # depth: HyperTreeBase builds them deterministically), so the grid rows are
+    # restored onto the nodes they belong to after any restructure().
     def _state_tensors(self):
         names = ["grid", "grid_m", "grid_v", "grid_grad", "decoder", "decoder_m", "decoder_v", "step_counter"]
         if getattr(self, "grid_bf16", None) is not None:
@@ -426,16 +438,33 @@ class FusedTrainer:
         step number and the seed."""
         torch.cuda.synchronize(self.dev)
         sd = {n: v.detach().cpu().clone() for n, v in self._state_tensors().items()}
+        sd["tree_max_depth"] = int(self.tree.max_depth)
+        sd["tree_active_node_ids"] = torch.from_numpy(self.tree.active_node_ids.copy())
         sd["step_id"] = int(self.step_id)
         sd["seed"] = int(self.seed)
         return sd
 
     def load_state_dict(self, sd):
-        """Restores a state_dict() of a trainer built with the same tree, model
-        sizes and options: values are copied into the existing buffers, whose
-        device addresses the step descriptors hold."""
+        """Restores a state_dict() of a trainer built with the same tree depth,
+        model sizes and options.  When the saved active-node set differs from
+        this trainer's (a checkpoint taken after restructure()), the trainer
+        first moves to the saved structure; then every value is copied into the
+        trainer's buffers, whose device addresses the step descriptors hold."""
         if int(sd["seed"]) != self.seed:
             raise ValueError("state was saved by a trainer with another seed")
+        if "tree_max_depth" not in sd or "tree_active_node_ids" not in sd:
+            raise KeyError("state has no tree (tree_max_depth, tree_active_node_ids)")
+        if int(sd["tree_max_depth"]) != self.tree.max_depth:
+            raise ValueError(f"state was saved with a depth-{int(sd['tree_max_depth'])} tree, "
+                             f"this trainer's tree has depth {self.tree.max_depth}")
+        ids = sd["tree_active_node_ids"].cpu().numpy().astype(np.int64)
+        if not np.array_equal(ids, self.tree.active_node_ids):
+            if ids.size == 0 or ids.min() < 0 or ids.max() >= self.tree.NumNodes() or np.any(np.diff(ids) <= 0):
+                raise ValueError("state holds an invalid active-node set")
+            tree = self.tree.copy()
+            tree.SetActiveNodes(ids)
+            self._adopt_tree(tree, torch.empty((tree.NumActiveNodes(), self.G, self.G, self.G, self.C),
+                                               dtype=torch.float32, device=self.dev))
         for n, v in self._state_tensors().items():
             if n not in sd:
                 raise KeyError(f"state has no {n}")

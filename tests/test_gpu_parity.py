@@ -864,6 +864,52 @@ def test_checkpoint_resume_reproduces_the_next_step(neat, case, proposal):
         b.load_state_dict(sd2)
 
 
+def test_checkpoint_after_restructure_restores_the_saved_tree(neat, case):
+    """A checkpoint taken after restructure() holds the new active-node set; a
+    trainer built on the original tree moves to that set before copying the
+    grid rows, so every row lands on its own node and the next step matches."""
+    from neat_b200.trainer import FusedTrainer
+
+    def make():
+        return FusedTrainer(case.tree, _camera(case), case.C, case.G, case.M, lr_grid=1e-2, lr_decoder=5e-5, seed=7,
+                            grid=torch.from_numpy(case.grid), decoder=torch.from_numpy(case.dec))
+    uv, img, tgt = _dev(case.uv), _dev(case.img), _dev(case.target)
+    a = make()
+    a.step(uv, img, tgt)
+    # split two leaves' parents... the depth-2 tree: keep every other leaf and activate
+    # the depth-1 parent of the first leaf instead of its 8 children
+    T = case.tree
+    first = int(T.active_node_ids[0])
+    parent = int(T.node_parent[first])
+    kids = set(int(k) for k in T.node_children[parent])
+    new_ids = sorted([parent] + [int(i) for i in T.active_node_ids if int(i) not in kids])
+    nt = T.copy()
+    nt.SetActiveNodes(new_ids)
+    a.restructure(nt)
+    a.step(uv, img, tgt)
+    a.check_status()
+    sd = a.state_dict()
+    assert sd["tree_active_node_ids"].tolist() == new_ids
+    la = float(a.step(uv, img, tgt).item())
+    b = make()
+    assert b.A != a.A
+    b.load_state_dict(sd)
+    assert b.A == a.A and np.array_equal(b.tree.active_node_ids, np.asarray(new_ids))
+    assert torch.equal(b.grid.cpu(), sd["grid"])
+    lb = float(b.step(uv, img, tgt).item())
+    torch.cuda.synchronize()
+    b.check_status()
+    assert lb == pytest.approx(la, rel=1e-6)
+    # a checkpoint of another depth, or without a tree, is refused
+    bad = dict(sd)
+    bad["tree_max_depth"] = T.max_depth + 1
+    with pytest.raises(ValueError):
+        b.load_state_dict(bad)
+    bad = {k: v for k, v in sd.items() if k != "tree_active_node_ids"}
+    with pytest.raises(KeyError):
+        b.load_state_dict(bad)
+
+
 def test_pose_sgd_step(neat, oracle):
     """neat_pose_sgd: SGD on tangent / translation / intrinsics, q <- exp(-lr g) q
     renormalised, gradients zeroed; the optimize flags select the groups."""

@@ -233,8 +233,10 @@ def test_settings_map_to_trainer_arguments():
     assert kw["softplus_beta"] == 2.0 and kw["seed"] == 3746934646
     assert kw["loss_edge"] == pytest.approx(0.001) and kw["loss_tv"] == 0.0
     assert kw["optimize_pose"] is True and kw["optimize_intrinsics"] is False and kw["lr_pose"] == 0.002
-    assert kw["tonemap"] == {"response_enable": True, "response_range": 2.0, "exposure_enable": True,
-                             "exposure_mult": False, "sensor_bias_enable": False, "sensor_bias_size_w": 32}
+    # keys the section lists, the rest from PhotometricCalibrationParams' initialisers
+    assert kw["tonemap"] == {"response_enable": True, "response_range": 2.0, "response_lr": 0.1,
+                             "exposure_enable": True, "exposure_mult": False, "exposure_lr": 0.01,
+                             "sensor_bias_enable": False, "sensor_bias_size_w": 32, "sensor_bias_lr": 0.05}
     run = config.run_settings(st)
     assert run == {"batch_size": 16000, "train_interval_jitter": True, "tree_depth": 4, "start_layer": 2}
     # the signature of FusedTrainer accepts every mapped argument
@@ -242,6 +244,32 @@ def test_settings_map_to_trainer_arguments():
     from neat_b200.trainer import FusedTrainer
     params = inspect.signature(FusedTrainer.__init__).parameters
     assert all(k in params for k in kw)
+
+
+def test_settings_defaults_follow_the_reference():
+    """An INI without the keys gets the reference's struct initialisers
+    (src/Settings.h: Netparams :46-57, OctreeParams :85-89, MyTrainParams
+    :216-240; src/modules/ToneMapper.h:36-47): regularisers, pose and
+    intrinsics refinement and the photometric calibration are on."""
+    from neat_b200 import config
+    for text in ("", "[TrainParams]\n[Netparams]\n[OctreeParams]\n"):
+        st = config.load_settings(text=text)
+        kw = config.trainer_kwargs(st)
+        assert kw["num_features"] == 4 and kw["grid_size"] == 17 and kw["softplus_beta"] == 2.0
+        assert kw["lr_decoder"] == pytest.approx(5e-5) and kw["lr_grid"] == pytest.approx(0.04)
+        assert kw["max_samples_per_node"] == 32
+        assert kw["loss_tv"] == pytest.approx(1e-4) and kw["loss_edge"] == pytest.approx(1e-3)
+        assert kw["optimize_pose"] is True and kw["optimize_intrinsics"] is True
+        assert kw["lr_pose"] == pytest.approx(1e-3) and kw["lr_intrinsics"] == 100.0
+        assert kw["tonemap"] == config.TONEMAP_DEFAULTS
+        assert kw["tonemap"]["response_enable"] and kw["tonemap"]["exposure_enable"]
+        assert kw["tonemap"]["sensor_bias_enable"] and kw["tonemap"]["sensor_bias_size_w"] == 32
+        run = config.run_settings(st)
+        assert run["tree_depth"] == 4 and run["start_layer"] == 3
+    # all three calibration parts disabled: no tone mapper
+    st = config.load_settings(text="[PhotometricCalibrationParams]\nresponse_enable = false\n"
+                                   "exposure_enable = false\nsensor_bias_enable = false\n")
+    assert "tonemap" not in config.trainer_kwargs(st)
 
 
 @pytest.mark.parametrize("section,key,value", [("Netparams", "decoder_hidden_layers", "2"),

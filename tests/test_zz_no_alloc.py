@@ -8,7 +8,8 @@ sampler's per-ray scratch in one static device array (at most
 NEAT_NOALLOC_MAX_RAYS rays).  These tests call it through the C ABI and check
 its SampleList against the workspace entry point, bit for bit, on two calls in
 a row whose second batch is smaller than the first (a stale first call would
-show), and that an oversize batch is refused before any launch.
+show), and that an oversize batch is refused before any kernel launch, with
+its count zeroed.
 
 Collected last (file name) so a failure here cannot hide the other tests.
 """
@@ -70,7 +71,10 @@ def test_noalloc_matches_workspace_entry_point_two_calls(neat, oracle):
 def test_noalloc_rejects_batches_beyond_its_array(neat):
     from neat_b200 import _lib
     R = _lib.NEAT_NOALLOC_MAX_RAYS + 1
-    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    cnt = torch.full((2,), -1, dtype=torch.int64, device="cuda")
     rc = neat.neat_create_samples_noalloc(None, 0, 2, None, None, R, 16, 0, 0, 1, 0, None, None, None, None, None,
                                           None, cnt.data_ptr(), None, None)
+    torch.cuda.synchronize()
     assert rc == _lib.NEAT_ERR_CAPACITY
+    # the count is zeroed before the refusal, so a caller that skips rc reads 0
+    assert cnt.tolist() == [0, 0]

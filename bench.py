@@ -33,16 +33,8 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOADS = {
-    "full": dict(desc="plain FP32 full size: 64 ellipsoids + 200 voids, 360 x 512^2 projections, Poisson I0=1e4, "
-                      "adaptive octree depth 4 (~1500 active), C=8, G=17, decoder 8-64-64-1, M=32, 2^18 rays/batch",
-                 n_ell=64, n_void=200, n_angles=360, w=512, h=512, photons=1e4, depth=4, active=1500, C=8, G=17,
-                 M=32, R=1 << 18, seed=2, cpu_rays=1 << 14),
-    "small": dict(desc="plain FP32 small: 8 ellipsoids, 32 x 128^2 projections, octree depth 2 (64 leaves), C=4, "
-                       "G=11, decoder 4-64-64-1, M=16, 4096 rays/batch",
-                  n_ell=8, n_void=0, n_angles=32, w=128, h=128, photons=None, depth=2, active=None, C=4, G=11, M=16,
-                  R=4096, seed=1, cpu_rays=4096),
-}
+from neat_b200.workloads import WORKLOADS, build_workload, phantom  # noqa: E402
+
 METRIC = "train rays/s (fwd+bwd)"
 DECODER_DESC = {"simt": "FP32 FFMA (CUDA cores)",
                 "bf16x3": "tcgen05, FP32-accurate: operands split in 3 BF16 pieces, 6 products, FP32 accumulation",
@@ -63,6 +55,21 @@ KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_bwd_rec<C=%d> (BF16x3 backward from the forward's records, MMA warp)",
                "bf16": "k_step_tiles_tc<C=%d, BF16, backward>"}
 PSNR_TARGET_DB = 40.0
+
+
+PROPOSAL_ITERS = 50  # proposal Adam iterations on a TRAIN step (FusedTrainer default)
+
+
+def step_launches(decoder, C, proposal, train):
+    """Kernels one neat_train_step launches: STEP_LAUNCHES, plus the records
+    backward of the three-piece path at C = 4, 8 (the plain backward kernel
+    then returns at once); with the learned proposal a SAMPLE step adds the CDF
+    kernel and a TRAIN step the histogram zeroing, the node descriptors and 3
+    kernels per proposal iteration."""
+    n = STEP_LAUNCHES + (1 if decoder == "bf16x3" and C in (4, 8) else 0)
+    if proposal:
+        n += (2 + 3 * PROPOSAL_ITERS) if train else 1
+    return n
 
 
 def hidden_flops(C, H=64):
@@ -154,22 +161,9 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # workload
 # --------------------------------------------------------------------------
-def build_workload(cfg, device):
-    from neat_b200 import scene as SC
-    from neat_b200.api import CameraModel
-    from neat_b200.tree import HyperTreeBase
-    objs = SC.ellipsoid_phantom(cfg["n_ell"], cfg["n_void"], seed=cfg["seed"])
-    scene = SC.SyntheticScene(objs, cfg["n_angles"], cfg["w"], cfg["h"], device=device, photons=cfg["photons"],
-                              noise_seed=cfg["seed"])
-    tree = HyperTreeBase(3, cfg["depth"])
-    if cfg["active"]:
-        tree.RefineByVariance(scene.density, cfg["active"], samples_per_axis=4)
-    else:
-        tree.SetActive(cfg["depth"])
-    return scene, tree, CameraModel.from_scene(scene)
-
-
 def cpu_tree(cfg, objs):
+    """The configuration's octree refined with the oracle's density (the CPU
+    leg has no device projector)."""
     from oracle import oracle as O
     from neat_b200.tree import HyperTreeBase
     tree = HyperTreeBase(3, cfg["depth"])
@@ -190,8 +184,7 @@ def cpu_reference_rays_per_s(cfg, steps, warmup, budget_s=None, min_s=None):
     once budget_s is spent, more (up to 4x) until min_s is reached.
     Returns (rays/s, info)."""
     from oracle import cpu_reference as CR
-    from neat_b200 import scene as SC
-    objs = SC.ellipsoid_phantom(cfg["n_ell"], cfg["n_void"], seed=cfg["seed"])
+    objs = phantom(cfg)
     tree = cpu_tree(cfg, objs)
     runner = CR.CpuReferenceStep(objs, tree, cfg)
     R = cfg["cpu_rays"]
@@ -269,55 +262,101 @@ def time_to_psnr(dev, decoders, target_db=PSNR_TARGET_DB, max_steps=3000, every=
 # --------------------------------------------------------------------------
 # variants of the step at the full-size workload
 # --------------------------------------------------------------------------
-def step_variants(cfg, scene, tree, cam, dev, steps=50):
+PATH_NAMES = ("simt", "bf16x3", "bf16")
+
+
+def decoder_path(name):
+    from neat_b200 import _lib
+    return {"simt": _lib.NEAT_DECODER_SIMT_FP32, "bf16x3": _lib.NEAT_DECODER_TC_BF16X3,
+            "bf16": _lib.NEAT_DECODER_TC_BF16}[name]
+
+
+def make_trainer(cfg, tree, cam, dev, decoder, proposal, seed):
+    """FusedTrainer of a workload: decoder path by name; with the learned
+    proposal the BF16 grid copy, the workload's sample budget and a 50-step
+    proposal cycle (one uniform TRAIN step, then SAMPLE steps)."""
+    from neat_b200.trainer import FusedTrainer
+    kw = dict(decoder_path=decoder_path(decoder), device=dev)
+    if proposal:
+        kw.update(proposal=True, proposal_budget=cfg.get("proposal_budget", 12), proposal_every=50,
+                  grid_bf16=decoder == "bf16")
+    elif decoder == "bf16":
+        kw.update(grid_bf16=True)
+    tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=seed, **kw)
+    tr.reserve(cfg["R"])
+    return tr
+
+
+def time_steps(tr, batches, phase_events=True):
+    """CUDA-event time of tr.step over the batches (one stream), the mean
+    per-phase times and the total samples of the steps (copied to pinned host
+    memory after each step, no synchronisation inside)."""
+    from neat_b200 import _lib
+    K = len(batches)
+    ev = None
+    if phase_events:
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(_lib.NEAT_STEP_PHASES)] for _ in range(K)]
+        for row in ev:  # torch creates the CUDA event on first record; the step records it again
+            for e in row:
+                e.record()
+    counts = torch.zeros((K, 4), dtype=torch.int64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for i, b in enumerate(batches):
+        tr.step(*b, phase_events=ev[i] if ev else None)
+        counts[i].copy_(tr.counters, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    tr.check_status()
+    ms = t0.elapsed_time(t1)
+    phase_ms = None
+    if ev:
+        phase_ms = {p: sum(ev[i][j].elapsed_time(ev[i][j + 1]) for i in range(K)) / K for j, p in enumerate(PHASES)}
+    return ms, phase_ms, counts
+
+
+def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
     """rays/s of the plain FP32 SIMT step, the BF16 step (BF16 grid copy and
     decoder operands, FP32 accumulation) and the BF16 step with the learned
     proposal (12 samples per segment; one full 50-step cycle, its uniform
-    TRAIN step included), CUDA events around each timed loop."""
-    from neat_b200 import _lib
-    from neat_b200.trainer import FusedTrainer
+    TRAIN step included), CUDA events around each timed loop; the BF16 +
+    proposal step against both FP32 steps (ref_rays_per_s: the FP32-accurate
+    tensor-core step of the main line)."""
     R = cfg["R"]
     gen = torch.Generator(device=dev)
     gen.manual_seed(4242)
     batches = [scene.sample_batch(R, gen) for _ in range(steps)]
     out = {}
-    for name, path, prop in (("fp32_simt", _lib.NEAT_DECODER_SIMT_FP32, False),
-                             ("bf16", _lib.NEAT_DECODER_TC_BF16, False),
-                             ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
-        tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
-                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50,
-                          grid_bf16=path == _lib.NEAT_DECODER_TC_BF16)
-        tr.reserve(R)
+    for name, dec, prop in (("fp32_simt", "simt", False), ("bf16", "bf16", False), ("bf16_proposal12", "bf16", True)):
+        tr = make_trainer(cfg, tree, cam, dev, dec, prop, cfg["seed"])
         k = steps if prop else 10
         for i in range(3 if not prop else 0):
             tr.step(*batches[i])
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for i in range(k):
-            tr.step(*batches[i])
-        e1.record()
-        torch.cuda.synchronize()
-        tr.check_status()
-        ms = e0.elapsed_time(e1)
+        ms, phase_ms, counts = time_steps(tr, batches[:k])
         out[name] = {"rays_per_s": R * k / (ms / 1000.0), "ms_per_step": ms / k, "steps": k,
-                     "samples_last_step": int(tr.counters[1].item())}
+                     "samples_per_step": float(counts[:, 1].double().mean()), "phase_ms": phase_ms}
         del tr
         torch.cuda.empty_cache()
     out["bf16_proposal12_vs_fp32_simt"] = out["bf16_proposal12"]["rays_per_s"] / out["fp32_simt"]["rays_per_s"]
+    out["bf16_proposal12_vs_fp32_accurate_tcgen05"] = out["bf16_proposal12"]["rays_per_s"] / ref_rays_per_s
+    out["note"] = ("ratios of rays/s on the same workload: against the FP32 SIMT step (FP32 FFMA on CUDA cores) and "
+                   "against the FP32-accurate tcgen05 step of the main line (3-piece BF16 operands)")
     return out
 
 
-def volume_psnr_race(cfg, scene, tree, cam, dev, steps, n_eval=20, vol_n=256):
-    """Plain method (FP32-accurate decoder, uniform 32 samples) for `steps`
-    steps, then BF16 + learned proposal (12 samples) until it reaches the plain
-    method's final volume PSNR within 0.1 dB.  Volume PSNR = 10 log10(peak^2 /
-    MSE) over the vol_n^3 voxel-corner lattice against the phantom density,
-    peak = the phantom's maximum, MSE in f64.  Wall clock = CUDA-event time of
-    the training steps (evaluations excluded)."""
-    from neat_b200 import _lib
-    from neat_b200.trainer import FusedTrainer
+def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
+    """Time to the plain method's volume PSNR.  The plain method (FP32-accurate
+    decoder, uniform 32 samples) trains `steps` steps; its final volume PSNR is
+    the target.  Then BF16 + learned proposal (12 samples per segment) trains
+    until it reaches the target within 0.1 dB (at most `steps` steps).  Both
+    runs see the same batches from the same initial state and are evaluated
+    every `every` steps; each run's time to the target - 0.1 dB is the
+    CUDA-event time of its training steps up to the first evaluation at or
+    above it (evaluations excluded).  Volume PSNR = 10 log10(peak^2 / MSE) over
+    the vol_n^3 voxel-corner lattice (UniformSampledVolume) against the f64
+    phantom density, peak = the phantom's maximum, MSE in f64."""
     gt = scene.density_volume(vol_n)
     peak2 = float(gt.max()) ** 2
     R = cfg["R"]
@@ -329,43 +368,70 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, n_eval=20, vol_n=256):
 
     res = {}
     target = None
-    for name, path, prop in (("plain_fp32", _lib.NEAT_DECODER_TC_BF16X3, False),
-                             ("bf16_proposal12", _lib.NEAT_DECODER_TC_BF16, True)):
-        tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"],
-                          decoder_path=path, device=dev, proposal=prop, proposal_budget=12, proposal_every=50,
-                          grid_bf16=prop)
-        tr.reserve(R)
+    for name, dec, prop in (("plain_fp32", "bf16x3", False), ("bf16_proposal12", "bf16", True)):
+        tr = make_trainer(cfg, tree, cam, dev, dec, prop, cfg["seed"])
         gen = torch.Generator(device=dev)
         gen.manual_seed(777)
-        every = max(1, steps // n_eval)
-        ms, curve, k, reached_ms = 0.0, [], 0, None
+        ms, curve, k = 0.0, [], 0
         while k < steps:
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            bs = [scene.sample_batch(R, gen) for _ in range(every)]
-            e0.record()
-            for b in bs:
-                tr.step(*b)
-            e1.record()
-            torch.cuda.synchronize()
-            k += every
-            ms += e0.elapsed_time(e1)
+            n = min(every, steps - k)
+            bs = [scene.sample_batch(R, gen) for _ in range(n)]
+            t, _, _ = time_steps(tr, bs, phase_events=False)
+            k += n
+            ms += t
             p = vpsnr(tr)
             curve.append([k, round(ms, 1), round(p, 3)])
-            if target is not None and reached_ms is None and p >= target - 0.1:
-                reached_ms = ms
+            if target is not None and p >= target - 0.1:
                 break
-        tr.check_status()
-        res[name] = {"steps": k, "train_ms": ms, "volume_psnr_db": curve[-1][2], "curve": curve}
+        res[name] = {"steps": k, "train_ms": ms, "ms_per_step": ms / k, "volume_psnr_db": curve[-1][2],
+                     "curve": curve}
         if target is None:
             target = curve[-1][2]
-        else:
-            res[name]["reached_plain_minus_0.1dB_at_ms"] = reached_ms
         del tr
         torch.cuda.empty_cache()
-    res["definition"] = ("volume PSNR = 10 log10(peak^2 / MSE), %d^3 voxel-corner lattice vs the phantom density, "
-                         "f64" % vol_n)
+    for name in ("plain_fp32", "bf16_proposal12"):
+        hit = [c for c in res[name]["curve"] if c[2] >= target - 0.1]
+        res[name]["ms_to_target"] = hit[0][1] if hit else None
+        res[name]["steps_to_target"] = hit[0][0] if hit else None
+    a, b = res["plain_fp32"]["ms_to_target"], res["bf16_proposal12"]["ms_to_target"]
+    res["target_db"] = target - 0.1
+    res["plain_final_db"] = target
+    res["speedup_to_target"] = (a / b) if (a and b) else None
+    res["definition"] = ("target = plain method's final volume PSNR - 0.1 dB; volume PSNR = 10 log10(peak^2 / MSE), "
+                         "%d^3 voxel-corner lattice vs the phantom density, f64; time = CUDA events around the "
+                         "training steps" % vol_n)
     return res
+
+
+def large_workload(dev, steps=50, warmup=3):
+    """The large porous configuration, BF16 + learned proposal: rays/s over one
+    full 50-step proposal cycle (its uniform 32-sample TRAIN step included),
+    device-resident batches, CUDA events; per-phase times and samples per
+    step."""
+    cfg = dict(WORKLOADS["large"])
+    scene, tree, cam = build_workload(cfg, dev)
+    tr = make_trainer(cfg, tree, cam, dev, "bf16", True, cfg["seed"])
+    R = cfg["R"]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(99)
+    batches = [scene.sample_batch(R, gen) for _ in range(warmup + steps)]
+    for i in range(warmup):  # the warm-up includes the first TRAIN step; the timed cycle has its own
+        tr.step(*batches[i])
+    while (tr.step_id % 50) != 0:  # start the timed region at a cycle boundary
+        tr.step(*batches[0])
+    ms, phase_ms, counts = time_steps(tr, batches[warmup:])
+    S = counts[:, 1].double()
+    out = {"workload": cfg["desc"], "rays_per_s": R * steps / (ms / 1000.0), "ms_per_step": ms / steps,
+           "steps": steps, "timed": "one 50-step proposal cycle: 1 uniform TRAIN step (32 samples per segment) + "
+                                    "49 SAMPLE steps (12 per segment)",
+           "samples_per_step_mean": float(S.mean()), "samples_train_step": float(S.max()),
+           "samples_sample_step": float(S.min()), "active_nodes": tree.NumActiveNodes(),
+           "node_depths": {int(k): int(v) for k, v in zip(*np.unique(tree.node_depth[tree.active_node_ids],
+                                                                    return_counts=True))},
+           "grid_params": int(tr.grid.numel()), "phase_ms": phase_ms}
+    del tr
+    torch.cuda.empty_cache()
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -379,19 +445,25 @@ def main():
     ap.add_argument("--impl", default="neat", choices=["neat", "reference"])
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-psnr", action="store_true", help="skip the time-to-PSNR leg")
+    ap.add_argument("--no-psnr", action="store_true", help="skip the small workload's time-to-PSNR leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / BF16 / BF16+proposal step variants")
-    ap.add_argument("--volume-psnr", type=int, default=0,
-                    help="also race plain vs BF16+proposal to the plain method's volume PSNR over this many steps")
+    ap.add_argument("--no-large", action="store_true", help="skip the large porous workload's sub-line")
+    ap.add_argument("--volume-psnr", type=int, default=5000,
+                    help="race plain vs BF16+proposal to the plain method's volume PSNR over this many steps "
+                         "(full workload; 0 skips)")
     ap.add_argument("--rays", type=int, default=0, help="override rays per batch (profiling runs only)")
-    ap.add_argument("--decoder", default="bf16x3", choices=["simt", "bf16x3", "bf16"],
-                    help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16")
+    ap.add_argument("--decoder", default=None, choices=list(PATH_NAMES),
+                    help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16 "
+                         "(default: bf16x3; bf16 for the large workload)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     cfg = dict(WORKLOADS[args.workload])
     if args.rays:
         cfg["R"] = args.rays
+    large = args.workload == "large"
+    decoder = args.decoder or ("bf16" if large else "bf16x3")
+    proposal = large
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -425,15 +497,11 @@ def main():
 
     from neat_b200 import _lib
     from neat_b200.csrc import build
-    from neat_b200.trainer import FusedTrainer
     build.build()
     scene, tree, cam = build_workload(cfg, dev)
+    n_active = tree.NumActiveNodes()
     R, K, W = cfg["R"], args.steps, args.warmup
-    path = {"simt": _lib.NEAT_DECODER_SIMT_FP32, "bf16x3": _lib.NEAT_DECODER_TC_BF16X3,
-            "bf16": _lib.NEAT_DECODER_TC_BF16}[args.decoder]
-    tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=cfg["seed"] + rank,
-                      decoder_path=path, device=dev)
-    tr.reserve(R)
+    tr = make_trainer(cfg, tree, cam, dev, decoder, proposal, cfg["seed"] + rank)
     gen = torch.Generator(device=dev)
     gen.manual_seed(1000 + rank)
     batches = [scene.sample_batch(R, gen) for _ in range(W + K)]
@@ -449,39 +517,25 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- warm-up (device-resident batches)
+    # ---- warm-up (device-resident batches; with the proposal it includes the first TRAIN step)
     for i in range(W):
         tr.step(*batches[i])
     torch.cuda.synchronize()
     tr.check_status()
 
     # ---- timed: device-resident inputs (value)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(_lib.NEAT_STEP_PHASES)] for _ in range(K)]
-    for row in ev:  # torch creates the CUDA event on first record; the step records it again
-        for e in row:
-            e.record()
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record()
-    for i in range(K):
-        tr.step(*batches[W + i], phase_events=ev[i])
-    t_end.record()
-    torch.cuda.synchronize()
+    ms, phase_ms, counts = time_steps(tr, batches[W:])
     clock_info = clocks.stop()
     barrier()
-    ms = max_over_ranks(t_start.elapsed_time(t_end))
-    tr.check_status()
-    counters = tr.counters.cpu().tolist()
-    phase_ms = {p: 0.0 for p in PHASES}
-    for i in range(K):
-        for j, p in enumerate(PHASES):
-            phase_ms[p] += ev[i][j].elapsed_time(ev[i][j + 1])
-    phase_ms = {p: v / K for p, v in phase_ms.items()}
+    ms = max_over_ranks(ms)
     value = R * K * world / (ms / 1000.0)
+    S_steps = counts[:, 1].double()
+    S = float(S_steps.mean())
+    counters = counts[-1].tolist()
 
     # ---- timed: end to end through the public API with host buffers (e2e)
     hb = []
@@ -511,9 +565,11 @@ def main():
     tr.check_status()
     e2e = R * K * world / (e2e_ms / 1000.0)
     h2d = R * (8 + 4 + 4)
+    grid_numel = tr.grid.numel()
+    del tr
+    torch.cuda.empty_cache()
 
     # ---- roofline of the dominant kernel (backward tiles)
-    S = counters[1]
     H = 64
     flops_bwd = 4.0 * hidden_flops(cfg["C"], H) * S  # dX + dW products of the decoder backward
     t_bwd = phase_ms["backward_tiles"] / 1000.0
@@ -527,11 +583,16 @@ def main():
     if not args.no_psnr:
         ttp = time_to_psnr(dev, ["simt", "bf16x3", "bf16"])
     variants = None
-    if not args.no_variants:
-        variants = step_variants(cfg, scene, tree, cam, dev)
+    if not args.no_variants and not large:
+        variants = step_variants(cfg, scene, tree, cam, dev, value / world)
     vrace = None
-    if args.volume_psnr:
+    if args.volume_psnr and not large:
         vrace = volume_psnr_race(cfg, scene, tree, cam, dev, args.volume_psnr)
+    large_line = None
+    if not args.no_large and not large:
+        del scene, tree, cam, batches
+        torch.cuda.empty_cache()
+        large_line = large_workload(dev)
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cv, ci = cpu_reference_rays_per_s(cfg, 5, 1, budget_s=30.0, min_s=12.0)
@@ -542,34 +603,40 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    launches = sum(step_launches(decoder, cfg["C"], proposal, proposal and (i - 1) % 50 == 0)
+                   for i in range(W + 1, W + K + 1))
+    traffic_key = (args.workload, decoder)
     line = {
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16" if args.decoder == "bf16" else "f32",
+        "dtype": "bf16" if decoder == "bf16" else "f32",
         "data": "synthetic",
-        "config": {"workload": cfg["desc"], "decoder": DECODER_DESC[args.decoder], "rays_per_step": R, "samples_per_step": S, "segments_per_step":
-                   counters[0], "active_nodes": tree.NumActiveNodes(), "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2: grid + Adam state %.2f GB per replica" % (
-                       4 * 4 * tr.grid.numel() / 1e9)},
+        "config": {"workload": cfg["desc"], "decoder": DECODER_DESC[decoder],
+                   "proposal": ("learned, %d samples per segment, 50-step cycle; %d of the timed steps are "
+                                "uniform TRAIN steps" % (cfg.get("proposal_budget", 12),
+                                                         sum((i - 1) % 50 == 0 for i in range(W + 1, W + K + 1))))
+                   if proposal else None,
+                   "rays_per_step": R, "samples_per_step": S, "segments_per_step": counters[0],
+                   "active_nodes": n_active, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2: grid + Adam state %.2f GB per replica" % (4 * 4 * grid_numel / 1e9)},
         "phase_ms": phase_ms,
-        "roofline": {"kernel": KERNEL_NAME[args.decoder] % cfg["C"], "bound": "tensor", "achieved": achieved,
+        "roofline": {"kernel": KERNEL_NAME[decoder] % cfg["C"], "bound": "tensor", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": (TRAFFIC_BYTES_PER_SAMPLE[(args.workload, args.decoder)] * S
-                                 if (args.workload, args.decoder) in TRAFFIC_BYTES_PER_SAMPLE else None),
+                     "traffic": (TRAFFIC_BYTES_PER_SAMPLE[traffic_key] * S
+                                 if traffic_key in TRAFFIC_BYTES_PER_SAMPLE else None),
                      "traffic_source": "ncu capture at 2^16 rays scaled by samples (upper bound)",
                      "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                      "fp32_simt_peak_tflops": simt_peak,
                      "frac_of_fp32_simt": achieved / simt_peak},
-        "step_roofline": step_roofline(S, R, tr.grid.numel(), cfg["C"], ms / K, peaks, simt_peak),
+        "step_roofline": step_roofline(S, R, grid_numel, cfg["C"], ms / K, peaks, simt_peak),
         "e2e": {"value": e2e, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
-        # the three-piece backward from records adds one launch (the plain
-        # backward kernel then returns at once)
-        "gpu_launches": (STEP_LAUNCHES + (1 if args.decoder == "bf16x3" and cfg["C"] in (4, 8) else 0)) * K,
+        "gpu_launches": launches,
         "clocks": clock_info,
         "cpu_baseline": cpu_base,
         "time_to_psnr": ttp,
         "variants": variants,
         "volume_psnr_race": vrace,
+        "large_workload": large_line,
     }
     print(json.dumps(line))
 

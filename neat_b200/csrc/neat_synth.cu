@@ -1,9 +1,18 @@
 // neat_synth.cu -- synthetic cone-beam scans: analytic line integrals through
-// a phantom of ellipsoids (additive) and voids (density forced to 0), in
-// f64.  This stands in for the reference's measured projections (KAUST
-// Pepper, loaded by SceneBase::LoadImagesCT); it is data generation, not part
-// of the training step.  Compiled with --fmad=false so every f64 operation is
-// rounded as written.
+// a phantom of additive ellipsoids and cylinders and of override ellipsoids
+// (inside them the density is the object's own: 0 for a void, a sphere's
+// density for the inclusions of a porous volume), in f64.  This stands in for
+// the reference's measured projections (KAUST Pepper, loaded by
+// SceneBase::LoadImagesCT); it is data generation, not part of the training
+// step.  Compiled with --fmad=false so every f64 operation is rounded as
+// written.
+//
+// Object record (17 doubles): centre(3), semi-axes(3), rotation R(9, row-major,
+// local = R^T (p - c)), density, kind.  kind 0: additive ellipsoid; kind 1:
+// override ellipsoid; kind 2: additive cylinder along the local z axis (radii
+// semi-axes x, y; half-height semi-axis z).  Override objects with a non-zero
+// density must not overlap one another (a point inside two would take the
+// first one's density, a line through both would count both).
 #include "neat_common.cuh"
 
 namespace neat
@@ -11,10 +20,11 @@ namespace neat
 
 constexpr int OBJ = 17;
 constexpr int MAX_VOID_HITS = 64;
+constexpr double kFar = 1e300;  // unbounded extent of a chord along a cylinder's axis
 
-__device__ bool ellipsoid_chord(const double* ob, const double o[3], const double d[3], double& t0, double& t1)
+// Ray o + t d in the object's scaled local frame: q = (R^T (o - c)) / axes, e = (R^T d) / axes.
+__device__ void object_local(const double* ob, const double o[3], const double d[3], double q[3], double e[3])
 {
-    double q[3], e[3];
     const double p[3] = {o[0] - ob[0], o[1] - ob[1], o[2] - ob[2]};
     const double* R   = ob + 6;
     for (int i = 0; i < 3; ++i)
@@ -24,6 +34,12 @@ __device__ bool ellipsoid_chord(const double* ob, const double o[3], const doubl
         q[i]            = lq / ob[3 + i];
         e[i]            = le / ob[3 + i];
     }
+}
+
+__device__ bool ellipsoid_chord(const double* ob, const double o[3], const double d[3], double& t0, double& t1)
+{
+    double q[3], e[3];
+    object_local(ob, o, d, q, e);
     const double A    = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
     const double B    = q[0] * e[0] + q[1] * e[1] + q[2] * e[2];
     const double Cc   = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] - 1.0;
@@ -35,11 +51,57 @@ __device__ bool ellipsoid_chord(const double* ob, const double o[3], const doubl
     return true;
 }
 
+// Chord of the cylinder x^2 + y^2 <= 1, |z| <= 1 (scaled local frame): the
+// ray's interval inside the infinite cylinder intersected with the slab.
+__device__ bool cylinder_chord(const double* ob, const double o[3], const double d[3], double& t0, double& t1)
+{
+    double q[3], e[3];
+    object_local(ob, o, d, q, e);
+    double a0 = -kFar, a1 = kFar;
+    const double A  = e[0] * e[0] + e[1] * e[1];
+    const double B  = q[0] * e[0] + q[1] * e[1];
+    const double Cc = q[0] * q[0] + q[1] * q[1] - 1.0;
+    if (A > 0)
+    {
+        const double disc = B * B - A * Cc;
+        if (disc <= 0) return false;
+        const double sq = sqrt(disc);
+        a0              = (-B - sq) / A;
+        a1              = (-B + sq) / A;
+    }
+    else if (Cc > 0)
+        return false;  // parallel to the axis, outside
+    double z0 = -kFar, z1 = kFar;
+    if (e[2] != 0)
+    {
+        z0 = (-1.0 - q[2]) / e[2];
+        z1 = (1.0 - q[2]) / e[2];
+        if (z0 > z1)
+        {
+            const double t = z0;
+            z0             = z1;
+            z1             = t;
+        }
+    }
+    else if (q[2] < -1.0 || q[2] > 1.0)
+        return false;  // in a plane of constant z outside the slab
+    t0 = a0 > z0 ? a0 : z0;
+    t1 = a1 < z1 ? a1 : z1;
+    return t1 > t0;
+}
+
+__device__ bool object_chord(const double* ob, const double o[3], const double d[3], double& t0, double& t1)
+{
+    return ob[16] == 2.0 ? cylinder_chord(ob, o, d, t0, t1) : ellipsoid_chord(ob, o, d, t0, t1);
+}
+
 __device__ double phantom_line(const double* __restrict__ obj, int n_obj, const double o[3], const double d[3],
                                int* status)
 {
+    // override intervals (kind 1), merged; each adds its own density x chord
     double vs[MAX_VOID_HITS], ve[MAX_VOID_HITS];
-    int nv = 0;
+    int nv       = 0;
+    double total = 0;
     for (int k = 0; k < n_obj; ++k)
     {
         const double* ob = obj + OBJ * k;
@@ -51,6 +113,7 @@ __device__ double phantom_line(const double* __restrict__ obj, int n_obj, const 
             raise_status(status, NEAT_ERR_CAPACITY);
             continue;
         }
+        if (ob[15] != 0.0) total += ob[15] * (t1 - t0);
         // insertion by start
         int p = nv++;
         while (p > 0 && vs[p - 1] > t0)
@@ -76,13 +139,13 @@ __device__ double phantom_line(const double* __restrict__ obj, int n_obj, const 
             ++m;
         }
     }
-    double total = 0;
+    // additive objects (kinds 0 and 2), outside the override intervals
     for (int k = 0; k < n_obj; ++k)
     {
         const double* ob = obj + OBJ * k;
-        if (ob[16] != 0.0) continue;
+        if (ob[16] != 0.0 && ob[16] != 2.0) continue;
         double t0, t1;
-        if (!ellipsoid_chord(ob, o, d, t0, t1)) continue;
+        if (!object_chord(ob, o, d, t0, t1)) continue;
         double len = t1 - t0;
         for (int v = 0; v < m; ++v)
         {
@@ -134,18 +197,19 @@ __global__ void k_synth_density(const double* __restrict__ obj, int n_obj, const
     {
         const double* ob = obj + OBJ * k;
         const double* R  = ob + 6;
-        double s         = 0;
+        double l[3];
         for (int a = 0; a < 3; ++a)
         {
-            double l = R[0 * 3 + a] * (p[0] - ob[0]) + R[1 * 3 + a] * (p[1] - ob[1]) + R[2 * 3 + a] * (p[2] - ob[2]);
-            l        = l / ob[3 + a];
-            s += l * l;
+            l[a] = R[0 * 3 + a] * (p[0] - ob[0]) + R[1 * 3 + a] * (p[1] - ob[1]) + R[2 * 3 + a] * (p[2] - ob[2]);
+            l[a] = l[a] / ob[3 + a];
         }
-        if (s <= 1.0)
+        const bool inside = ob[16] == 2.0 ? (l[0] * l[0] + l[1] * l[1] <= 1.0 && l[2] * l[2] <= 1.0)
+                                          : ((l[0] * l[0] + l[1] * l[1]) + l[2] * l[2] <= 1.0);
+        if (inside)
         {
             if (ob[16] == 1.0)
             {
-                rho = 0;
+                rho = ob[15];  // override: the first override object containing p
                 break;
             }
             rho += ob[15];

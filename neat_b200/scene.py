@@ -5,6 +5,9 @@ samples/nikon2neat.cpp).  Here a seeded phantom of ellipsoids (and void
 spheres) is projected analytically in f64 with the same camera model the
 training step uses:
 
+* kinds of objects: additive ellipsoids (0), override ellipsoids whose inside
+  takes the object's density (1; a void has density 0) and additive cylinders
+  along the local z axis (2);
 * geometry after nikon2neat.cpp:268-301: volume [-1,1]^3, source at distance
   3 from the centre, detector at 1.5 behind it (SrcToDetector 4.5), source
   direction (sin(-a), -cos(-a), 0), up (0,0,-1), R = [right, up, forward],
@@ -47,6 +50,37 @@ def _obj(center, axes, R, density, kind):
     o[15] = density
     o[16] = kind
     return o
+
+
+def porous_phantom(n_spheres=2000, seed=0, radius=(0.002, 0.02), density=(0.2, 1.0), cylinder_radius=0.7,
+                   cylinder_half_height=0.8, cylinder_density=0.3, max_tries=200000):
+    """Porous volume: an additive cylinder of density cylinder_density along z
+    (radius cylinder_radius, half-height cylinder_half_height, centred) holding
+    n_spheres override spheres (radius U[radius], density U[density]; inside a
+    sphere the density is the sphere's own).  Sphere centres are uniform in the
+    cylinder, rejected until the sphere lies wholly inside it and touches no
+    earlier sphere, so every point has one well-defined density."""
+    rng = np.random.default_rng(seed)
+    objs = [_obj([0.0, 0.0, 0.0], [cylinder_radius, cylinder_radius, cylinder_half_height], np.eye(3),
+                 cylinder_density, 2)]
+    centres = np.zeros((n_spheres, 3))
+    radii = np.zeros(n_spheres)
+    k = tries = 0
+    while k < n_spheres:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("porous_phantom: could not place the spheres apart")
+        r = rng.uniform(*radius)
+        c = np.array([rng.uniform(-1, 1) * cylinder_radius, rng.uniform(-1, 1) * cylinder_radius,
+                      rng.uniform(-1, 1) * cylinder_half_height])
+        if math.hypot(c[0], c[1]) > cylinder_radius - r or abs(c[2]) > cylinder_half_height - r:
+            continue
+        if k and np.any(np.linalg.norm(centres[:k] - c, axis=1) < radii[:k] + r):
+            continue
+        centres[k], radii[k] = c, r
+        objs.append(_obj(c, [r, r, r], np.eye(3), rng.uniform(*density), 1))
+        k += 1
+    return np.stack(objs)
 
 
 def ellipsoid_phantom(n_ellipsoids=8, n_voids=0, seed=0):
@@ -128,6 +162,15 @@ def cone_beam_geometry(n_angles, w, h, src_dist=3.0, det_dist=1.5):
 # --------------------------------------------------------------------------
 # scene
 # --------------------------------------------------------------------------
+def pixel_to_uv(px, size):
+    """PixelToUV with align_corners (src/modules/CameraPose.h:38-54): px / (size - 1)
+    in float32, correctly rounded as the reference's CPU tensors divide.  The
+    divisor is a tensor: torch divides a CUDA tensor by a Python scalar through
+    its reciprocal, which is off by one ulp for some pixels."""
+    xf = px.to(torch.float32)
+    return xf / torch.full_like(xf, float(size - 1))
+
+
 class SyntheticScene:
     """Projections [n_img, h, w] f32 on the device plus the camera model."""
 
@@ -201,7 +244,7 @@ class SyntheticScene:
             img = ids[torch.randint(0, ids.numel(), (num_rays,), generator=g, device=g.device)]
         x = torch.randint(0, self.w, (num_rays,), generator=g, device=g.device)
         y = torch.randint(0, self.h, (num_rays,), generator=g, device=g.device)
-        uv = torch.stack([x.float() / (self.w - 1), y.float() / (self.h - 1)], 1)
+        uv = torch.stack([pixel_to_uv(x, self.w), pixel_to_uv(y, self.h)], 1)
         proj = self.projection if self.projection.device == img.device else self.projection.to(img.device)
         target = proj[img, y, x]
         return uv.to(dev).contiguous(), img.to(torch.int32).to(dev).contiguous(), target.to(dev).contiguous()

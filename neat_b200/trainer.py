@@ -16,6 +16,7 @@ import torch
 from . import _lib
 from .api import CameraModel, decoder_init, grid_init
 from .proposal import proposal_init
+from .scene import pixel_to_uv
 from .tree import HyperTreeBase
 
 
@@ -312,13 +313,13 @@ class FusedTrainer:
         w, h = self.camera.w, self.camera.h
         if rows_per_batch is None:
             rows_per_batch = max(1, min(h, max(self.ws_rays, 1 << 16) // w))
-        xs = torch.arange(w, device=self.dev, dtype=torch.float32) / float(w - 1)
+        xs = pixel_to_uv(torch.arange(w, device=self.dev), w)
         out_imgs = torch.empty((len(image_ids), h, w), dtype=torch.float32, device=self.dev)
         sums = torch.zeros((len(image_ids), 2), dtype=torch.float64, device=self.dev)
         for k, img in enumerate(image_ids):
             for r0 in range(0, h, rows_per_batch):
                 r1 = min(h, r0 + rows_per_batch)
-                ys = torch.arange(r0, r1, device=self.dev, dtype=torch.float32) / float(h - 1)
+                ys = pixel_to_uv(torch.arange(r0, r1, device=self.dev), h)
                 uv = torch.stack([xs.repeat(r1 - r0), ys.repeat_interleave(w)], 1).contiguous()
                 ids = torch.full((uv.shape[0],), int(img), dtype=torch.int32, device=self.dev)
                 tgt = projections[int(img), r0:r1].reshape(-1).contiguous()

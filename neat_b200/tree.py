@@ -35,21 +35,20 @@ class HyperTreeBase:
         children = np.full((n, ns), -1, np.int32)
         pmin[0] = -1.0
         pmax[0] = 1.0
-        cur, layer_start, layer_count = 1, 0, 1
+        # one breadth-first layer at a time: child i of node n is 8 n + 1 + i and
+        # takes, on axis k, the upper half [centre, max] when bit k of i is set
+        bits = np.array([[(i >> k) & 1 for k in range(3)] for i in range(ns)], bool)  # [8, 3]
+        layer_start, layer_count = 0, 1
         for dep in range(1, max_depth + 1):
-            nxt = cur
             ids = np.arange(layer_start, layer_start + layer_count)
             center = (pmin[ids] + pmax[ids]) * np.float32(0.5)
-            for j, nid in enumerate(ids):
-                for i in range(ns):
-                    bits = np.array([(i >> k) & 1 for k in range(3)], bool)
-                    pmin[cur] = np.where(bits, center[j], pmin[nid])
-                    pmax[cur] = np.where(bits, pmax[nid], center[j])
-                    children[nid, i] = cur
-                    depth[cur] = dep
-                    parent[cur] = nid
-                    cur += 1
-            layer_start, layer_count = nxt, layer_count * ns
+            kids = (8 * ids[:, None] + 1 + np.arange(ns)[None, :])  # [L, 8]
+            pmin[kids] = np.where(bits[None], center[:, None, :], pmin[ids][:, None, :])
+            pmax[kids] = np.where(bits[None], pmax[ids][:, None, :], center[:, None, :])
+            children[ids] = kids
+            depth[kids] = dep
+            parent[kids] = ids[:, None]
+            layer_start, layer_count = layer_start + layer_count, layer_count * ns
         self.node_position_min = pmin
         self.node_position_max = pmax
         self.node_depth = depth

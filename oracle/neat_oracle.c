@@ -608,14 +608,17 @@ void oracle_igs_backward(const float* grid, long N, int C, int Z, int Y, int X, 
 /* ------------------------------------------------------------------------ */
 /* Synthetic phantom (stands in for the reference's measured scans).         */
 /* obj: [n_obj, 17] doubles = centre(3), semi-axes(3), rotation R(9,        */
-/* row-major, local = R^T (p - c)), density, kind (0 additive ellipsoid,     */
-/* 1 void: density forced to 0 inside).                                      */
+/* row-major, local = R^T (p - c)), density, kind: 0 additive ellipsoid,     */
+/* 1 override ellipsoid (inside, the density is the object's own: 0 for a    */
+/* void), 2 additive cylinder along the local z axis (radii = semi-axes x,   */
+/* y; half-height = semi-axis z).  Override objects with a non-zero density  */
+/* must not overlap one another.                                             */
 /* ------------------------------------------------------------------------ */
 #define OBJ_STRIDE 17
+#define FAR_T 1e300
 
-static int ellipsoid_chord(const double* ob, const double* o, const double* d, double* t0, double* t1)
+static void object_local(const double* ob, const double* o, const double* d, double* q, double* e)
 {
-    double q[3], e[3];
     double p[3] = {o[0] - ob[0], o[1] - ob[1], o[2] - ob[2]};
     const double* Rm = ob + 6;
     for (int i = 0; i < 3; ++i)
@@ -626,6 +629,12 @@ static int ellipsoid_chord(const double* ob, const double* o, const double* d, d
         q[i]      = lq / ob[3 + i];
         e[i]      = le / ob[3 + i];
     }
+}
+
+static int ellipsoid_chord(const double* ob, const double* o, const double* d, double* t0, double* t1)
+{
+    double q[3], e[3];
+    object_local(ob, o, d, q, e);
     double A = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
     double B = q[0] * e[0] + q[1] * e[1] + q[2] * e[2];
     double C = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] - 1.0;
@@ -637,17 +646,64 @@ static int ellipsoid_chord(const double* ob, const double* o, const double* d, d
     return 1;
 }
 
+/* The ray's interval inside x^2 + y^2 <= 1 (scaled local frame), intersected */
+/* with the slab |z| <= 1.                                                    */
+static int cylinder_chord(const double* ob, const double* o, const double* d, double* t0, double* t1)
+{
+    double q[3], e[3];
+    object_local(ob, o, d, q, e);
+    double a0 = -FAR_T, a1 = FAR_T;
+    double A = e[0] * e[0] + e[1] * e[1];
+    double B = q[0] * e[0] + q[1] * e[1];
+    double C = q[0] * q[0] + q[1] * q[1] - 1.0;
+    if (A > 0)
+    {
+        double disc = B * B - A * C;
+        if (disc <= 0) return 0;
+        double sq = sqrt(disc);
+        a0 = (-B - sq) / A;
+        a1 = (-B + sq) / A;
+    }
+    else if (C > 0)
+        return 0;
+    double z0 = -FAR_T, z1 = FAR_T;
+    if (e[2] != 0)
+    {
+        z0 = (-1.0 - q[2]) / e[2];
+        z1 = (1.0 - q[2]) / e[2];
+        if (z0 > z1)
+        {
+            double t = z0;
+            z0 = z1;
+            z1 = t;
+        }
+    }
+    else if (q[2] < -1.0 || q[2] > 1.0)
+        return 0;
+    *t0 = a0 > z0 ? a0 : z0;
+    *t1 = a1 < z1 ? a1 : z1;
+    return *t1 > *t0;
+}
+
+static int object_chord(const double* ob, const double* o, const double* d, double* t0, double* t1)
+{
+    return ob[16] == 2.0 ? cylinder_chord(ob, o, d, t0, t1) : ellipsoid_chord(ob, o, d, t0, t1);
+}
+
 static int dcmp(const void* a, const void* b)
 {
     double x = *(const double*)a, y = *(const double*)b;
     return (x < y) ? -1 : (x > y);
 }
 
-/* Line integral of the phantom density along o + t d (|d| = 1), t in R. */
+/* Line integral of the phantom density along o + t d (|d| = 1), t in R:     */
+/* each override object adds density x chord; additive objects add density  */
+/* x (chord minus the union of the override intervals).                      */
 double oracle_phantom_line(const double* obj, int n_obj, const double* o, const double* d)
 {
     double vi[2 * 512];
     int nv = 0;
+    double total = 0;
     for (int k = 0; k < n_obj; ++k)
     {
         const double* ob = obj + OBJ_STRIDE * k;
@@ -655,12 +711,13 @@ double oracle_phantom_line(const double* obj, int n_obj, const double* o, const 
         double t0, t1;
         if (ellipsoid_chord(ob, o, d, &t0, &t1) && nv < 512)
         {
+            if (ob[15] != 0.0) total += ob[15] * (t1 - t0);
             vi[2 * nv]     = t0;
             vi[2 * nv + 1] = t1;
             nv++;
         }
     }
-    /* merge void intervals (sorted by start) */
+    /* merge override intervals (sorted by start) */
     qsort(vi, nv, 2 * sizeof(double), dcmp);
     int m = 0;
     for (int k = 0; k < nv; ++k)
@@ -676,13 +733,12 @@ double oracle_phantom_line(const double* obj, int n_obj, const double* o, const 
             m++;
         }
     }
-    double total = 0;
     for (int k = 0; k < n_obj; ++k)
     {
         const double* ob = obj + OBJ_STRIDE * k;
-        if (ob[16] != 0.0) continue;
+        if (ob[16] != 0.0 && ob[16] != 2.0) continue;
         double t0, t1;
-        if (!ellipsoid_chord(ob, o, d, &t0, &t1)) continue;
+        if (!object_chord(ob, o, d, &t0, &t1)) continue;
         double len = t1 - t0;
         for (int v = 0; v < m; ++v)
         {
@@ -695,7 +751,8 @@ double oracle_phantom_line(const double* obj, int n_obj, const double* o, const 
     return total;
 }
 
-/* Density of the phantom at a point. */
+/* Density of the phantom at a point: the sum of the additive objects that   */
+/* contain it, or the density of the first override object that does.        */
 double oracle_phantom_density(const double* obj, int n_obj, const double* p)
 {
     double rho = 0;
@@ -703,16 +760,17 @@ double oracle_phantom_density(const double* obj, int n_obj, const double* p)
     {
         const double* ob = obj + OBJ_STRIDE * k;
         const double* Rm = ob + 6;
-        double s = 0;
+        double l[3];
         for (int i = 0; i < 3; ++i)
         {
-            double l = Rm[0 * 3 + i] * (p[0] - ob[0]) + Rm[1 * 3 + i] * (p[1] - ob[1]) + Rm[2 * 3 + i] * (p[2] - ob[2]);
-            l        = l / ob[3 + i];
-            s += l * l;
+            l[i] = Rm[0 * 3 + i] * (p[0] - ob[0]) + Rm[1 * 3 + i] * (p[1] - ob[1]) + Rm[2 * 3 + i] * (p[2] - ob[2]);
+            l[i] = l[i] / ob[3 + i];
         }
-        if (s <= 1.0)
+        int inside = ob[16] == 2.0 ? (l[0] * l[0] + l[1] * l[1] <= 1.0 && l[2] * l[2] <= 1.0)
+                                   : ((l[0] * l[0] + l[1] * l[1]) + l[2] * l[2] <= 1.0);
+        if (inside)
         {
-            if (ob[16] == 1.0) return 0.0;
+            if (ob[16] == 1.0) return ob[15];
             rho += ob[15];
         }
     }

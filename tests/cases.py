@@ -37,3 +37,32 @@ def cfg1_case(R=4096, seed=0, n_angles=32, w=128, h=128, depth=2, C=4, G=11, M=1
     c.grid = grid_init(c.A, C, G, gen).numpy()
     c.dec = decoder_init(C, gen).numpy()
     return c
+
+
+def workload_case(name, R=4096, seed=0):
+    """A slice of a measured workload (neat_b200.workloads): the very scene,
+    scan geometry and octree the benchmark trains on, R rays drawn from its
+    projections by the benchmark's batch sampler, and a seeded initial grid
+    and decoder of the workload's sizes.  Needs CUDA (the device projector
+    makes the scans)."""
+    from neat_b200.workloads import WORKLOADS, build_workload
+    cfg = WORKLOADS[name]
+    scene, tree, cam = build_workload(cfg, "cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    uv, img, tgt = scene.sample_batch(R, gen)
+    c = Case()
+    c.name, c.cfg, c.scene = name, cfg, scene
+    c.R, c.C, c.G, c.M = R, cfg["C"], cfg["G"], cfg["M"]
+    c.w, c.h, c.n_img = scene.w, scene.h, scene.n_img
+    c.objects = scene.objects
+    c.intr, c.rot, c.trans = scene.intrinsics, scene.rotation, scene.translation
+    c.tree = tree
+    c.A = tree.NumActiveNodes()
+    c.uv = uv.cpu().numpy()
+    c.img = img.cpu().numpy()
+    c.target = tgt.cpu().numpy()
+    g = torch.Generator().manual_seed(seed + 7)
+    c.grid = grid_init(c.A, c.C, c.G, g).numpy()
+    c.dec = decoder_init(c.C, g).numpy()
+    return c

@@ -252,6 +252,21 @@ def test_fused_step_long_tile_loops(neat, oracle, c8_long_case, path):
     _check_fused_step(oracle, c8_long_case, "c8_long", path)
 
 
+def _oracle_step(oracle, c):
+    """The oracle's samples, segments and f64 step for the case's batch (seed
+    99, step 1: what _trainer's first step draws), computed once per case."""
+    if getattr(c, "_oracle_step", None) is None:
+        o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+        T = c.tree
+        ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
+                                      seed=99, step=1)
+        seg = oracle.ray_segments(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M)
+        ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
+                              T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
+        c._oracle_step = (ref_s, seg, ref)
+    return c._oracle_step
+
+
 def _check_fused_step(oracle, c, which, path, **kw):
     _, tol_p, tol_g, tol_w = PATHS[path]
     tr = _trainer(c, path, **kw)
@@ -259,17 +274,11 @@ def _check_fused_step(oracle, c, which, path, **kw):
     loss = tr.step(_dev(c.uv), _dev(c.img), _dev(c.target), prediction=pred)
     torch.cuda.synchronize()
     tr.check_status()
-    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
-    T = c.tree
-    ref_s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, True,
-                                  seed=99, step=1)
-    seg = oracle.ray_segments(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M)
+    ref_s, seg, ref = _oracle_step(oracle, c)
     cnt = tr.counters.cpu().numpy()
     assert cnt[0] == seg["n"].shape[0]          # segments (bit-exact hit lists)
     assert cnt[1] == ref_s["ray_t"].shape[0]    # samples
     assert cnt[2] == seg["ray_nseg"].max()
-    ref = oracle.step_f64(ref_s, c.grid, c.dec, c.target, T.node_position_min, T.node_position_max,
-                          T.node_active_prefix_sum, lr_grid=1e-2, lr_decoder=5e-5, step=1)
     err = dict(pred=_rel2(pred.cpu().numpy(), ref["pred"]), loss=abs(float(loss.item()) - ref["loss"]) / ref["loss"],
                dec=_rel2(tr.decoder_grad.cpu().numpy(), ref["grad_dec"]),
                grid=_rel2(tr.grad_reference_layout(tr.grid_m).cpu().numpy().astype(np.float64) / 0.1,

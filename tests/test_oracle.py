@@ -213,6 +213,42 @@ def test_projector_matches_numeric_integral(oracle):
         assert abs(num - ana) < 2e-3 * max(1.0, ana)
 
 
+def test_porous_projector_matches_numeric_integral(oracle):
+    """Cylinder (additive) holding override spheres of their own density: the
+    analytic chord sums against the trapezoid rule over the point density,
+    for rays across the axis, along it (A = 0 in the radial quadratic) and in
+    a plane of constant z (no slab crossing)."""
+    from neat_b200 import scene as SC
+    objs = SC.porous_phantom(60, seed=4, radius=(0.05, 0.12), cylinder_radius=0.6, cylinder_half_height=0.5)
+    assert objs[0, 16] == 2 and np.all(objs[1:, 16] == 1) and np.all(objs[1:, 15] >= 0.2)
+    # no two spheres overlap, each lies inside the cylinder
+    c, r = objs[1:, 0:3], objs[1:, 3]
+    dist = np.linalg.norm(c[:, None] - c[None], axis=2) + np.eye(len(r)) * 10
+    assert np.all(dist >= r[:, None] + r[None, :])
+    assert np.all(np.hypot(c[:, 0], c[:, 1]) + r <= 0.6) and np.all(np.abs(c[:, 2]) + r <= 0.5)
+    rng = np.random.default_rng(8)
+    rays = []
+    for _ in range(6):
+        o = np.array([0.0, -3.0, 0.0]) + rng.uniform(-0.3, 0.3, 3)
+        d = np.array([0.0, 1.0, 0.0]) + rng.uniform(-0.15, 0.15, 3)
+        rays.append((o, d / np.linalg.norm(d)))
+    rays.append((np.array([0.1, 0.2, -3.0]), np.array([0.0, 0.0, 1.0])))   # along the axis
+    rays.append((np.array([0.05, -3.0, 0.3]), np.array([0.0, 1.0, 0.0])))  # constant z inside the slab
+    rays.append((np.array([0.05, -3.0, 0.7]), np.array([0.0, 1.0, 0.0])))  # constant z above it
+    for o, d in rays:
+        t = np.linspace(1.0, 5.0, 200001)
+        dens = oracle.phantom_density(objs, o[None, :] + t[:, None] * d[None, :])
+        num = np.trapezoid(dens, t)
+        ana = oracle.phantom_line(objs, o, d)
+        assert abs(num - ana) < 2e-4 * max(1.0, ana), (o, d, num, ana)
+    # density: inside a sphere its own, elsewhere in the cylinder 0.3, outside 0
+    grid = rng.uniform(-0.5, 0.5, (2000, 3))
+    free = grid[np.all(np.linalg.norm(grid[:, None] - c[None], axis=2) > r[None, :], axis=1)
+                & (np.hypot(grid[:, 0], grid[:, 1]) < 0.6)][0]
+    rho = oracle.phantom_density(objs, np.stack([objs[1, 0:3], free, [0.9, 0.0, 0.0]]))
+    assert rho[0] == objs[1, 15] and rho[1] == 0.3 and rho[2] == 0.0
+
+
 def test_step_f64_gradient_matches_finite_differences(oracle):
     c = cfg1_case(R=64, oracle=oracle, n_angles=4, w=32, h=32)
     o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)

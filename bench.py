@@ -403,6 +403,100 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
     return res
 
 
+def reference_gpu_igs(cfg, scene, tree, cam, dev, reps=5):
+    """The reference's own GPU grid sampler (IndirectGridSample3DForward/
+    BackwardCUDAKernel, src/modules/IndirectGridSample3D.cu:432-801, compiled
+    unmodified for sm_100a into oracle/_ref by `make -C oracle ref-cuda`)
+    against this library's standalone neat_igs_forward/backward, on the same
+    inputs: the SampleList of one batch of the workload (CreateSamplesForRays,
+    ray-major as the reference produces it; the local coordinates and grid
+    rows of ComputeLocalSamples), a random [A, C, G, G, G] grid and output
+    gradient.  Median CUDA-event time of `reps` launches per kernel on the
+    legacy default stream the reference launches on; the backward's zeroed
+    gradients are reset outside the timed region.  Also the forward on the
+    node-sorted sample order the fused step uses."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libneat_ref_cuda.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libneat_ref_cuda.so is not built (make -C oracle ref-cuda)"}
+    from neat_b200 import _lib
+    from neat_b200.api import ComputeLocalSamples, CreateSamplesForRays, GetRays
+    ref = ctypes.CDLL(path)
+    P, L, I = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    ref.ref_igs_forward_cuda.argtypes = [P, L, I, I, I, I, P, P, L, P]
+    ref.ref_igs_backward_cuda.argtypes = [P, L, I, I, I, I, P, P, L, P, P, P]
+    lib = _lib.load()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(31)
+    uv, img, _ = scene.sample_batch(cfg["R"], gen)
+    s = CreateSamplesForRays(tree, GetRays(cam, uv, img), cfg["M"], True, seed=1, step=1)
+    local = ComputeLocalSamples(tree, s.global_coordinate, s.node_id).contiguous()
+    index = tree.GlobalNodeIdToLocalActiveId(s.node_id).contiguous()
+    A, C, G = tree.NumActiveNodes(), cfg["C"], cfg["G"]
+    S = int(index.numel())
+    g = torch.Generator(device=dev)
+    g.manual_seed(32)
+    grid = torch.rand((A, C, G, G, G), generator=g, device=dev) * 2 - 1
+    go = torch.randn((S, C), generator=g, device=dev)
+    out_r = torch.empty((S, C), device=dev)
+    out_n = torch.empty((S, C), device=dev)
+    gg = torch.zeros_like(grid)
+    gu = torch.zeros((S, 3), device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+
+    def timed(fn, reset=None):
+        fn()  # warm-up
+        ts = []
+        for _ in range(reps):
+            if reset is not None:
+                reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rc = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if rc:
+                raise RuntimeError(f"IGS launch failed ({rc})")
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def reset():
+        gg.zero_()
+        gu.zero_()
+
+    def fwd_ref(ix=index, lc=local, out=out_r):
+        return ref.ref_igs_forward_cuda(grid.data_ptr(), A, C, G, G, G, ix.data_ptr(), lc.data_ptr(), S,
+                                        out.data_ptr())
+
+    def fwd_neat(ix=index, lc=local, out=out_n):
+        return lib.neat_igs_forward(grid.data_ptr(), A, C, G, G, G, ix.data_ptr(), lc.data_ptr(), S, out.data_ptr(), st)
+
+    def bwd_ref():
+        return ref.ref_igs_backward_cuda(grid.data_ptr(), A, C, G, G, G, index.data_ptr(), local.data_ptr(), S,
+                                         go.data_ptr(), gg.data_ptr(), gu.data_ptr())
+
+    def bwd_neat():
+        return lib.neat_igs_backward(grid.data_ptr(), A, C, G, G, G, index.data_ptr(), local.data_ptr(), S,
+                                     go.data_ptr(), gg.data_ptr(), gu.data_ptr(), st)
+
+    res = {"samples": S, "C": C, "G": G, "grid_rows": A,
+           "ref_forward_ms": timed(fwd_ref), "neat_forward_ms": timed(fwd_neat)}
+    res["forward_max_abs_diff"] = float((out_r - out_n).abs().max())
+    res["ref_backward_ms"] = timed(bwd_ref, reset)
+    res["neat_backward_ms"] = timed(bwd_neat, reset)
+    order = torch.sort(index, stable=True).indices
+    ix_s, lc_s = index[order].contiguous(), local[order].contiguous()
+    res["ref_forward_node_sorted_ms"] = timed(lambda: fwd_ref(ix_s, lc_s))
+    res["neat_forward_node_sorted_ms"] = timed(lambda: fwd_neat(ix_s, lc_s))
+    res["note"] = ("reference kernels built unmodified for sm_100a (nvcc defaults, FMA contraction on); "
+                   "forward_max_abs_diff is that contraction's rounding.  The fused step does not call these: its "
+                   "gather and scatter run inside the tile kernels on a channel-last grid (phase_ms)")
+    del grid, go, out_r, out_n, gg, gu
+    torch.cuda.empty_cache()
+    return res
+
+
 def large_workload(dev, steps=50, warmup=3):
     """The large porous configuration, BF16 + learned proposal: rays/s over one
     full 50-step proposal cycle (its uniform 32-sample TRAIN step included),
@@ -448,6 +542,8 @@ def main():
     ap.add_argument("--no-psnr", action="store_true", help="skip the small workload's time-to-PSNR leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / BF16 / BF16+proposal step variants")
     ap.add_argument("--no-large", action="store_true", help="skip the large porous workload's sub-line")
+    ap.add_argument("--no-ref-igs", action="store_true",
+                    help="skip timing the reference's GPU IGS kernels beside this library's")
     ap.add_argument("--volume-psnr", type=int, default=5000,
                     help="race plain vs BF16+proposal to the plain method's volume PSNR over this many steps "
                          "(full workload; 0 skips)")
@@ -588,6 +684,9 @@ def main():
     vrace = None
     if args.volume_psnr and not large:
         vrace = volume_psnr_race(cfg, scene, tree, cam, dev, args.volume_psnr)
+    ref_igs = None
+    if not args.no_ref_igs and not large:
+        ref_igs = reference_gpu_igs(cfg, scene, tree, cam, dev)
     large_line = None
     if not args.no_large and not large:
         del scene, tree, cam, batches
@@ -637,6 +736,7 @@ def main():
         "variants": variants,
         "volume_psnr_race": vrace,
         "large_workload": large_line,
+        "reference_gpu_igs": ref_igs,
     }
     print(json.dumps(line))
 

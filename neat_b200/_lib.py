@@ -8,6 +8,7 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libneat_b200.so")
+TORCH_SHIM_PATH = os.path.join(_HERE, "libneat_torch.so")
 
 NEAT_OK = 0
 NEAT_ERR_BAD_INPUT = 1
@@ -170,6 +171,29 @@ def load():
 
 def exported_symbols():
     return list(_SIGS)
+
+
+_torch_ops = None
+
+# operators the libtorch shim registers (namespace "neat"); each runs the C++
+# API of neat_b200/shim/neat_torch.h
+TORCH_OPS = ("IndirectGridSample3D", "GetRays", "CreateSamplesForRays", "ComputeLocalSamples", "ComputeImage",
+             "AdamSteps")
+
+
+def load_torch_ops():
+    """Load the libtorch shim (libneat_torch.so) into this process and return
+    torch.ops.neat; raises if it was not built."""
+    global _torch_ops
+    if _torch_ops is not None:
+        return _torch_ops
+    import torch
+    if not os.path.exists(TORCH_SHIM_PATH):
+        raise RuntimeError(f"{TORCH_SHIM_PATH} is missing: build it with `python -m neat_b200.csrc.build`")
+    load()
+    torch.ops.load_library(TORCH_SHIM_PATH)
+    _torch_ops = torch.ops.neat
+    return _torch_ops
 
 
 class NeatError(RuntimeError):

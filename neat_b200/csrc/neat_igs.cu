@@ -11,9 +11,9 @@
 namespace neat
 {
 
-__global__ void k_igs_forward(const float* __restrict__ grid, int64_t N, int C, int Z, int Y, int X,
-                              const int64_t* __restrict__ index, const float* __restrict__ uv, int64_t S,
-                              float* __restrict__ out)
+__global__ void __launch_bounds__(128)
+    k_igs_forward(const float* __restrict__ grid, int64_t N, int C, int Z, int Y, int X,
+                  const int64_t* __restrict__ index, const float* __restrict__ uv, int64_t S, float* __restrict__ out)
 {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -29,20 +29,27 @@ __global__ void k_igs_forward(const float* __restrict__ grid, int64_t N, int C, 
 #pragma unroll
     for (int q = 0; q < 8; ++q) cell[q] = corner_cell(k, q, Y, X);
     const int64_t G3 = (int64_t)Z * Y * X;
-    for (int c = 0; c < C; ++c)
+    const float* g   = grid + n * C * G3;  // channel c of row n: g + c G3
+    float* o         = out + s * C;
+    // two channels' 16 corner loads in flight per thread; plain (L1-cached)
+    // loads: neighbouring samples of a ray reuse the corner lines
+#pragma unroll 2
+    for (int c = 0; c < C; ++c, g += G3)
     {
-        const float* g = grid + (n * C + c) * G3;
-        float acc      = 0.0f;
+        float v[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc = fmaf(__ldg(g + cell[q]), k.w[q], acc);
-        out[s * C + c] = acc;
+        for (int q = 0; q < 8; ++q) v[q] = g[cell[q]];
+        float acc = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc = fmaf(v[q], k.w[q], acc);
+        o[c] = acc;
     }
 }
 
-__global__ void k_igs_backward(const float* __restrict__ grid, int64_t N, int C, int Z, int Y, int X,
-                               const int64_t* __restrict__ index, const float* __restrict__ uv, int64_t S,
-                               const float* __restrict__ grad_out, float* __restrict__ grad_grid,
-                               float* __restrict__ grad_uv)
+__global__ void __launch_bounds__(128)
+    k_igs_backward(const float* __restrict__ grid, int64_t N, int C, int Z, int Y, int X,
+                   const int64_t* __restrict__ index, const float* __restrict__ uv, int64_t S,
+                   const float* __restrict__ grad_out, float* __restrict__ grad_grid, float* __restrict__ grad_uv)
 {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -62,11 +69,13 @@ __global__ void k_igs_backward(const float* __restrict__ grid, int64_t N, int C,
     const float az0 = __fsub_rn(z1, iz), az1 = __fsub_rn(iz, z0);
     float gix = 0.0f, giy = 0.0f, giz = 0.0f;
     const float m1 = -1.0f;
-    for (int c = 0; c < C; ++c)
+    const float* g = grid + n * C * G3;  // channel c of row n: g + c G3
+    float* gg      = grad_grid + n * C * G3;
+    const float* gout = grad_out + s * C;
+#pragma unroll 1
+    for (int c = 0; c < C; ++c, g += G3, gg += G3)
     {
-        const float go = grad_out[s * C + c];
-        const float* g = grid + (n * C + c) * G3;
-        float* gg      = grad_grid + (n * C + c) * G3;
+        const float go = gout[c];
         float v[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q)

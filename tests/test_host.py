@@ -30,6 +30,21 @@ def test_library_exports_every_declared_symbol():
     assert sorted(_lib.exported_symbols()) == names
 
 
+def test_torch_shim_loads_and_registers_its_operators():
+    """libneat_torch.so (the reference's libtorch module API in C++) is built
+    against the installed torch, links libneat_b200.so and registers one torch
+    operator per entry of neat_torch.h; a call with CPU tensors is refused."""
+    import torch
+    from neat_b200 import _lib
+    from neat_b200.csrc import build
+    build.build()
+    ops = _lib.load_torch_ops()
+    for name in _lib.TORCH_OPS:
+        assert hasattr(ops, name), name
+    with pytest.raises(RuntimeError, match="CUDA tensor"):
+        ops.IndirectGridSample3D(torch.zeros(1, 1, 2, 2, 2), torch.zeros(1, dtype=torch.long), torch.zeros(1, 3))
+
+
 def test_library_host_calls_without_gpu():
     from neat_b200 import _lib
     lib = _lib.load()

@@ -429,6 +429,11 @@ typedef struct
     double* error_sums; /* optional device f64[2], accumulated */
     int64_t* counters;  /* device int64[4], as neat_step_out */
     int* status;        /* device int, OR-ed neat_status flags */
+    /* optional (host struct, may be NULL): the photometric calibration the   */
+    /* evaluation applies to the prediction before the error sums, as        */
+    /* EvalStepProjection calls tone_mapper->forward (samples/reconstruct.cpp:559); */
+    /* uses batch->uv and batch->image_id.                                    */
+    const neat_tonemap* tonemap;
 } neat_project_out;
 
 int neat_project(const neat_step_desc* desc, const float* grid, const float* decoder, const neat_proposal* proposal,

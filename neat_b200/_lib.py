@@ -91,7 +91,8 @@ NEAT_STEP_PHASES = 6
 
 
 class ProjectOut(ctypes.Structure):
-    _fields_ = [("prediction", c_void_p), ("error_sums", c_void_p), ("counters", c_void_p), ("status", c_void_p)]
+    _fields_ = [("prediction", c_void_p), ("error_sums", c_void_p), ("counters", c_void_p), ("status", c_void_p),
+                ("tonemap", c_void_p)]
 
 
 # name -> (restype, argtypes)

@@ -220,6 +220,61 @@ struct ToneMap
 __device__ __forceinline__ int tm_off_bias(const neat_tonemap& t) { return 2 * t.num_images; }
 __device__ __forceinline__ int tm_off_resp(const neat_tonemap& t) { return 2 * t.num_images + t.bias_w * t.bias_h; }
 
+// Where the forward of one ray landed: what its backward needs.
+struct TmPoint
+{
+    float ef = 1.0f;                  // exposure factor
+    int bx0 = 0, bx1 = 0, by0 = 0, by1 = 0;
+    float wx = 0.0f, wy = 0.0f;       // sensor-bias bilinear weights
+    float slope = 1.0f;               // d response / d input
+    int r0      = 0;
+    float rf    = 0.0f;               // response segment and its fraction
+};
+
+// Forward of the calibration for ray r with integral x (the enabled parts in
+// the reference's order: exposure, sensor bias, response).
+__device__ __forceinline__ float tonemap_forward(const ToneMap& tm, int64_t r, float x, TmPoint& q)
+{
+    const neat_tonemap& T = tm.t;
+    const int img         = tm.image_id[r];
+    float y               = x;
+    if (T.exposure)
+    {
+        if (T.exposure_mult) q.ef = T.params[img];
+        y = y * q.ef + T.params[T.num_images + img];
+    }
+    if (T.sensor_bias)
+    {
+        // grid_sample, align_corners false, border: ix = u W - 0.5 clamped to [0, W-1]
+        const float* sb = T.params + tm_off_bias(T);
+        float ix = fminf(fmaxf(tm.uv[2 * r] * (float)T.bias_w - 0.5f, 0.0f), (float)(T.bias_w - 1));
+        float iy = fminf(fmaxf(tm.uv[2 * r + 1] * (float)T.bias_h - 0.5f, 0.0f), (float)(T.bias_h - 1));
+        q.bx0    = (int)floorf(ix);
+        q.by0    = (int)floorf(iy);
+        q.bx1    = min(q.bx0 + 1, T.bias_w - 1);
+        q.by1    = min(q.by0 + 1, T.bias_h - 1);
+        q.wx     = ix - (float)q.bx0;
+        q.wy     = iy - (float)q.by0;
+        y += (1.0f - q.wy) * ((1.0f - q.wx) * sb[q.by0 * T.bias_w + q.bx0] + q.wx * sb[q.by0 * T.bias_w + q.bx1]) +
+             q.wy * ((1.0f - q.wx) * sb[q.by1 * T.bias_w + q.bx0] + q.wx * sb[q.by1 * T.bias_w + q.bx1]);
+    }
+    if (T.response)
+    {
+        // x / range * (P-1), clamped (border), linear interpolation; leak above range
+        const float* rp = T.params + tm_off_resp(T);
+        const float ix  = fminf(fmaxf(y / T.response_range * (float)(NEAT_RESPONSE_PARAMS - 1), 0.0f),
+                                (float)(NEAT_RESPONSE_PARAMS - 1));
+        q.r0            = min((int)floorf(ix), NEAT_RESPONSE_PARAMS - 2);
+        q.rf            = ix - (float)q.r0;
+        const float in_range = (y > 0.0f && y < T.response_range) ? 1.0f : 0.0f;
+        const float leak     = y > T.response_range ? y - T.response_range : 0.0f;
+        q.slope = in_range * (rp[q.r0 + 1] - rp[q.r0]) * ((float)(NEAT_RESPONSE_PARAMS - 1) / T.response_range) +
+                  (y > T.response_range ? 1.0f : 0.0f);
+        y = (1.0f - q.rf) * rp[q.r0] + q.rf * rp[q.r0 + 1] + leak;
+    }
+    return y;
+}
+
 __global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const double* __restrict__ partial,
                            const float* __restrict__ target, float* __restrict__ dpred, float* __restrict__ pred_out,
                            float* __restrict__ loss_part, float invR, const int64_t* nseg_eff, ToneMap tm)
@@ -254,46 +309,10 @@ __global__ void k_ray_loss(int64_t R, const int* __restrict__ ray_seg_off, const
         {
             // forward
             const int img = tm.image_id[r];
-            float ef = 1.0f, y = pred;
-            if (T.exposure)
-            {
-                if (T.exposure_mult) ef = T.params[img];
-                y = y * ef + T.params[T.num_images + img];
-            }
-            int bx0 = 0, bx1 = 0, by0 = 0, by1 = 0;
-            float wx = 0.0f, wy = 0.0f;
-            if (T.sensor_bias)
-            {
-                // grid_sample, align_corners false, border: ix = u W - 0.5 clamped to [0, W-1]
-                const float* sb = T.params + tm_off_bias(T);
-                float ix = fminf(fmaxf(tm.uv[2 * r] * (float)T.bias_w - 0.5f, 0.0f), (float)(T.bias_w - 1));
-                float iy = fminf(fmaxf(tm.uv[2 * r + 1] * (float)T.bias_h - 0.5f, 0.0f), (float)(T.bias_h - 1));
-                bx0 = (int)floorf(ix);
-                by0 = (int)floorf(iy);
-                bx1 = min(bx0 + 1, T.bias_w - 1);
-                by1 = min(by0 + 1, T.bias_h - 1);
-                wx  = ix - (float)bx0;
-                wy  = iy - (float)by0;
-                y += (1.0f - wy) * ((1.0f - wx) * sb[by0 * T.bias_w + bx0] + wx * sb[by0 * T.bias_w + bx1]) +
-                     wy * ((1.0f - wx) * sb[by1 * T.bias_w + bx0] + wx * sb[by1 * T.bias_w + bx1]);
-            }
-            float slope = 1.0f;
-            int r0 = 0;
-            float rf = 0.0f;
-            if (T.response)
-            {
-                // x / range * (P-1), clamped (border), linear interpolation; leak above range
-                const float* rp = T.params + tm_off_resp(T);
-                const float ix  = fminf(fmaxf(y / T.response_range * (float)(NEAT_RESPONSE_PARAMS - 1), 0.0f),
-                                        (float)(NEAT_RESPONSE_PARAMS - 1));
-                r0              = min((int)floorf(ix), NEAT_RESPONSE_PARAMS - 2);
-                rf              = ix - (float)r0;
-                const float in_range = (y > 0.0f && y < T.response_range) ? 1.0f : 0.0f;
-                const float leak     = y > T.response_range ? y - T.response_range : 0.0f;
-                slope = in_range * (rp[r0 + 1] - rp[r0]) * ((float)(NEAT_RESPONSE_PARAMS - 1) / T.response_range) +
-                        (y > T.response_range ? 1.0f : 0.0f);
-                y = (1.0f - rf) * rp[r0] + rf * rp[r0 + 1] + leak;
-            }
+            TmPoint q;
+            const float y = tonemap_forward(tm, r, pred, q);
+            const float ef = q.ef, wx = q.wx, wy = q.wy, slope = q.slope, rf = q.rf;
+            const int bx0 = q.bx0, bx1 = q.bx1, by0 = q.by0, by1 = q.by1, r0 = q.r0;
             const float diff = y - target[r];
             const float dy   = 2.0f * diff * invR;
             sq               = diff * diff;
@@ -842,7 +861,7 @@ static cudaError_t launch_tiles_path(const neat_step_desc* d, bool bwd, const St
 // optional per-block squared and absolute error sums against the target.
 __global__ void k_ray_project(int64_t R, const int* __restrict__ ray_seg_off, const double* __restrict__ partial,
                               const float* __restrict__ target, float* __restrict__ pred_out,
-                              double* __restrict__ err_part, const int64_t* nseg_eff)
+                              double* __restrict__ err_part, const int64_t* nseg_eff, ToneMap tm)
 {
     __shared__ double red[2][256];
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -856,6 +875,13 @@ __global__ void k_ray_project(int64_t R, const int* __restrict__ ray_seg_off, co
             double acc  = 0.0;
             for (int k = b; k < e; ++k) acc += partial[k];
             pred = (float)acc;
+        }
+        if (tm.t.params != nullptr)
+        {
+            // the evaluation applies the tone mapper to the prediction
+            // (EvalStepProjection, samples/reconstruct.cpp:559)
+            TmPoint q;
+            pred = tonemap_forward(tm, r, pred, q);
         }
         pred_out[r] = pred;
         if (target)
@@ -1054,8 +1080,15 @@ extern "C" int neat_project(const neat_step_desc* d, const float* grid, const fl
     // the loss-partials slab holds L.loss_blocks floats; the error sums need two
     // doubles per block, which the (larger) dpred slab of R floats provides
     double* err_part = out->error_sums ? (double*)w.dpred : nullptr;
+    ToneMap tm{};
+    if (out->tonemap)
+    {
+        tm.t        = *out->tonemap;
+        tm.uv       = b->uv;
+        tm.image_id = b->image_id;
+    }
     k_ray_project<<<L.loss_blocks, 256, 0, st>>>(R, w.ray_seg_off, w.partial, b->target, out->prediction, err_part,
-                                                  cnt + 0);
+                                                  cnt + 0, tm);
     if (err_part) k_err_final<<<1, 32, 0, st>>>(err_part, L.loss_blocks, out->error_sums);
     ok = ok && cudaGetLastError() == cudaSuccess;
     return ok ? NEAT_OK : NEAT_ERR_CUDA;

@@ -270,8 +270,10 @@ class FusedTrainer:
                 samples_per_node=None):
         """Deterministic projection (a = 0.5) of a ray batch with the current
         parameters: the forward of EvalStepProjection
-        (samples/reconstruct.cpp:551-559).  error_sums: optional device f64[2]
-        that receives += sum (pred-target)^2 and += sum |pred-target|."""
+        (samples/reconstruct.cpp:551-559), the trainer's photometric
+        calibration applied when it has one (tone_mapper->forward, :559).
+        error_sums: optional device f64[2] that receives += sum (pred-target)^2
+        and += sum |pred-target|."""
         R = uv.shape[0]
         self.reserve(R)
         if prediction is None:
@@ -282,7 +284,8 @@ class FusedTrainer:
                                target=target.data_ptr() if target is not None else None, num_rays=R)
         out = _lib.ProjectOut(prediction=prediction.data_ptr(),
                               error_sums=error_sums.data_ptr() if error_sums is not None else None,
-                              counters=self.counters.data_ptr(), status=self.status.data_ptr())
+                              counters=self.counters.data_ptr(), status=self.status.data_ptr(),
+                              tonemap=ctypes.addressof(self.tonemap.struct) if self.tonemap is not None else None)
         desc = _lib.StepDesc.from_buffer_copy(self.desc)
         prop = None
         if use_proposal:

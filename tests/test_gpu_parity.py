@@ -794,6 +794,50 @@ def test_photometric_calibration_step(neat, oracle, case):
     assert float(tm.grad.abs().max()) == 0.0
 
 
+def test_projection_applies_the_tone_mapper(neat, oracle, case):
+    """The evaluation path (EvalStepProjection, samples/reconstruct.cpp:551-559)
+    applies tone_mapper->forward to the predicted projection: the trainer's
+    projection with a calibration equals the f64 tone map (exposure factor and
+    bias, sensor-bias map, response curve) of the oracle's a = 0.5 projection,
+    and so do the error sums against the target."""
+    c = case
+    from neat_b200.trainer import FusedTrainer
+    tr = FusedTrainer(c.tree, _camera(c), c.C, c.G, c.M, seed=99, grid=torch.from_numpy(c.grid),
+                      decoder=torch.from_numpy(c.dec), tonemap=dict(exposure_mult=True, response_range=2.0))
+    tm = tr.tonemap
+    rng = np.random.default_rng(5)
+    n, b = tm.num_images, tm.bias_w * tm.bias_h
+    p0 = tm.params.cpu().numpy().astype(np.float64)
+    p0[:n] = rng.uniform(0.8, 1.2, n)
+    p0[n:2 * n] = rng.uniform(0.0, 0.05, n)
+    p0[2 * n:2 * n + b] = rng.uniform(0.0, 0.05, b)
+    p0[2 * n + b:] = np.sort(p0[2 * n + b:] + rng.uniform(-0.02, 0.02, 25))
+    p0[2 * n + b] = 0.0
+    tm.params.copy_(torch.from_numpy(p0.astype(np.float32)))
+    p0 = tm.params.cpu().numpy().astype(np.float64)
+    sums = torch.zeros(2, dtype=torch.float64, device="cuda")
+    pred = tr.project(_dev(c.uv), _dev(c.img), _dev(c.target), sums)
+    torch.cuda.synchronize()
+    tr.check_status()
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    s = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, c.M, False)
+    x = oracle.image_f64(s, torch.from_numpy(c.grid.astype(np.float64)), torch.from_numpy(c.dec.astype(np.float64)),
+                         T.node_position_min, T.node_position_max, T.node_active_prefix_sum, c.R)
+    P = torch.from_numpy(p0)
+    y = oracle.tonemap_f64(torch, x, torch.from_numpy(c.uv.astype(np.float64)), torch.from_numpy(c.img.astype(np.int64)),
+                           P[:n], P[n:2 * n], P[2 * n:2 * n + b].reshape(tm.bias_h, tm.bias_w), P[2 * n + b:], 2.0,
+                           mult=True).numpy()
+    assert _rel2(pred.cpu().numpy(), y) < 1e-5
+    diff = y - c.target.astype(np.float64)
+    got = sums.cpu().numpy()
+    assert abs(got[0] - (diff ** 2).sum()) <= 2e-5 * (diff ** 2).sum()
+    assert abs(got[1] - np.abs(diff).sum()) <= 2e-5 * np.abs(diff).sum()
+    # without a calibration the projection is the plain integral
+    plain = _trainer(c, "bf16x3").project(_dev(c.uv), _dev(c.img))
+    assert _rel2(plain.cpu().numpy(), x.numpy()) < 1e-5
+
+
 # ---------------------------------------------------------------- camera pose gradients
 @pytest.mark.parametrize("path", ["bf16x3", "bf16"])
 @pytest.mark.parametrize("which", ["cfg1", "c8"])

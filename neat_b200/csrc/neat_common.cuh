@@ -168,12 +168,17 @@ __device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, in
     return ok;
 }
 
-// Stratified sample position j of a segment, HyperTree.cu:341-358.
+// Stratified sample position j of a segment, HyperTree.cu:341-358, rounded as
+// the reference's CUDA build computes it: nvcc contracts `tmin + j * step` into
+// one fused multiply-add (checked bit for bit against the reference kernel
+// compiled for sm_100a), and `t1 * (1 - a) + t2 * a` into
+// fma(t1, 1 - a, t2 * a), the first product fused.  With a = 0.5 both products
+// of the blend are exact, so the blend is the correctly rounded sum either way.
 __device__ __forceinline__ float seg_t(float tmin, float step, int j, float a)
 {
-    float t1 = __fadd_rn(tmin, __fmul_rn((float)j, step));
-    float t2 = __fadd_rn(tmin, __fmul_rn((float)(j + 1), step));
-    return __fadd_rn(__fmul_rn(t1, __fsub_rn(1.0f, a)), __fmul_rn(t2, a));
+    float t1 = __fmaf_rn((float)j, step, tmin);
+    float t2 = __fmaf_rn((float)(j + 1), step, tmin);
+    return __fmaf_rn(t1, __fsub_rn(1.0f, a), __fmul_rn(t2, a));
 }
 
 __device__ __forceinline__ float jitter_a(bool jitter, uint64_t seed, uint32_t step, int ray, int local_index)

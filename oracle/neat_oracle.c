@@ -297,12 +297,16 @@ static int ray_hits(const float* o, const float* d, int A, const long* active_id
     return k;
 }
 
-/* Stratified sample j of a segment: HyperTree.cu:341-358.                   */
+/* Stratified sample j of a segment: HyperTree.cu:341-358, with the fused    */
+/* multiply-adds the reference's nvcc build forms (contraction is on there):  */
+/* t1 = fma(j, step, tmin), t2 = fma(j + 1, step, tmin),                      */
+/* t = fma(t1, 1 - a, t2 * a).  This file is compiled with contraction off,   */
+/* so every other operation rounds as written.                                */
 static float seg_sample_t(float tmin, float step, int j, float a)
 {
-    float t1 = tmin + (float)j * step;
-    float t2 = tmin + (float)(j + 1) * step;
-    return t1 * (1.0f - a) + t2 * a;
+    float t1 = fmaf((float)j, step, tmin);
+    float t2 = fmaf((float)(j + 1), step, tmin);
+    return fmaf(t1, 1.0f - a, t2 * a);
 }
 
 static float jitter_a(int jitter, uint64_t seed, uint32_t step_id, int ray, int local_index)

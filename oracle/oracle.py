@@ -61,12 +61,14 @@ _lib = None
 def build():
     """Builds the oracle library and, where the reference checkout the
     Makefile's REF names is present, oracle/_ref (the reference's own CPU
-    IGS, and its GPU IGS kernels for sm_100a, timed by bench.py's comparison
-    leg).  Without that checkout the prebuilt oracle/_ref, if any, is kept."""
+    IGS; its GPU IGS kernels for sm_100a, timed by bench.py's comparison leg;
+    its GPU ray sampler for sm_100a, which the tests compare against).
+    Without that checkout the prebuilt oracle/_ref, if any, is kept."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if subprocess.run(["make", "-s", "-C", HERE, "-q", "ref-available"], capture_output=True).returncode == 0:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
         subprocess.run(["make", "-s", "-C", HERE, "ref-cuda"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref-sampler"], check=True)
 
 
 def lib():

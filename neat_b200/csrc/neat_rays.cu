@@ -53,6 +53,9 @@ using WarpHits = WarpHitsT<kMaxHits, MAX_FRONT, kMaxDepth>;
 // meets at most 3 * 2^4 - 2 = 46 nodes of level 4, so 64 frontier entries
 // hold every internal level; 2.7 KB per warp instead of 10.7 KB.
 using WarpHitsStep = WarpHitsT<64, 64, 5>;
+// Depth 5 with room for every hit a line can have (3 * 2^5 - 2 = 94): the
+// step's per-ray capacity of a depth-5 tree; 3.6 KB per warp.
+using WarpHitsStep96 = WarpHitsT<96, 64, 5>;
 
 // Hits of one ray: active nodes whose slab test passes and whose segment is
 // at least 1e-5 long (HyperTree.cu:274-277).  Returns the raw count (only
@@ -487,6 +490,11 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
                                                                    (const NodeEntry*)table, D, M, cap_ray, origin,
                                                                    direction, ray_hits, ray_nseg, node_nseg, counters,
                                                                    status);
+    else if (cap_ray <= WarpHitsStep96::kHits && D <= WarpHitsStep96::kDepth)
+        k_step_rays<WarpHitsStep96><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
+                                                                     (const NodeEntry*)table, D, M, cap_ray, origin,
+                                                                     direction, ray_hits, ray_nseg, node_nseg,
+                                                                     counters, status);
     else
         k_step_rays<WarpHits><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
                                                                (const NodeEntry*)table, D, M, cap_ray, origin,

@@ -52,8 +52,8 @@ STEP_LAUNCHES = 22
 # larger batches (more grid reuse in L2)
 TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 463.2e6 / 2.908e6}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
-               "bf16x3": "k_bwd_rec<C=%d> (BF16x3 backward from the forward's records, MMA warp)",
-               "bf16": "k_step_tiles_tc<C=%d, BF16, backward>"}
+               "bf16x3": "k_bwd_rec<C=%d, BF16x3> (backward from the forward's records, MMA warp)",
+               "bf16": "k_bwd_rec<C=%d, BF16> (backward from the forward's records, MMA warp)"}
 PSNR_TARGET_DB = 40.0
 
 
@@ -62,11 +62,12 @@ PROPOSAL_ITERS = 50  # proposal Adam iterations on a TRAIN step (FusedTrainer de
 
 def step_launches(decoder, C, proposal, train):
     """Kernels one neat_train_step launches: STEP_LAUNCHES, plus the records
-    backward of the three-piece path at C = 4, 8 (the plain backward kernel
-    then returns at once); with the learned proposal a SAMPLE step adds the CDF
+    backward (three pieces at C = 4, 8; BF16 at C = 4, 8, 16; the plain
+    backward kernel then returns at once); with the learned proposal a SAMPLE step adds the CDF
     kernel and a TRAIN step the histogram zeroing, the node descriptors and 3
     kernels per proposal iteration."""
-    n = STEP_LAUNCHES + (1 if decoder == "bf16x3" and C in (4, 8) else 0)
+    records = (decoder == "bf16x3" and C in (4, 8)) or (decoder == "bf16" and C in (4, 8, 16))
+    n = STEP_LAUNCHES + (1 if records else 0)
     if proposal:
         n += (2 + 3 * PROPOSAL_ITERS) if train else 1
     return n

@@ -56,28 +56,48 @@ constexpr int BR_THREADS = 384;
 constexpr int BR_REGS_COMPUTE = 192, BR_REGS_MMA = 120;
 static_assert(8 * BR_REGS_COMPUTE + 4 * BR_REGS_MMA <= 12 * 168, "register split exceeds the launch's registers");
 
-template <int C>
+// Shared-memory and TMEM plan of the records backward for precision PREC.
+// Shared memory: the tile plan of Cfg<C, PREC, true> up to its slot data,
+// then [3][6][128] slot data for the second thread of a sample, the
+// reduction scratch and the mbarriers.  TMEM columns:
+//   three pieces (one CTA per SM, 512 columns): D1 [0,64) Z1 / silu'(z1);
+//     D2 [64,128) Z2; dH1 [64,256) (one block per W2 piece); h1 pieces
+//     [128,224); dX [64,112) until the next tile's Z2; weight gradients
+//     [256,496);
+//   one piece (BF16, 256 columns): D1 [0,64); D2 [64,128) Z2, then dH1, then
+//     dX [64, 64 + K1); h1 [128,160); weight gradients [160, 160 + NW).
+template <int C, int PREC>
 struct BwdRecPlan
 {
-    using K = Cfg<C, BF16X3, true>;
-    // [3][6][128] slot data for the second thread of a sample (in the place of
-    // the plain kernel's [2][6][128] slot data and placement records)
-    static constexpr int QB    = 6 * 128;
-    static constexpr int BYTES = K::OFF_M + 96;  // 10 mbarriers, then the TMEM slot at +88
-    static_assert(K::OFF_R - K::OFF_Q >= 3 * QB * 4, "three slot-data buffers must fit");
-    static_assert(K::NX1 == 1 && K::WCAT && K::CACHE && K::D4 == 256 && K::TA_COL == 128,
-                  "TMEM plan: D1 [0,64) Z1 / silu'(z1); D2 [64,128) Z2; dH1 [64,256); "
+    using K  = Cfg<C, PREC, true>;
+    using PP = Prec<PREC>;
+    static constexpr int QB     = 6 * 128;
+    static constexpr int OFF_Q  = K::OFF_Q;
+    static constexpr int OFF_R0 = OFF_Q + 3 * QB * 4;
+    static constexpr int OFF_R  = K::OFF_R > OFF_R0 ? K::OFF_R : OFF_R0;
+    static constexpr int OFF_M0 = ((OFF_R + 8 * HH * 4) + 15) / 16 * 16;
+    static constexpr int OFF_M  = K::OFF_M > OFF_M0 ? K::OFF_M : OFF_M0;
+    static constexpr int BYTES  = OFF_M + 96;  // 10 mbarriers, then the TMEM slot at +88
+    static constexpr int TTA    = 128;         // h1 pieces (layer-2 A operand)
+    static constexpr int TD4    = PREC == BF16X3 ? 256 : TTA + 32 * PP::PIECES;
+    static constexpr uint32_t TMEM_COLS = PREC == BF16X3 ? 512 : 256;
+    static_assert(PREC != BF16X3 || (K::CACHE && K::D4 == 256 && K::OFF_R - K::OFF_Q >= 3 * QB * 4 &&
+                                     OFF_R == K::OFF_R && OFF_M == K::OFF_M),
+                  "three-piece plan: D1 [0,64) Z1 / silu'(z1); D2 [64,128) Z2; dH1 [64,256); "
                   "h1 pieces [128,224); dX [64,112) until the next tile's Z2; weight gradients [256,496)");
-    static_assert(3 * K::K1 <= 64, "dX column blocks must fit below the h1 pieces");
+    static_assert(K::NX1 == 1 && K::WCAT && K::TA_COL == TTA, "one [x | 1] buffer, piece-concatenated GEMMs");
+    static_assert(PP::PIECES * K::K1 <= 64, "dX column blocks must fit below the h1 pieces");
+    static_assert(64 + 64 * PP::PIECES <= TD4 && TTA + 32 * PP::PIECES <= TD4 || PREC == BF16X3,
+                  "one piece: dH1 and the h1 pieces below the weight gradients");
+    static_assert(TD4 + PP::PIECES * K::NW <= (int)TMEM_COLS, "weight gradients must fit the allocation");
     static_assert(BYTES <= 232448, "shared-memory plan exceeds the per-CTA limit");
 };
 
-template <int C, bool POSE>
+template <int C, int PREC, bool POSE>
 __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
 {
-    constexpr int PREC = BF16X3;
     using K            = Cfg<C, PREC, true>;
-    using L            = BwdRecPlan<C>;
+    using L            = BwdRecPlan<C, PREC>;
     using P            = Prec<PREC>;
     using HB           = typename K::HB;
     using X1           = typename K::X1;
@@ -102,10 +122,10 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     float* sb3         = sw3 + HH;
     float* sval        = reinterpret_cast<float*>(sm + K::OFF_V);  // [2][128] y halves
     float* sq          = reinterpret_cast<float*>(sm + K::OFF_Q);  // [3][6][128]
-    float* sred        = reinterpret_cast<float*>(sm + K::OFF_R);
-    uint32_t* tslot    = reinterpret_cast<uint32_t*>(sm + K::OFF_M + 88);
+    float* sred        = reinterpret_cast<float*>(sm + L::OFF_R);
+    uint32_t* tslot    = reinterpret_cast<uint32_t*>(sm + L::OFF_M + 88);
     const uint32_t s_base = smem_u32(sm);
-    const uint32_t mbase  = smem_u32(sm + K::OFF_M);
+    const uint32_t mbase  = smem_u32(sm + L::OFF_M);
     // MMA completion (tcgen05.commit, count 1)
     const uint32_t m_l1 = mbase, m_z2 = mbase + 8, m_dh1 = mbase + 16, m_wg = mbase + 24, m_end = mbase + 32;
     // operands ready (one arrival per compute warp, count 8)
@@ -156,7 +176,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     if (w == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(512)
+                     "r"(L::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -166,7 +186,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t lane = (uint32_t)((w & 3) * 32) << 16;  // TMEM lane quadrant of this warp
-    const uint32_t tD1 = tmem, tD2 = tmem + 64, tTA = tmem + K::TA_COL, tD4 = tmem + K::D4;
+    const uint32_t tD1 = tmem, tD2 = tmem + 64, tTA = tmem + L::TTA, tD4 = tmem + L::TD4;
 
     const int64_t ntiles = (S + 127) / 128, T0 = blockIdx.x, G = gridDim.x;
     constexpr uint32_t idF = make_idesc(P::FMT, 0, 0, 128, HH);  // layers 1 and 2
@@ -863,34 +883,49 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
     fence_before();
     __syncthreads();
     if (w == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::TMEM_COLS)
+                     : "memory");
 }
 
-template <int C, bool POSE>
+template <int C, int PREC, bool POSE>
 static cudaError_t launch_bwd_rec_t(int grid, const StepTcArgs& args, cudaStream_t st)
 {
-    constexpr int smem = BwdRecPlan<C>::BYTES;
+    constexpr int smem = BwdRecPlan<C, PREC>::BYTES;
     static bool attr   = false;
     if (!attr)
     {
-        cudaFuncSetAttribute(k_bwd_rec<C, POSE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_bwd_rec<C, PREC, POSE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    k_bwd_rec<C, POSE><<<grid, BR_THREADS, smem, st>>>(args);
+    k_bwd_rec<C, PREC, POSE><<<grid, BR_THREADS, smem, st>>>(args);
     return cudaGetLastError();
+}
+
+template <int C, int PREC>
+static cudaError_t launch_bwd_rec_p(int grid, const StepTcArgs& args, cudaStream_t st)
+{
+    return args.seg_pgrad != nullptr ? launch_bwd_rec_t<C, PREC, true>(grid, args, st)
+                                     : launch_bwd_rec_t<C, PREC, false>(grid, args, st);
 }
 
 }  // namespace tc
 
-bool bwd_rec_supported(int C) { return C == 4 || C == 8; }
-
-cudaError_t launch_bwd_rec(int C, int grid, const StepTcArgs& args, cudaStream_t st)
+// Three pieces: C = 4, 8 (at C = 16 the three dX blocks do not fit below the
+// h1 pieces); one piece (BF16): C = 4, 8, 16.
+bool bwd_rec_supported(int C, int prec)
 {
-    const bool pose = args.seg_pgrad != nullptr;
-    switch (C)
+    return prec == tc::BF16X3 ? (C == 4 || C == 8) : (C == 4 || C == 8 || C == 16);
+}
+
+cudaError_t launch_bwd_rec(int C, int prec, int grid, const StepTcArgs& args, cudaStream_t st)
+{
+    switch (C * 2 + prec)
     {
-        case 4: return pose ? tc::launch_bwd_rec_t<4, true>(grid, args, st) : tc::launch_bwd_rec_t<4, false>(grid, args, st);
-        case 8: return pose ? tc::launch_bwd_rec_t<8, true>(grid, args, st) : tc::launch_bwd_rec_t<8, false>(grid, args, st);
+        case 4 * 2 + tc::BF16X3: return tc::launch_bwd_rec_p<4, tc::BF16X3>(grid, args, st);
+        case 8 * 2 + tc::BF16X3: return tc::launch_bwd_rec_p<8, tc::BF16X3>(grid, args, st);
+        case 4 * 2 + tc::BF16: return tc::launch_bwd_rec_p<4, tc::BF16>(grid, args, st);
+        case 8 * 2 + tc::BF16: return tc::launch_bwd_rec_p<8, tc::BF16>(grid, args, st);
+        case 16 * 2 + tc::BF16: return tc::launch_bwd_rec_p<16, tc::BF16>(grid, args, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -85,8 +85,8 @@ using StepTcArgs = StepTileArgs;
 // Backward tiles from the forward's per-sample records with a warp that only
 // issues the tensor-core work (neat_bwd_rec.cu): three-piece operands, C = 4
 // or 8.  Runs while the step's samples fit the records (else returns at once).
-bool bwd_rec_supported(int C);
-cudaError_t launch_bwd_rec(int C, int grid, const StepTileArgs& args, cudaStream_t st);
+bool bwd_rec_supported(int C, int prec);
+cudaError_t launch_bwd_rec(int C, int prec, int grid, const StepTileArgs& args, cudaStream_t st);
 
 // Camera pose gradients (neat_pose.cu): per-segment sums -> per-ray dL/do,
 // dL/dd -> per-image rotation tangent and translation, camera intrinsics.

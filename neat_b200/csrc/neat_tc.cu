@@ -1283,12 +1283,23 @@ static cudaError_t launch(bool bwd, const StepTcArgs& args, cudaStream_t st)
         // the step's decoder partials are sized by the plain backward's grid
         const int g = tc_grid<C, PREC, true>(smem);
         StepTcArgs a2 = args;
-        if (PREC == BF16X3 && args.rec != nullptr && bwd_rec_supported(C))
+        if (args.rec != nullptr && bwd_rec_supported(C, PREC))
         {
-            // the records backward; the plain kernel below then runs only
-            // when the step's samples exceed the records
-            const cudaError_t e = launch_bwd_rec(C, g, args, st);
+            // the records backward (one CTA per SM); the plain kernel below
+            // then runs only when the step's samples exceed the records.  The
+            // decoder partials have a row per CTA of the plain kernel's grid:
+            // the rows past the records kernel's grid are zeroed first (the
+            // plain kernel, when it runs, writes every row)
+            const int gr          = std::min(g, sm_count());
+            const cudaError_t e = launch_bwd_rec(C, PREC, gr, args, st);
             if (e != cudaSuccess) return e;
+            if (gr < g)
+            {
+                const size_t row = (size_t)DecOff<C>::total;
+                const cudaError_t z =
+                    cudaMemsetAsync(args.dec_part + (size_t)gr * row, 0, (size_t)(g - gr) * row * sizeof(float), st);
+                if (z != cudaSuccess) return z;
+            }
             a2.rec_skip = 1;
         }
         if (args.seg_pgrad)

@@ -393,25 +393,49 @@ __global__ void k_prop_begin(int* counter, float lr, float b1, float b2, float* 
     scal[1]      = (float)sqrt(bc2);
 }
 
-// Reduce the block partials (fixed order), normalise by the number of
-// segments used, Adam.
-__global__ void k_prop_adam(const float* __restrict__ part, int nblocks, const float* __restrict__ scal,
-                            neat_proposal pr)
+// Reduce the block partials, normalise by the number of segments used, Adam.
+// A block takes 32 parameters (one per lane, so each partial row is read
+// coalesced); its 8 warps split the partial rows (warp w: rows w, w + 8, ..)
+// and their sums are added in warp order: a fixed association, the same
+// every call.  Every block forms the segment count the same way.
+constexpr int PA_WARPS = 8;
+__global__ void __launch_bounds__(32 * PA_WARPS)
+    k_prop_adam(const float* __restrict__ part, int nblocks, const float* __restrict__ scal, neat_proposal pr)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= PropOff::total) return;
+    __shared__ float red[PA_WARPS][35];  // 32 parameter sums, count, loss sum, target-entropy sum
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i    = blockIdx.x * 32 + lane;
     float g = 0.0f, cnt = 0.0f, ls = 0.0f, hs = 0.0f;
-    for (int b = 0; b < nblocks; ++b)
+    for (int b = w; b < nblocks; b += PA_WARPS)
     {
-        g += part[(int64_t)b * PT_PARTS + i];
-        cnt += part[(int64_t)b * PT_PARTS + PropOff::total + 1];
-        if (i == 0)
+        const float* pb = part + (int64_t)b * PT_PARTS;
+        if (i < PropOff::total) g += pb[i];
+        if (lane == 0)
         {
-            ls += part[(int64_t)b * PT_PARTS + PropOff::total];
-            hs += part[(int64_t)b * PT_PARTS + PropOff::total + 2];
+            ls += pb[PropOff::total];
+            cnt += pb[PropOff::total + 1];
+            hs += pb[PropOff::total + 2];
         }
     }
-    g = cnt > 0.0f ? g / cnt : 0.0f;
+    red[w][lane] = g;
+    if (lane == 0)
+    {
+        red[w][32] = cnt;
+        red[w][33] = ls;
+        red[w][34] = hs;
+    }
+    __syncthreads();
+    if (w != 0 || i >= PropOff::total) return;
+    g = cnt = ls = hs = 0.0f;
+#pragma unroll
+    for (int k = 0; k < PA_WARPS; ++k)
+    {
+        g += red[k][lane];
+        cnt += red[k][32];
+        ls += red[k][33];
+        hs += red[k][34];
+    }
+    g          = cnt > 0.0f ? g / cnt : 0.0f;
     pr.grad[i] = g;
     if (i == 0 && pr.loss)
     {
@@ -444,7 +468,7 @@ cudaError_t launch_proposal_train(const SegRec* segs, const int64_t* counters, c
         k_prop_grad<<<nb, 32 * PT_WARPS, smem, st>>>(segs, counters, seg_hist, pr->params, pr->node_desc, pr->mix,
                                                      it, part);
         k_prop_begin<<<1, 32, 0, st>>>(pr->step_counter, pr->lr, pr->beta1, pr->beta2, scal);
-        k_prop_adam<<<(PropOff::total + 255) / 256, 256, 0, st>>>(part, nb, scal, *pr);
+        k_prop_adam<<<(PropOff::total + 31) / 32, 32 * PA_WARPS, 0, st>>>(part, nb, scal, *pr);
     }
     return cudaGetLastError();
 }

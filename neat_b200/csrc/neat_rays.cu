@@ -447,34 +447,77 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
     }
 }
 
-// Place every ray's segments into its nodes' buckets (thread per segment).
 // Place every ray's segments into its nodes' buckets: one thread per segment
-// (ray-major index rm < counters[0]); its ray by binary search in the ray
-// offsets.
-__global__ void k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_seg_off, int64_t R,
-                             int cap_ray, const int* __restrict__ node_seg_off, int* __restrict__ node_cursor,
-                             SegRec* __restrict__ segs, int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
+// (ray-major index rm < counters[0]), 256 consecutive segments per block.  The
+// ray of a segment is the last r with ray_seg_off[r] <= rm: thread 0 finds the
+// block's first ray in global memory, the block stages the next 257 ray
+// offsets in shared memory and each thread searches there (rays that miss the
+// volume own no segment, so a window can end before the block's last segment;
+// such a thread searches global memory from the window's end).
+constexpr int PLACE_T = 256;
+
+__device__ __forceinline__ int64_t last_le(const int* __restrict__ off, int64_t lo, int64_t hi, int64_t v)
 {
-    const int64_t nseg = *nseg_eff;  // 0 after a capacity overflow
-    for (int64_t rm = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rm < nseg;
-         rm += (int64_t)gridDim.x * blockDim.x)
+    // off[lo] <= v < off[hi]
+    while (hi - lo > 1)
     {
-        int64_t lo = 0, hi = R;  // ray_seg_off[lo] <= rm < ray_seg_off[hi]
-        while (hi - lo > 1)
+        const int64_t mid = (lo + hi) >> 1;
+        if (off[mid] <= v)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(PLACE_T)
+    k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_seg_off, int64_t R, int cap_ray,
+                 const int* __restrict__ node_seg_off, int* __restrict__ node_cursor, SegRec* __restrict__ segs,
+                 int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
+{
+    __shared__ int soff[PLACE_T + 1];
+    __shared__ int64_t sr0;
+    const int64_t nseg = *nseg_eff;  // 0 after a capacity overflow
+    for (int64_t base = (int64_t)blockIdx.x * PLACE_T; base < nseg; base += (int64_t)gridDim.x * PLACE_T)
+    {
+        if (threadIdx.x == 0) sr0 = last_le(ray_seg_off, 0, R, base);
+        __syncthreads();
+        const int64_t r0 = sr0;
+        for (int j = threadIdx.x; j <= PLACE_T; j += PLACE_T)
+            soff[j] = (r0 + j <= R) ? ray_seg_off[r0 + j] : 0x7fffffff;
+        __syncthreads();
+        const int64_t rm = base + threadIdx.x;
+        if (rm < nseg)
         {
-            const int64_t mid = (lo + hi) >> 1;
-            if (ray_seg_off[mid] <= rm)
-                lo = mid;
+            int64_t ray;
+            if (rm < soff[PLACE_T])
+            {
+                int lo = 0, hi = PLACE_T;  // soff[lo] <= rm < soff[hi]
+                while (hi - lo > 1)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (soff[mid] <= rm)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                ray = r0 + lo;
+            }
             else
-                hi = mid;
+            {
+                ray = last_le(ray_seg_off, r0 + PLACE_T, R, rm);
+            }
+            const int p  = (int)(rm - ray_seg_off[ray]);
+            SegRec sg    = ray_hits[ray * cap_ray + p];
+            const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
+            if (rm < cap && nm < cap)  // always: the totals were checked against cap
+            {
+                sg.rm     = (int32_t)rm;
+                segs[nm]  = sg;
+                seg_n[nm] = sg.n;
+            }
         }
-        const int p  = (int)(rm - ray_seg_off[lo]);
-        SegRec sg    = ray_hits[lo * cap_ray + p];
-        const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
-        if (rm >= cap || nm >= cap) continue;  // unreachable: the totals were checked against cap
-        sg.rm     = (int32_t)rm;
-        segs[nm]  = sg;
-        seg_n[nm] = sg.n;
+        __syncthreads();  // soff and sr0 are rewritten by the next round
     }
 }
 
@@ -510,9 +553,10 @@ cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const
     if (R <= 0) return cudaSuccess;
     (void)ray_nseg;
     const int64_t est = std::min<int64_t>(cap, R * 8);
-    const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((est + 255) / 256, (int64_t)sm_count() * 16));
-    k_step_place<<<nb, 256, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, node_cursor, segs, seg_n,
-                                     nseg_eff, cap);
+    const unsigned nb =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((est + PLACE_T - 1) / PLACE_T, (int64_t)sm_count() * 16));
+    k_step_place<<<nb, PLACE_T, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, node_cursor, segs, seg_n,
+                                         nseg_eff, cap);
     return cudaGetLastError();
 }
 

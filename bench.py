@@ -50,7 +50,9 @@ STEP_LAUNCHES = 22
 # the same scene at 2^16 rays (dram__bytes_read.sum + dram__bytes_write.sum = 463.2 MB
 # for 2.908 M samples), scaled to a launch by its samples -- an upper bound at
 # larger batches (more grid reuse in L2)
-TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 463.2e6 / 2.908e6}
+TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 463.2e6 / 2.908e6,
+                            # k_bwd_rec<C=8, BF16>, same scene and case: 344.3 + 119.7 MB
+                            ("full", "bf16"): 464.0e6 / 2.908e6}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_bwd_rec<C=%d, BF16x3> (backward from the forward's records, MMA warp)",
                "bf16": "k_bwd_rec<C=%d, BF16> (backward from the forward's records, MMA warp)"}

@@ -353,8 +353,10 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
     """Time to the plain method's volume PSNR.  The plain method (FP32-accurate
     decoder, uniform 32 samples) trains `steps` steps; its final volume PSNR is
     the target.  Then BF16 + learned proposal (12 samples per segment) trains
-    until it reaches the target within 0.1 dB (at most `steps` steps).  Both
-    runs see the same batches from the same initial state and are evaluated
+    until it reaches the target within 0.1 dB (at most `steps` steps), and so
+    does BF16 with 12 uniform samples per segment (the same budget without the
+    network: the proposal's ablation).  All runs see the same batches from the
+    same initial state and are evaluated
     every `every` steps; each run's time to the target - 0.1 dB is the
     CUDA-event time of its training steps up to the first evaluation at or
     above it (evaluations excluded).  Volume PSNR = 10 log10(peak^2 / MSE) over
@@ -371,8 +373,11 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
 
     res = {}
     target = None
-    for name, dec, prop in (("plain_fp32", "bf16x3", False), ("bf16_proposal12", "bf16", True)):
-        tr = make_trainer(cfg, tree, cam, dev, dec, prop, cfg["seed"])
+    # the third run is the ablation of the learned part: the same BF16 step and
+    # the same 12-sample budget per segment, placed uniformly (no network)
+    for name, dec, prop, M in (("plain_fp32", "bf16x3", False, cfg["M"]), ("bf16_proposal12", "bf16", True, cfg["M"]),
+                               ("bf16_uniform12", "bf16", False, 12)):
+        tr = make_trainer(dict(cfg, M=M), tree, cam, dev, dec, prop, cfg["seed"])
         gen = torch.Generator(device=dev)
         gen.manual_seed(777)
         ms, curve, k = 0.0, [], 0
@@ -392,7 +397,7 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
             target = curve[-1][2]
         del tr
         torch.cuda.empty_cache()
-    for name in ("plain_fp32", "bf16_proposal12"):
+    for name in ("plain_fp32", "bf16_proposal12", "bf16_uniform12"):
         hit = [c for c in res[name]["curve"] if c[2] >= target - 0.1]
         res[name]["ms_to_target"] = hit[0][1] if hit else None
         res[name]["steps_to_target"] = hit[0][0] if hit else None
@@ -400,6 +405,8 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
     res["target_db"] = target - 0.1
     res["plain_final_db"] = target
     res["speedup_to_target"] = (a / b) if (a and b) else None
+    u = res["bf16_uniform12"]["ms_to_target"]
+    res["proposal_vs_uniform12_to_target"] = (u / b) if (u and b) else None
     res["definition"] = ("target = plain method's final volume PSNR - 0.1 dB; volume PSNR = 10 log10(peak^2 / MSE), "
                          "%d^3 voxel-corner lattice vs the phantom density, f64; time = CUDA events around the "
                          "training steps" % vol_n)

@@ -685,20 +685,23 @@ def main():
     sm_mhz = clock_info.get("sm_mhz") or 1965.0
     simt_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
 
+    # single-GPU characterisation legs (N = 1 only, like the CPU baseline): the
+    # step variants, the races, the large workload and the reference kernels
+    single = world == 1
     ttp = None
-    if not args.no_psnr:
+    if not args.no_psnr and single:
         ttp = time_to_psnr(dev, ["simt", "bf16x3", "bf16"])
     variants = None
-    if not args.no_variants and not large:
+    if not args.no_variants and not large and single:
         variants = step_variants(cfg, scene, tree, cam, dev, value / world)
     vrace = None
-    if args.volume_psnr and not large:
+    if args.volume_psnr and not large and single:
         vrace = volume_psnr_race(cfg, scene, tree, cam, dev, args.volume_psnr)
     ref_igs = None
-    if not args.no_ref_igs and not large:
+    if not args.no_ref_igs and not large and single:
         ref_igs = reference_gpu_igs(cfg, scene, tree, cam, dev)
     large_line = None
-    if not args.no_large and not large:
+    if not args.no_large and not large and single:
         del scene, tree, cam, batches
         torch.cuda.empty_cache()
         large_line = large_workload(dev)

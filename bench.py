@@ -59,7 +59,7 @@ KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
 PSNR_TARGET_DB = 40.0
 
 
-PROPOSAL_ITERS = 50  # proposal Adam iterations on a TRAIN step (FusedTrainer default)
+PROPOSAL_ITERS = 10  # proposal Adam iterations on a TRAIN step (FusedTrainer default)
 
 
 def step_launches(decoder, C, proposal, train):

@@ -24,7 +24,7 @@ class FusedTrainer:
     def __init__(self, tree: HyperTreeBase, camera: CameraModel, num_features=4, grid_size=17,
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
-                 proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=50,
+                 proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=10,
                  proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
                  tonemap=None, pose_grad=False, optimize_pose=False, optimize_intrinsics=False, lr_pose=1e-3,
                  lr_intrinsics=100.0, record_samples_per_ray=0):

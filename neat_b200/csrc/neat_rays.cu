@@ -425,8 +425,10 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
         sg.tmin       = ws.tmin[i];
         sg.tmax       = ws.tmax[i];
         sg.n          = ws.n[i];
-        sg.rm         = p;  // rank in the ray; made global when placed
         sg.row        = ws.a[i];
+        // rank in its node's bucket (the count's own increment); the placement
+        // puts the segment there and makes rm its ray-major index
+        sg.rm         = atomicAdd(&node_nseg[sg.row], 1);
         sg.step       = __fdiv_rn(__fsub_rn(sg.tmax, sg.tmin), (float)sg.n);
         const NodeEntry e = table[ws.node[i]];
 #pragma unroll
@@ -438,7 +440,6 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
             sg.mx[c] = plane_coord(e.k[2 * c + 1], D);
         }
         out[p] = sg;
-        atomicAdd(&node_nseg[sg.row], 1);
     }
     if (lane == 0)
     {
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
 }
 
 // Place every ray's segments into its nodes' buckets: one thread per segment
-// (ray-major index rm < counters[0]), 256 consecutive segments per block.  The
+// (ray-major index rm < counters[0]), 256 consecutive segments per block; the
+// slot in the bucket is the rank the walk drew when it counted the segment.  The
 // ray of a segment is the last r with ray_seg_off[r] <= rm: thread 0 finds the
 // block's first ray in global memory, the block stages the next 257 ray
 // offsets in shared memory and each thread searches there (rays that miss the
@@ -472,7 +474,7 @@ __device__ __forceinline__ int64_t last_le(const int* __restrict__ off, int64_t 
 
 __global__ void __launch_bounds__(PLACE_T)
     k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_seg_off, int64_t R, int cap_ray,
-                 const int* __restrict__ node_seg_off, int* __restrict__ node_cursor, SegRec* __restrict__ segs,
+                 const int* __restrict__ node_seg_off, SegRec* __restrict__ segs,
                  int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
 {
     __shared__ int soff[PLACE_T + 1];
@@ -509,7 +511,7 @@ __global__ void __launch_bounds__(PLACE_T)
             }
             const int p  = (int)(rm - ray_seg_off[ray]);
             SegRec sg    = ray_hits[ray * cap_ray + p];
-            const int nm = node_seg_off[sg.row] + atomicAdd(&node_cursor[sg.row], 1);
+            const int nm = node_seg_off[sg.row] + sg.rm;  // the rank the walk drew in the node's bucket
             if (rm < cap && nm < cap)  // always: the totals were checked against cap
             {
                 sg.rm     = (int32_t)rm;
@@ -547,7 +549,7 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
 }
 
 cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,
-                              int cap_ray, const int* node_seg_off, int* node_cursor, SegRec* segs, int* seg_n,
+                              int cap_ray, const int* node_seg_off, SegRec* segs, int* seg_n,
                               const int64_t* nseg_eff, int64_t cap, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
@@ -555,7 +557,7 @@ cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const
     const int64_t est = std::min<int64_t>(cap, R * 8);
     const unsigned nb =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((est + PLACE_T - 1) / PLACE_T, (int64_t)sm_count() * 16));
-    k_step_place<<<nb, PLACE_T, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, node_cursor, segs, seg_n,
+    k_step_place<<<nb, PLACE_T, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, segs, seg_n,
                                          nseg_eff, cap);
     return cudaGetLastError();
 }

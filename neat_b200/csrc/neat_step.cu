@@ -610,7 +610,7 @@ struct StepLayout
 {
     enum
     {
-        ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_CURSOR, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
+        ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
         SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, SEG_CDF, SEG_HIST,
         PROP_PART, SEG_PGRAD, RAY_PGRAD, REC, NUM
     };
@@ -642,8 +642,8 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
     if (L.bwd_grid <= 0) return false;
     const int64_t P        = decoder_params(d->C);
     const int64_t scan_max = std::max(std::max(R, A), cap) + 1;
-    size_t sz[StepLayout::NUM] = {
-        (size_t)R * 3 * 4, (size_t)R * 3 * 4, (size_t)R * 4, (size_t)(R + 1) * 4, (size_t)A * 4, (size_t)A * 4,
+    size_t sz[] = {
+        (size_t)R * 3 * 4, (size_t)R * 3 * 4, (size_t)R * 4, (size_t)(R + 1) * 4, (size_t)A * 4,
         (size_t)(A + 1) * 4, (size_t)R * L.cap_ray * sizeof(SegRec), (size_t)cap * sizeof(SegRec), (size_t)cap * 4,
         (size_t)(cap + 1) * 4,
         (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
@@ -652,6 +652,7 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         d->proposal ? proposal_part_floats() * 4 : 0, d->pose_grad ? (size_t)cap * 6 * 4 : 0,
         d->pose_grad ? (size_t)R * 6 * 4 : 0,
         d->decoder_path != NEAT_DECODER_SIMT_FP32 ? (size_t)L.rec_cap * (8 + d->C) * 4 : 0};
+    static_assert(sizeof(sz) / sizeof(sz[0]) == StepLayout::NUM, "one size per workspace buffer");
     size_t o = 0;
     for (int i = 0; i < StepLayout::NUM; ++i)
     {
@@ -727,7 +728,7 @@ namespace neat
 struct StepBufs
 {
     float *origin, *direction;
-    int *ray_nseg, *ray_seg_off, *node_nseg, *node_cursor, *node_seg_off;
+    int *ray_nseg, *ray_seg_off, *node_nseg, *node_seg_off;
     SegRec *ray_hits, *segs;
     int *seg_n, *samp_off, *tile_seg;
     double* partial;
@@ -749,7 +750,6 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.ray_nseg     = (int*)P_(StepLayout::RAY_NSEG);
     w.ray_seg_off  = (int*)P_(StepLayout::RAY_SEG_OFF);
     w.node_nseg    = (int*)P_(StepLayout::NODE_NSEG);
-    w.node_cursor  = (int*)P_(StepLayout::NODE_CURSOR);
     w.node_seg_off = (int*)P_(StepLayout::NODE_SEG_OFF);
     w.ray_hits     = (SegRec*)P_(StepLayout::RAY_HITS);
     w.segs         = (SegRec*)P_(StepLayout::SEGS);
@@ -798,7 +798,6 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
     const int A = d->num_active, D = d->max_depth, M = d->max_samples_per_node;
     bool ok = true;
     ok      = ok && cudaMemsetAsync(w.node_nseg, 0, (size_t)A * 4, st) == cudaSuccess;
-    ok      = ok && cudaMemsetAsync(w.node_cursor, 0, (size_t)A * 4, st) == cudaSuccess;
     ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
     ok = ok && launch_step_rays(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation, d->translation,
                                 d->tree_table, D, M, L.cap_ray, w.origin, w.direction, w.ray_hits, w.ray_nseg,
@@ -806,8 +805,8 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
     ok = ok && scan_exclusive<int>(w.ray_nseg, nullptr, R, w.ray_seg_off, w.scratch, cnt + 0, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.node_nseg, nullptr, A, w.node_seg_off, w.scratch, nullptr, st) == cudaSuccess;
     k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, status);
-    ok = ok && launch_step_place(w.ray_hits, w.ray_nseg, w.ray_seg_off, R, L.cap_ray, w.node_seg_off, w.node_cursor,
-                                 w.segs, w.seg_n, cnt + 0, cap, st) == cudaSuccess;
+    ok = ok && launch_step_place(w.ray_hits, w.ray_nseg, w.ray_seg_off, R, L.cap_ray, w.node_seg_off, w.segs,
+                                 w.seg_n, cnt + 0, cap, st) == cudaSuccess;
     k_zero_partial<<<sm_count() * 4, 256, 0, st>>>(w.partial, cnt);
     ok = ok && scan_exclusive<int>(w.seg_n, cnt + 0, cap, w.samp_off, w.scratch, cnt + 1, st) == cudaSuccess;
     k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, status);

@@ -13,6 +13,8 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS   = 8;
 constexpr int SCAN_TILE    = SCAN_THREADS * SCAN_ITEMS;  // 2048 elements per block
 
+int sm_count();  // the device's SM count (neat_step.cu)
+
 template <typename T>
 __device__ __forceinline__ T block_exclusive_scan(T v, T* warp_tot, T& total)
 {
@@ -55,28 +57,32 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_blocks(const int* __restr
                                                                TO* __restrict__ block_sums)
 {
     __shared__ TO warp_tot[SCAN_THREADS / 32];
-    const int64_t n    = scan_count(n_dev, n_host);
-    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
-    if (base >= n) return;  // whole block idle: uniform exit
-    TO loc[SCAN_ITEMS];
-    TO sum = 0;
-#pragma unroll
-    for (int i = 0; i < SCAN_ITEMS; ++i)
+    const int64_t n = scan_count(n_dev, n_host);
+    // grid-stride over the 2048-element tiles (uniform per block); the grid is
+    // sized for the SMs, n_max only bounds it
+    for (int64_t b = blockIdx.x; b * SCAN_TILE < n; b += gridDim.x)
     {
-        int64_t idx = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
-        TO v        = (idx < n) ? (TO)in[idx] : (TO)0;
-        loc[i]      = sum;
-        sum += v;
-    }
-    TO total;
-    TO pre = block_exclusive_scan<TO>(sum, warp_tot, total);
+        const int64_t base = b * SCAN_TILE;
+        TO loc[SCAN_ITEMS];
+        TO sum = 0;
 #pragma unroll
-    for (int i = 0; i < SCAN_ITEMS; ++i)
-    {
-        int64_t idx = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
-        if (idx < n) out[idx] = pre + loc[i];
+        for (int i = 0; i < SCAN_ITEMS; ++i)
+        {
+            int64_t idx = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
+            TO v        = (idx < n) ? (TO)in[idx] : (TO)0;
+            loc[i]      = sum;
+            sum += v;
+        }
+        TO total;
+        TO pre = block_exclusive_scan<TO>(sum, warp_tot, total);  // ends with a barrier: warp_tot reusable
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; ++i)
+        {
+            int64_t idx = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
+            if (idx < n) out[idx] = pre + loc[i];
+        }
+        if (threadIdx.x == 0) block_sums[b] = total;
     }
-    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
 // One block: exclusive scan of the block sums in place; writes the grand
@@ -109,14 +115,16 @@ template <typename TO>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(TO* __restrict__ out, const int64_t* n_dev, int64_t n_host,
                                                             const TO* __restrict__ block_sums)
 {
-    const int64_t n    = scan_count(n_dev, n_host);
-    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
-    if (base >= n) return;
-    const TO add = block_sums[blockIdx.x];
-    for (int i = threadIdx.x; i < SCAN_TILE; i += SCAN_THREADS)
+    const int64_t n = scan_count(n_dev, n_host);
+    for (int64_t b = blockIdx.x; b * SCAN_TILE < n; b += gridDim.x)
     {
-        int64_t idx = base + i;
-        if (idx < n) out[idx] += add;
+        const int64_t base = b * SCAN_TILE;
+        const TO add       = block_sums[b];
+        for (int i = threadIdx.x; i < SCAN_TILE; i += SCAN_THREADS)
+        {
+            int64_t idx = base + i;
+            if (idx < n) out[idx] += add;
+        }
     }
 }
 
@@ -131,6 +139,7 @@ inline cudaError_t scan_exclusive(const int* in, const int64_t* n_dev, int64_t n
 {
     int64_t nb = (n_max + SCAN_TILE - 1) / SCAN_TILE;
     if (nb < 1) nb = 1;
+    nb = nb < (int64_t)sm_count() * 4 ? nb : (int64_t)sm_count() * 4;
     k_scan_blocks<TO><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n_dev, n_max, out, scratch);
     k_scan_sums<TO><<<1, 1024, 0, st>>>(scratch, n_dev, n_max, out, total64);
     k_scan_add<TO><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(out, n_dev, n_max, scratch);

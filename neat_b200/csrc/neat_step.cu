@@ -199,12 +199,16 @@ __global__ void k_zero_per_segment(float* __restrict__ p, const int64_t* counter
 __global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, const int64_t* counters,
                            int* __restrict__ tile_seg, int64_t tiles_cap)
 {
-    const int64_t i    = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nseg = counters[0];
-    if (i >= nseg || counters[1] == 0) return;
-    const int64_t o = samp_off[i], e = o + seg_n[i];
-    const int64_t t = (o + TT - 1) / TT;
-    if (t * TT < e && t < tiles_cap) tile_seg[t] = (int)i;
+    if (counters[1] == 0) return;
+    // grid-stride over the step's segments (the grid is sized for the SMs, not
+    // for the segment capacity, most of which a step leaves unused)
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t o = samp_off[i], e = o + seg_n[i];
+        const int64_t t = (o + TT - 1) / TT;
+        if (t * TT < e && t < tiles_cap) tile_seg[t] = (int)i;
+    }
 }
 
 // Photometric calibration of one ray's integral x (PhotometricCalibration::forward,
@@ -810,7 +814,8 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
     k_zero_partial<<<sm_count() * 4, 256, 0, st>>>(w.partial, cnt);
     ok = ok && scan_exclusive<int>(w.seg_n, cnt + 0, cap, w.samp_off, w.scratch, cnt + 1, st) == cudaSuccess;
     k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, status);
-    k_tile_seg<<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(w.samp_off, w.seg_n, cnt, w.tile_seg, L.tiles_cap);
+    k_tile_seg<<<(unsigned)std::min<int64_t>((cap + 255) / 256, (int64_t)sm_count() * 8), 256, 0, st>>>(
+        w.samp_off, w.seg_n, cnt, w.tile_seg, L.tiles_cap);
     return ok;
 }
 

@@ -46,13 +46,15 @@ PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 # x 3 kernels, segment clamp, placement, partial zeroing, sample clamp, tile
 # map, forward tiles, ray loss, loss total, backward tiles, decoder Adam, grid Adam
 STEP_LAUNCHES = 22
-# DRAM bytes per sample of the records backward (k_bwd_rec) from one ncu capture of
-# the same scene at 2^16 rays (dram__bytes_read.sum + dram__bytes_write.sum = 463.2 MB
-# for 2.908 M samples), scaled to a launch by its samples -- an upper bound at
-# larger batches (more grid reuse in L2)
-TRAFFIC_BYTES_PER_SAMPLE = {("full", "bf16x3"): 463.2e6 / 2.908e6,
-                            # k_bwd_rec<C=8, BF16>, same scene and case: 344.3 + 119.7 MB
-                            ("full", "bf16"): 464.0e6 / 2.908e6}
+# DRAM bytes per sample of the records backward (k_bwd_rec), dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch in a single-pass ncu capture, scaled to the
+# measured launch by its samples:
+TRAFFIC_BYTES_PER_SAMPLE = {
+    # BF16x3 at the full-size workload itself (2^18 rays, 11.64 M samples): 886.6 + 176.5 MB
+    ("full", "bf16x3"): (1063.1e6 / 11.6376e6, "ncu capture of a full-size launch (2^18 rays), per sample"),
+    # BF16, same scene at 2^16 rays (2.908 M samples): 344.3 + 119.7 MB -- an upper bound at
+    # larger batches, which reuse more of the grid gradient in L2
+    ("full", "bf16"): (464.0e6 / 2.908e6, "ncu capture at 2^16 rays scaled by samples (upper bound)")}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_bwd_rec<C=%d, BF16x3> (backward from the forward's records, MMA warp)",
                "bf16": "k_bwd_rec<C=%d, BF16> (backward from the forward's records, MMA warp)"}
@@ -734,9 +736,10 @@ def main():
         "phase_ms": phase_ms,
         "roofline": {"kernel": KERNEL_NAME[decoder] % cfg["C"], "bound": "tensor", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": (TRAFFIC_BYTES_PER_SAMPLE[traffic_key] * S
+                     "traffic": (TRAFFIC_BYTES_PER_SAMPLE[traffic_key][0] * S
                                  if traffic_key in TRAFFIC_BYTES_PER_SAMPLE else None),
-                     "traffic_source": "ncu capture at 2^16 rays scaled by samples (upper bound)",
+                     "traffic_source": (TRAFFIC_BYTES_PER_SAMPLE[traffic_key][1]
+                                        if traffic_key in TRAFFIC_BYTES_PER_SAMPLE else None),
                      "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                      "fp32_simt_peak_tflops": simt_peak,
                      "frac_of_fp32_simt": achieved / simt_peak},

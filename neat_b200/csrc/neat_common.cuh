@@ -73,8 +73,10 @@ static_assert(sizeof(NodeEntry) == 16, "NodeEntry must be 16 bytes");
 
 __device__ __forceinline__ float plane_coord(int k, int D)
 {
-    // exact: k * 2^(1-D) is a dyadic rational with < 24 significant bits
-    return __fadd_rn(__fmul_rn((float)k, __fdiv_rn(2.0f, (float)(1 << D))), -1.0f);
+    // exact: k * 2^(1-D) is a dyadic rational with < 24 significant bits.
+    // 2^(1-D) is built from its exponent field (128 - D; D <= 7 here), the
+    // value 2 / 2^D has exactly, without a division.
+    return __fadd_rn(__fmul_rn((float)k, __uint_as_float((uint32_t)(128 - D) << 23)), -1.0f);
 }
 
 // (box_max - box_min).norm() in float, evaluated a0 + (a1 + a2) (Eigen's

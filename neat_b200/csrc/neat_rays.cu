@@ -444,15 +444,23 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
     if (lane == 0)
     {
         ray_nseg[r] = k;
-        atomicMax((unsigned long long*)&counters[2], (unsigned long long)k);
+        // the step's largest hit count: every ray's atomic on one address would
+        // serialise at its L2 slice, so read first (a stale value only lets an
+        // atomic through; the maximum is monotone) and reduce only when k may
+        // raise it
+        if ((unsigned long long)k > *(volatile unsigned long long*)&counters[2])
+            atomicMax((unsigned long long*)&counters[2], (unsigned long long)k);
     }
 }
 
 // Place every ray's segments into its nodes' buckets: one thread per segment
 // (ray-major index rm < counters[0]), 256 consecutive segments per block; the
 // slot in the bucket is the rank the walk drew when it counted the segment.  The
-// ray of a segment is the last r with ray_seg_off[r] <= rm: thread 0 finds the
-// block's first ray in global memory, the block stages the next 257 ray
+// ray of a segment is the last r with ray_seg_off[r] <= rm: the block finds
+// its first ray by a 256-ary search in global memory (each round every thread
+// tests the lower end of one of 256 sub-ranges and __syncthreads_count picks
+// the last sub-range that starts at or before the block's first segment: three
+// rounds for 2^18 rays instead of 18 dependent loads), stages the next 257 ray
 // offsets in shared memory and each thread searches there (rays that miss the
 // volume own no segment, so a window can end before the block's last segment;
 // such a thread searches global memory from the window's end).
@@ -478,13 +486,21 @@ __global__ void __launch_bounds__(PLACE_T)
                  int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
 {
     __shared__ int soff[PLACE_T + 1];
-    __shared__ int64_t sr0;
     const int64_t nseg = *nseg_eff;  // 0 after a capacity overflow
     for (int64_t base = (int64_t)blockIdx.x * PLACE_T; base < nseg; base += (int64_t)gridDim.x * PLACE_T)
     {
-        if (threadIdx.x == 0) sr0 = last_le(ray_seg_off, 0, R, base);
-        __syncthreads();
-        const int64_t r0 = sr0;
+        // ray_seg_off[lo] <= base < ray_seg_off[hi] (ray_seg_off[R] = total > base);
+        // block-uniform bounds, the offsets are nondecreasing
+        int64_t lo = 0, hi = R;
+        while (hi - lo > 1)
+        {
+            const int64_t step = (hi - lo + PLACE_T - 1) / PLACE_T;
+            const int64_t c    = lo + (int64_t)threadIdx.x * step;
+            const int n        = __syncthreads_count(c < hi && ray_seg_off[c] <= base);  // >= 1: c = lo holds
+            lo                 = lo + (int64_t)(n - 1) * step;
+            hi                 = min(lo + step, hi);
+        }
+        const int64_t r0 = lo;
         for (int j = threadIdx.x; j <= PLACE_T; j += PLACE_T)
             soff[j] = (r0 + j <= R) ? ray_seg_off[r0 + j] : 0x7fffffff;
         __syncthreads();
@@ -519,7 +535,7 @@ __global__ void __launch_bounds__(PLACE_T)
                 seg_n[nm] = sg.n;
             }
         }
-        __syncthreads();  // soff and sr0 are rewritten by the next round
+        __syncthreads();  // soff is rewritten by the next round
     }
 }
 

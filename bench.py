@@ -113,41 +113,68 @@ def measured_peaks():
 # clocks
 # --------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons taken while the
+    timed region runs.  The sampler is started, and its first sample awaited,
+    before the region begins (nvidia-smi needs a few hundred ms to start); a
+    sample counts when it arrives between begin() and end() (plus one
+    interval).  If the region is shorter than an interval, the sample on each
+    side of it is reported instead, and `samples_in_region` says so."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 20
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.t_begin = self.t_end = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        t0 = time.monotonic()
+        while not self.lines and time.monotonic() - t0 < 10.0 and self.proc.poll() is None:
+            time.sleep(0.005)
+
+    def begin(self):
+        self.t_begin = time.monotonic()
+
+    def end(self):
+        self.t_end = time.monotonic()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+        time.sleep(3 * self.INTERVAL_MS / 1000.0)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        lines = list(self.lines)
+        tb = self.t_begin if self.t_begin is not None else -1e30
+        te = (self.t_end if self.t_end is not None else 1e30) + self.INTERVAL_MS / 1000.0
+        inside = [ln for t, ln in lines if tb <= t <= te]
+        n_inside = len(inside)
+        if not inside:
+            before = [ln for t, ln in lines if t < tb][-1:]
+            after = [ln for t, ln in lines if t > te][:1]
+            inside = before + after
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -160,7 +187,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_in_region": n_inside, "interval_ms": self.INTERVAL_MS}
 
 
 # --------------------------------------------------------------------------
@@ -636,7 +663,9 @@ def main():
     barrier()
     torch.cuda.synchronize()
     clocks.start()
+    clocks.begin()
     ms, phase_ms, counts = time_steps(tr, batches[W:])
+    clocks.end()
     clock_info = clocks.stop()
     barrier()
     ms = max_over_ranks(ms)

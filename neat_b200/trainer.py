@@ -79,6 +79,7 @@ class FusedTrainer:
             decoder_grad=self.decoder_grad.data_ptr(), step_counter=self.step_counter.data_ptr())
         self.ws = None
         self.ws_rays = 0
+        self._stage = None  # device staging of host batches (see _stage_host)
         self.step_id = 0
         self._graph = None
         self._graphs = {}
@@ -167,11 +168,56 @@ class FusedTrainer:
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
         self.ws_rays = int(num_rays)
 
+    def _stage_host(self, uv, image_id, target):
+        """A host batch (the reference's Dataloader hands the step host tensors,
+        src/utils/Dataloader.cpp:8-49) into device staging buffers.  Two buffer
+        sets alternate.  A set's copy runs on a copy stream once the step that
+        last read the set has finished (an event), and the step waits for its
+        own copy (another event), so the copy of the next batch overlaps this
+        step's kernels when the caller queues steps ahead.  Pinned host memory
+        makes the copies asynchronous; pageable memory is copied by CUDA
+        synchronously.  Returns the device views and the set index."""
+        R = uv.shape[0]
+        if uv.dtype != torch.float32 or image_id.dtype != torch.int32 or target.dtype != torch.float32:
+            raise TypeError("host batches: uv float32 [R, 2], image_id int32 [R], target float32 [R]")
+        if tuple(uv.shape) != (R, 2) or tuple(image_id.shape) != (R,) or tuple(target.shape) != (R,):
+            raise ValueError("host batches: uv [R, 2], image_id [R], target [R]")
+        if self._stage is None or self._stage["rays"] < R:
+            dev = self.dev
+            self._stage = {"rays": R, "next": 0, "stream": torch.cuda.Stream(dev), "used": [None, None],
+                           "bufs": [(torch.empty((R, 2), dtype=torch.float32, device=dev),
+                                     torch.empty(R, dtype=torch.int32, device=dev),
+                                     torch.empty(R, dtype=torch.float32, device=dev)) for _ in range(2)]}
+        st = self._stage
+        b = st["next"]
+        st["next"] = b ^ 1
+        cs, cur = st["stream"], torch.cuda.current_stream(self.dev)
+        if st["used"][b] is not None:
+            cs.wait_event(st["used"][b])
+        d_uv, d_img, d_tgt = (t[:R] for t in st["bufs"][b])
+        with torch.cuda.stream(cs):
+            d_uv.copy_(uv.contiguous(), non_blocking=True)
+            d_img.copy_(image_id.contiguous(), non_blocking=True)
+            d_tgt.copy_(target.contiguous(), non_blocking=True)
+        ready = torch.cuda.Event()
+        ready.record(cs)
+        cur.wait_event(ready)
+        return d_uv, d_img, d_tgt, b
+
+    def host_copy_stream(self):
+        """The stream that copies host batches in (None before the first one)."""
+        return None if self._stage is None else self._stage["stream"]
+
     def step(self, uv, image_id, target, prediction=None, phase_events=None):
         """One fused forward+backward+Adam step on a ray batch; returns the
         device loss tensor (mean squared projection error of the batch).
+        The batch may be device tensors or host tensors (pinned for an
+        asynchronous copy that overlaps the previous step: _stage_host).
         phase_events: optional list of NEAT_STEP_PHASES torch.cuda.Event
         (enable_timing) recorded at the step's phase boundaries."""
+        staged = None
+        if not uv.is_cuda:
+            uv, image_id, target, staged = self._stage_host(uv, image_id, target)
         R = uv.shape[0]
         self.reserve(R)
         self.step_id += 1
@@ -200,6 +246,10 @@ class FusedTrainer:
                                       self.seed, self.step_id, ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
                                       self._stream())
         _lib.check(rc, "neat_train_step")
+        if staged is not None:
+            done = torch.cuda.Event()
+            done.record(torch.cuda.current_stream(self.dev))
+            self._stage["used"][staged] = done  # the set's next copy waits for this step
         if self.optimize_pose or self.optimize_intrinsics:
             self.pose_step()
         return self.loss

@@ -917,6 +917,39 @@ def test_checkpoint_resume_reproduces_the_next_step(neat, case, proposal):
         b.load_state_dict(sd2)
 
 
+def test_host_batches_are_staged_like_device_batches(neat, case):
+    """FusedTrainer.step on pinned host batches (staged through the trainer's
+    copy stream into two alternating device buffer sets, each copy overlapping
+    the previous step) takes the same steps as on device batches: four steps
+    queued without a synchronisation, each on another batch, so a set is
+    rewritten while the other set's step runs.  Same losses (the forward is
+    deterministic; the parameters differ only by the grid-gradient atomics'
+    order) and the same parameters up to that order."""
+    from neat_b200.trainer import FusedTrainer
+    def make():
+        return FusedTrainer(case.tree, _camera(case), case.C, case.G, case.M, lr_grid=1e-2, lr_decoder=5e-5, seed=7,
+                            grid=torch.from_numpy(case.grid), decoder=torch.from_numpy(case.dec))
+    n = case.R // 4
+    parts = [(case.uv[k * n:(k + 1) * n], case.img[k * n:(k + 1) * n], case.target[k * n:(k + 1) * n])
+             for k in range(4)]
+    a, b = make(), make()
+    la = [a.step(_dev(u), _dev(i), _dev(t)).clone() for u, i, t in parts]
+    host = [tuple(torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in p) for p in parts]
+    lb = [b.step(u, i, t).clone() for u, i, t in host]
+    torch.cuda.synchronize()
+    a.check_status()
+    b.check_status()
+    assert b.host_copy_stream() is not None and a.host_copy_stream() is None
+    for x, y in zip(la, lb):
+        assert float(y) == pytest.approx(float(x), rel=1e-5)
+    def moved(x, y):
+        return float(((x - y).abs() > 1e-6).float().mean())
+    assert moved(b.decoder, a.decoder) < 1e-2
+    assert moved(b.grid, a.grid) < 1e-3
+    with pytest.raises(TypeError):
+        b.step(host[0][0].double(), host[0][1], host[0][2])
+
+
 def test_checkpoint_after_restructure_restores_the_saved_tree(neat, case):
     """A checkpoint taken after restructure() holds the new active-node set; a
     trainer built on the original tree moves to that set before copying the

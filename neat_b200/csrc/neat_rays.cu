@@ -376,26 +376,26 @@ __global__ void __launch_bounds__(32 * RAY_WARPS)
 // Fused step: one traversal per ray (canonical hit list kept per ray), then
 // the lists are placed node-major.
 // ---------------------------------------------------------------------------
+// The rays come from k_make_rays, one thread per ray, launched just before:
+// the f64 camera model (five divisions and a square root) would otherwise run
+// on all 32 lanes of the ray's warp alike.
 template <class WH>
 __global__ void __launch_bounds__(32 * RAY_WARPS)
-    k_step_rays(const float* __restrict__ uv, const int32_t* __restrict__ image_id, int64_t R, int w, int h,
-                const double* __restrict__ intr, const double* __restrict__ rot, const double* __restrict__ trans,
-                const NodeEntry* __restrict__ table, int D, int M, int cap_ray, float* __restrict__ origin,
-                float* __restrict__ direction, SegRec* __restrict__ ray_hits, int* __restrict__ ray_nseg,
-                int* __restrict__ node_nseg, int64_t* counters, int* status)
+    k_step_rays(int64_t R, const NodeEntry* __restrict__ table, int D, int M, int cap_ray,
+                const float* __restrict__ origin, const float* __restrict__ direction, SegRec* __restrict__ ray_hits,
+                int* __restrict__ ray_nseg, int* __restrict__ node_nseg, int64_t* counters, int* status)
 {
     constexpr int kMaxHits = WH::kHits;
     __shared__ WH sh[RAY_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t r = (int64_t)blockIdx.x * RAY_WARPS + warp;
     if (r >= R) return;
-    const int img = image_id[r];
     float o[3], d[3];
-    make_ray(uv[2 * r], uv[2 * r + 1], w, h, intr, rot + 4 * img, trans + 3 * img, o, d);
-    if (lane < 3)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
     {
-        origin[3 * r + lane]    = o[lane];
-        direction[3 * r + lane] = d[lane];
+        o[c] = origin[3 * r + c];
+        d[c] = direction[3 * r + c];
     }
     WH& ws   = sh[warp];
     bool ovf = false;
@@ -545,22 +545,19 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
                              int64_t* counters, int* status, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
+    k_make_rays<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(uv, image_id, nullptr, R, w, h, intr, rot, trans, origin,
+                                                            direction);
     const unsigned grid = (unsigned)((R + RAY_WARPS - 1) / RAY_WARPS);
+    const NodeEntry* tab = (const NodeEntry*)table;
     if (cap_ray <= WarpHitsStep::kHits && D <= WarpHitsStep::kDepth)
-        k_step_rays<WarpHitsStep><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
-                                                                   (const NodeEntry*)table, D, M, cap_ray, origin,
-                                                                   direction, ray_hits, ray_nseg, node_nseg, counters,
-                                                                   status);
+        k_step_rays<WarpHitsStep><<<grid, 32 * RAY_WARPS, 0, st>>>(R, tab, D, M, cap_ray, origin, direction, ray_hits,
+                                                                   ray_nseg, node_nseg, counters, status);
     else if (cap_ray <= WarpHitsStep96::kHits && D <= WarpHitsStep96::kDepth)
-        k_step_rays<WarpHitsStep96><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
-                                                                     (const NodeEntry*)table, D, M, cap_ray, origin,
-                                                                     direction, ray_hits, ray_nseg, node_nseg,
-                                                                     counters, status);
+        k_step_rays<WarpHitsStep96><<<grid, 32 * RAY_WARPS, 0, st>>>(R, tab, D, M, cap_ray, origin, direction,
+                                                                     ray_hits, ray_nseg, node_nseg, counters, status);
     else
-        k_step_rays<WarpHits><<<grid, 32 * RAY_WARPS, 0, st>>>(uv, image_id, R, w, h, intr, rot, trans,
-                                                               (const NodeEntry*)table, D, M, cap_ray, origin,
-                                                               direction, ray_hits, ray_nseg, node_nseg, counters,
-                                                               status);
+        k_step_rays<WarpHits><<<grid, 32 * RAY_WARPS, 0, st>>>(R, tab, D, M, cap_ray, origin, direction, ray_hits,
+                                                               ray_nseg, node_nseg, counters, status);
     return cudaGetLastError();
 }
 

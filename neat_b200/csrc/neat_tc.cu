@@ -269,6 +269,64 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
         return o;
     };
     auto stage_b = [&](int64_t tl, int b, int lo) -> Slot { return gather_b(place_b(tl, b, lo)); };
+    // Forward, two threads per sample (K::STG): the corner rows of a sample
+    // placed a tile ahead are copied into shared memory by cp.async when the
+    // tile before it starts, and gathered from there after its h1 epilogue --
+    // the L2 round trip runs under the epilogue.  Each thread stages and reads
+    // only its own sample's slots, so its own cp.async.wait_all orders them.
+    // Same products in the same order as gather_cl: the same features.
+    const bool use_stg = K::STG && a.grid_bf16 == nullptr;
+    float4* stg        = reinterpret_cast<float4*>(sm + K::OFF_STG);
+    auto stage_corners = [&](const Place& pl) {
+        if constexpr (K::STG)
+        {
+            Corners kc;
+            igs_corners(pl.q.lu, pl.q.lv, pl.q.lw, a.G, a.G, a.G, kc);
+            const int64_t base = (int64_t)pl.q.row * a.G * a.G * a.G;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const float* src = a.grid + (base + corner_cell(kc, q, a.G, a.G)) * C;
+#pragma unroll
+                for (int c4 = 0; c4 < C / 4; ++c4) cp_async16(smem_u32(stg + (q * (C / 4) + c4) * 128 + s), src + 4 * c4);
+            }
+            cp_async_commit();
+        }
+    };
+    auto gather_staged = [&](const Place& pl) -> Slot {
+        Slot o;
+        o.q   = pl.q;
+        o.seg = pl.seg;
+        o.dvw = 0.0f;
+        if constexpr (K::STG)
+        {
+            Corners kc;
+            igs_corners(o.q.lu, o.q.lv, o.q.lw, a.G, a.G, a.G, kc);
+            cp_async_wait_all();
+#pragma unroll
+            for (int c4 = 0; c4 < C / 4; ++c4)
+            {
+                float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                {
+                    const float4 v = stg[(q * (C / 4) + c4) * 128 + s];
+                    a0             = fmaf(v.x, kc.w[q], a0);
+                    a1             = fmaf(v.y, kc.w[q], a1);
+                    a2             = fmaf(v.z, kc.w[q], a2);
+                    a3             = fmaf(v.w, kc.w[q], a3);
+                }
+                o.x[4 * c4]     = a0;
+                o.x[4 * c4 + 1] = a1;
+                o.x[4 * c4 + 2] = a2;
+                o.x[4 * c4 + 3] = a3;
+            }
+            if (!o.q.valid)
+#pragma unroll
+                for (int c = 0; c < C; ++c) o.x[c] = 0.0f;
+        }
+        return o;
+    };
     // placement records in shared memory (slot s), see K::OFF_P
     float* prec = reinterpret_cast<float*>(sm + K::OFF_P);
     auto store_p = [&](const Place& pl) {
@@ -565,6 +623,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             // segment starts of the tile after next (stored before the barrier
             // ahead of its placement) and the tile_seg of the one after that
             int oa2 = INT_MAX, ob2 = INT_MAX;
+            // the next tile's corner rows into shared memory, under this tile's h1 epilogue
+            if (use_stg && has_next && h == 0) stage_corners(pl_next);
             if (has_next2) fetch_starts(lo_n2, oa2, ob2);
             const int lo_n3 = nxt2 + G < ntiles ? a.tile_seg[nxt2 + G] : 0;
             ok = wait_own(mbar_wg, phase_wg) && ok;
@@ -622,7 +682,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
             {
                 if (h == 0)
                 {
-                    const Slot nx = gather_b(pl_next);
+                    const Slot nx = use_stg ? gather_staged(pl_next) : gather_b(pl_next);
                     put_x1(nx.x, 0);
                     put_sr(nx, buf ^ 1);
                     write_rec(nx, nxt);

@@ -117,7 +117,13 @@ struct CfgPlan
     static constexpr int OFF_P  = OFF_Q + NQ * 4;
     static constexpr int OFF_R  = OFF_P + NP * 4;
     static constexpr int NRED   = BWD ? 8 * HH : 0;
-    static constexpr int OFF_M  = ((OFF_R + NRED * 4) + 15) / 16 * 16;
+    // forward with two threads per sample, C <= 8: the next tile's corner rows,
+    // staged by cp.async while the current tile's h1 epilogue runs
+    // ([8 corners][C / 4][128 samples] float4)
+    static constexpr bool STG    = !BWD && NH == 2 && C <= 8 && C % 4 == 0;
+    static constexpr int NSTG    = STG ? 8 * C * 128 : 0;  // floats
+    static constexpr int OFF_STG = ((OFF_R + NRED * 4) + 15) / 16 * 16;
+    static constexpr int OFF_M   = OFF_STG + NSTG * 4;
     static constexpr int NEED   = OFF_M + 32;                 // mbarriers at +0, +8, +24; TMEM slot at +16
 };
 
@@ -258,6 +264,14 @@ __device__ __forceinline__ void gemm_cat(uint32_t d, uint64_t da, uint64_t db, b
             mma<1>(d, a, b, make_idesc(Prec<PREC>::FMT, A_MN, B_MN, 128, (NP - p) * NB), (acc0 || p || kk) ? 1u : 0u);
         }
 }
+
+// cp.async (16 bytes, global -> shared, through L1); a thread waits for its own copies
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }

@@ -62,6 +62,7 @@ PSNR_TARGET_DB = 40.0
 
 
 PROPOSAL_ITERS = 10  # proposal Adam iterations on a TRAIN step (FusedTrainer default)
+PREFETCH = True      # timed steps build the next batch's segment lists under their Adam (--no-prefetch: off)
 
 
 def step_launches(decoder, C, proposal, train):
@@ -337,7 +338,9 @@ def time_steps(tr, batches, phase_events=True):
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
     for i, b in enumerate(batches):
-        tr.step(*b, phase_events=ev[i] if ev else None)
+        # the next batch's segment lists build under this step's Adam update
+        nxt = batches[i + 1] if PREFETCH and i + 1 < K else None
+        tr.step(*b, phase_events=ev[i] if ev else None, next=nxt)
         counts[i].copy_(tr.counters, non_blocking=True)
     t1.record()
     torch.cuda.synchronize()
@@ -581,6 +584,8 @@ def main():
     ap.add_argument("--no-psnr", action="store_true", help="skip the small workload's time-to-PSNR leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / BF16 / BF16+proposal step variants")
     ap.add_argument("--no-large", action="store_true", help="skip the large porous workload's sub-line")
+    ap.add_argument("--no-prefetch", action="store_true",
+                    help="build every step's segment lists inside the step (no look-ahead under Adam)")
     ap.add_argument("--no-ref-igs", action="store_true",
                     help="skip timing the reference's GPU IGS kernels beside this library's")
     ap.add_argument("--volume-psnr", type=int, default=5000,
@@ -591,6 +596,8 @@ def main():
                     help="decoder GEMM path: FP32 SIMT, tcgen05 FP32-accurate 3-piece BF16 split, tcgen05 BF16 "
                          "(default: bf16x3; bf16 for the large workload)")
     args = ap.parse_args()
+    global PREFETCH
+    PREFETCH = not args.no_prefetch
     if args.warmup < 3:
         args.warmup = 3
     cfg = dict(WORKLOADS[args.workload])
@@ -652,9 +659,12 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- warm-up (device-resident batches; with the proposal it includes the first TRAIN step)
+    # ---- warm-up (device-resident batches; with the proposal it includes the first TRAIN step).
+    # It exercises the look-ahead between warm-up batches (the process's first
+    # side-stream build carries a one-time start-up cost); the last warm-up step
+    # does not build the first timed batch's lists, which stay inside the timed region.
     for i in range(W):
-        tr.step(*batches[i])
+        tr.step(*batches[i], next=batches[i + 1] if PREFETCH and i + 1 < W else None)
     torch.cuda.synchronize()
     tr.check_status()
 
@@ -691,7 +701,7 @@ def main():
     e0.record()
     tr.host_copy_stream().wait_event(e0)
     for i in range(K):
-        loss = tr.step(*hb[i])
+        loss = tr.step(*hb[i], next=hb[i + 1] if PREFETCH and i + 1 < K else None)
         loss_host[i:i + 1].copy_(loss, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()

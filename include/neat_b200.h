@@ -410,6 +410,30 @@ int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, co
                     neat_stream_t stream);
 
 /* ----------------------------------------------------------------------- */
+/* Pipelined steps (optional): the next batch's segment lists built while   */
+/* the running step's Adam update runs.  The lists depend on the batch and */
+/* the octree only, not on any parameter, so the training loop of          */
+/* samples/reconstruct.cpp (TrainStep over Dataloader batches) may build   */
+/* them one step ahead.                                                     */
+/* neat_train_step_segments runs phase [1] of a step (rays, hit lists,      */
+/* node-major segments, sample offsets, tile map) for `batch` into          */
+/* `workspace` (neat_train_step_workspace_bytes bytes) and `counters` /     */
+/* `status` (as neat_step_out).  neat_train_step_prebuilt is               */
+/* neat_train_step for that batch without phase [1]: same arguments, with  */
+/* out->counters = the counters neat_train_step_segments filled.            */
+/* A step reads the segment buffers up to its phase [4] (backward done),    */
+/* or up to [5] when it trains the learned proposal: queue                  */
+/* neat_train_step_segments on a second stream behind that phase event of  */
+/* the running step (its counters must be another array than the running   */
+/* step's), and the prebuilt step behind the segments' completion.         */
+/* ----------------------------------------------------------------------- */
+int neat_train_step_segments(const neat_step_desc* desc, const neat_step_batch* batch, int64_t* counters,
+                             int* status, void* workspace, size_t workspace_bytes, neat_stream_t stream);
+int neat_train_step_prebuilt(const neat_step_desc* desc, const neat_step_state* state, const neat_step_batch* batch,
+                             uint64_t seed, int step, const neat_step_out* out, void* workspace,
+                             size_t workspace_bytes, neat_stream_t stream);
+
+/* ----------------------------------------------------------------------- */
 /* Projection (evaluation).                                                  */
 /* Replaces the per-batch forward of EvalStepProjection                     */
 /* (samples/reconstruct.cpp:551-583): GetRays -> CreateSamplesForRays with   */

@@ -943,9 +943,11 @@ static bool proposal_mode(const neat_step_desc* d, const neat_proposal* pr, int&
 
 }  // namespace neat
 
-extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
-                               uint64_t seed, int step, const neat_step_out* out, void* workspace,
-                               size_t workspace_bytes, neat_stream_t stream)
+// One training step; `prebuilt`: the segment lists of this batch are already
+// in the workspace and out->counters (neat_train_step_segments).
+static int train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b, uint64_t seed,
+                      int step, const neat_step_out* out, void* workspace, size_t workspace_bytes,
+                      neat_stream_t stream, bool prebuilt)
 {
     if (!d || !s || !b || !out || !out->loss || !out->counters || (!s->step_counter && step < 1))
         return NEAT_ERR_BAD_INPUT;
@@ -981,7 +983,7 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     phase(0);
     k_step_begin<<<1, 32, 0, st>>>(s->step_counter, step, (double)d->lr_grid, (double)d->lr_decoder,
                                    (double)d->beta1, (double)d->beta2, w.scal);
-    ok = build_segments(d, b, L, w, cnt, out->status, st);
+    if (!prebuilt) ok = build_segments(d, b, L, w, cnt, out->status, st);
     phase(1);
 
     StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
@@ -1035,7 +1037,9 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
                                                         s->decoder_m, s->decoder_v, d->beta1, d->beta2, d->eps,
                                                         w.scal);
     const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;
-    const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 8);
+    // four CTAs per SM (of eight) keep HBM busy and leave room for the next
+    // batch's segment build, queued on another stream behind phase [4]
+    const int agrid     = (int)std::min<int64_t>((ngrid / 4 + 255) / 256 + 1, (int64_t)sm_count() * 4);
     k_adam<<<agrid, 256, 0, st>>>(s->grid, s->grid_grad, s->grid_m, s->grid_v, ngrid, d->beta1, d->beta2, d->eps,
                                   0.0f, 1.0f, 1, w.scal, s->grid_bf16);
     if (s->tonemap)
@@ -1052,6 +1056,33 @@ extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s
     phase(5);
     ok = ok && cudaGetLastError() == cudaSuccess;
     return ok ? NEAT_OK : NEAT_ERR_CUDA;
+}
+
+extern "C" int neat_train_step(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
+                               uint64_t seed, int step, const neat_step_out* out, void* workspace,
+                               size_t workspace_bytes, neat_stream_t stream)
+{
+    return train_step(d, s, b, seed, step, out, workspace, workspace_bytes, stream, false);
+}
+
+extern "C" int neat_train_step_prebuilt(const neat_step_desc* d, const neat_step_state* s, const neat_step_batch* b,
+                                        uint64_t seed, int step, const neat_step_out* out, void* workspace,
+                                        size_t workspace_bytes, neat_stream_t stream)
+{
+    return train_step(d, s, b, seed, step, out, workspace, workspace_bytes, stream, true);
+}
+
+extern "C" int neat_train_step_segments(const neat_step_desc* d, const neat_step_batch* b, int64_t* counters,
+                                        int* status, void* workspace, size_t workspace_bytes, neat_stream_t stream)
+{
+    if (!d || !b || !counters || !status || !workspace) return NEAT_ERR_BAD_INPUT;
+    const int chk = check_desc(d, b);
+    if (chk != NEAT_OK) return chk;
+    StepLayout L;
+    if (!step_layout(d, b->num_rays, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
+    const StepBufs w = step_bufs(L, workspace);
+    const bool ok    = build_segments(d, b, L, w, counters, status, (cudaStream_t)stream);
+    return ok && cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 
 extern "C" int neat_project(const neat_step_desc* d, const float* grid, const float* decoder,

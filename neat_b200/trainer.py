@@ -80,6 +80,9 @@ class FusedTrainer:
         self.ws = None
         self.ws_rays = 0
         self._stage = None  # device staging of host batches (see _stage_host)
+        self._pf = None     # the next batch's segment lists, built ahead (see step)
+        self._cnt = [self.counters, torch.zeros_like(self.counters)]
+        self._ci = 0
         self.step_id = 0
         self._graph = None
         self._graphs = {}
@@ -159,6 +162,7 @@ class FusedTrainer:
         """Allocate the step workspace for batches of up to num_rays rays."""
         if self.ws is not None and num_rays <= self.ws_rays:
             return
+        self._drain_prefetch()
         self.desc.seg_capacity = int(num_rays) * self.seg_per_ray
         if self.proposal:
             self.desc_budget.seg_capacity = self.desc.seg_capacity
@@ -176,7 +180,8 @@ class FusedTrainer:
         own copy (another event), so the copy of the next batch overlaps this
         step's kernels when the caller queues steps ahead.  Pinned host memory
         makes the copies asynchronous; pageable memory is copied by CUDA
-        synchronously.  Returns the device views and the set index."""
+        synchronously.  Returns the device views, the set index and the event
+        that marks the copies done (the caller's stream waits on it)."""
         R = uv.shape[0]
         if uv.dtype != torch.float32 or image_id.dtype != torch.int32 or target.dtype != torch.float32:
             raise TypeError("host batches: uv float32 [R, 2], image_id int32 [R], target float32 [R]")
@@ -201,34 +206,71 @@ class FusedTrainer:
             d_tgt.copy_(target.contiguous(), non_blocking=True)
         ready = torch.cuda.Event()
         ready.record(cs)
-        cur.wait_event(ready)
-        return d_uv, d_img, d_tgt, b
+        return d_uv, d_img, d_tgt, b, ready
 
     def host_copy_stream(self):
         """The stream that copies host batches in (None before the first one)."""
         return None if self._stage is None else self._stage["stream"]
 
-    def step(self, uv, image_id, target, prediction=None, phase_events=None):
+    def step(self, uv, image_id, target, prediction=None, phase_events=None, next=None):
         """One fused forward+backward+Adam step on a ray batch; returns the
         device loss tensor (mean squared projection error of the batch).
         The batch may be device tensors or host tensors (pinned for an
         asynchronous copy that overlaps the previous step: _stage_host).
         phase_events: optional list of NEAT_STEP_PHASES torch.cuda.Event
-        (enable_timing) recorded at the step's phase boundaries."""
+        (enable_timing) recorded at the step's phase boundaries.
+        next: optional (uv, image_id, target) of the batch that the following
+        call takes.  Its segment lists (rays, hit lists, node-major segments,
+        tile map: they depend on the batch and the octree only) are then built
+        on a side stream while this step's Adam update runs
+        (neat_train_step_segments, queued behind the step's phase [4], or [5]
+        on a proposal TRAIN step), and that call skips building them
+        (neat_train_step_prebuilt).  Ignored while poses or intrinsics are
+        optimised (the pose update after the step moves the next rays)."""
+        cur = torch.cuda.current_stream(self.dev)
+        pf, self._pf = self._pf, None
         staged = None
         if not uv.is_cuda:
-            uv, image_id, target, staged = self._stage_host(uv, image_id, target)
+            key = (uv.data_ptr(), image_id.data_ptr(), target.data_ptr(), uv.shape[0])
+            if pf is not None and pf["host_key"] == key:
+                uv, image_id, target = pf["dev"]
+                staged = pf["set"]
+            else:
+                uv, image_id, target, staged, ready = self._stage_host(uv, image_id, target)
+                cur.wait_event(ready)
+        if pf is not None:
+            # the workspace's segment buffers and the staged batch, before anything
+            # (a reserve() below included) touches them
+            cur.wait_event(pf["done"])
         R = uv.shape[0]
         self.reserve(R)
         self.step_id += 1
+        train = self.proposal and (self.step_id - 1) % self.prop_every == 0
+        prebuilt = (pf is not None and pf["key"] == (uv.data_ptr(), image_id.data_ptr(), R)
+                    and pf["train"] == train)
+        if prebuilt:
+            self._ci = pf["ci"]
+        self.counters = self._cnt[self._ci]
         batch = _lib.StepBatch(uv=uv.data_ptr(), image_id=image_id.data_ptr(), target=target.data_ptr(), num_rays=R)
-        ev = None
+        prefetch = next is not None and not (self.optimize_pose or self.optimize_intrinsics)
+        handles = [None] * _lib.NEAT_STEP_PHASES
         if phase_events is not None:
             if len(phase_events) != _lib.NEAT_STEP_PHASES:
                 raise ValueError("phase_events needs NEAT_STEP_PHASES events")
             handles = [e.cuda_event for e in phase_events]
             if not all(handles):
                 raise ValueError("phase_events must be created (record them once) before use")
+        free_phase = 5 if train else 4  # the step's last read of its segment buffers
+        free_ev = None
+        if prefetch:
+            if phase_events is not None:
+                free_ev = phase_events[free_phase]
+            else:
+                free_ev = torch.cuda.Event()
+                free_ev.record(cur)  # creates the handle; recorded again by the step
+                handles[free_phase] = free_ev.cuda_event
+        ev = None
+        if any(h is not None for h in handles):
             self._ev_arr = (ctypes.c_void_p * _lib.NEAT_STEP_PHASES)(*handles)
             ev = ctypes.cast(self._ev_arr, ctypes.c_void_p)
         out = _lib.StepOut(loss=self.loss.data_ptr(), counters=self.counters.data_ptr(),
@@ -237,22 +279,68 @@ class FusedTrainer:
                            phase_events=ev)
         if self.loss_tv > 0 or self.loss_edge > 0:
             self.regularize()
-        desc = self.desc
-        if self.proposal:
-            train = (self.step_id - 1) % self.prop_every == 0
-            self.prop_struct.mode = _lib.NEAT_PROPOSAL_TRAIN if train else _lib.NEAT_PROPOSAL_SAMPLE
-            desc = self.desc if train else self.desc_budget
-        rc = self.lib.neat_train_step(ctypes.byref(desc), ctypes.byref(self.state), ctypes.byref(batch),
-                                      self.seed, self.step_id, ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
-                                      self._stream())
-        _lib.check(rc, "neat_train_step")
+        desc = self._step_desc(self.step_id)
+        fn = self.lib.neat_train_step_prebuilt if prebuilt else self.lib.neat_train_step
+        rc = fn(ctypes.byref(desc), ctypes.byref(self.state), ctypes.byref(batch), self.seed, self.step_id,
+                ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(), self._stream())
+        _lib.check(rc, "neat_train_step_prebuilt" if prebuilt else "neat_train_step")
         if staged is not None:
             done = torch.cuda.Event()
-            done.record(torch.cuda.current_stream(self.dev))
+            done.record(cur)
             self._stage["used"][staged] = done  # the set's next copy waits for this step
         if self.optimize_pose or self.optimize_intrinsics:
             self.pose_step()
+        if prefetch:
+            self._prefetch(next, free_ev)
         return self.loss
+
+    def _drain_prefetch(self):
+        """Order a pending look-ahead segment build before whatever follows on
+        the current stream (before the workspace is freed or replaced), and
+        drop it: the next step builds its own lists."""
+        if self._pf is not None:
+            torch.cuda.current_stream(self.dev).wait_event(self._pf["done"])
+            self._pf = None
+
+    def _step_desc(self, step_id):
+        """The step descriptor of step number step_id (with the learned
+        proposal: uniform TRAIN steps and budget SAMPLE steps)."""
+        if not self.proposal:
+            return self.desc
+        train = (step_id - 1) % self.prop_every == 0
+        self.prop_struct.mode = _lib.NEAT_PROPOSAL_TRAIN if train else _lib.NEAT_PROPOSAL_SAMPLE
+        return self.desc if train else self.desc_budget
+
+    def _prefetch(self, nxt, free_ev):
+        """The segment lists of the next step's batch nxt on a side stream,
+        behind free_ev (the running step's last read of its segment buffers),
+        into the workspace and the other counters array (see step)."""
+        uv, image_id, target = nxt
+        R = uv.shape[0]
+        if R > self.ws_rays:
+            return  # the next step re-reserves and builds its own lists
+        if getattr(self, "_pf_stream", None) is None:
+            self._pf_stream = torch.cuda.Stream(self.dev)
+        ps = self._pf_stream
+        host_key, set_idx = None, None
+        if not uv.is_cuda:
+            host_key = (uv.data_ptr(), image_id.data_ptr(), target.data_ptr(), R)
+            uv, image_id, target, set_idx, ready = self._stage_host(uv, image_id, target)
+            ps.wait_event(ready)
+        ps.wait_event(free_ev)
+        step_id = self.step_id + 1
+        train = self.proposal and (step_id - 1) % self.prop_every == 0
+        desc = self.desc if (not self.proposal or train) else self.desc_budget
+        ci = self._ci ^ 1
+        batch = _lib.StepBatch(uv=uv.data_ptr(), image_id=image_id.data_ptr(), target=target.data_ptr(), num_rays=R)
+        rc = self.lib.neat_train_step_segments(ctypes.byref(desc), ctypes.byref(batch), self._cnt[ci].data_ptr(),
+                                               self.status.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+                                               ps.cuda_stream)
+        _lib.check(rc, "neat_train_step_segments")
+        done = torch.cuda.Event()
+        done.record(ps)
+        self._pf = {"key": (uv.data_ptr(), image_id.data_ptr(), R), "host_key": host_key,
+                    "dev": (uv, image_id, target), "set": set_idx, "done": done, "ci": ci, "train": train}
 
     def pose_step(self):
         """The reference's structure optimizer step on the accumulated pose
@@ -287,6 +375,7 @@ class FusedTrainer:
         runs the step eagerly and captures it; later calls copy the batch into
         the captured input buffers and replay (one graph launch instead of the
         step's ~20 kernel launches).  Same results as step()."""
+        self._drain_prefetch()
         R = uv.shape[0]
         train = self.proposal and self.step_id % self.prop_every == 0
         key = (R, train)
@@ -324,6 +413,7 @@ class FusedTrainer:
         calibration applied when it has one (tone_mapper->forward, :559).
         error_sums: optional device f64[2] that receives += sum (pred-target)^2
         and += sum |pred-target|."""
+        self._drain_prefetch()  # this call rewrites the workspace's segment buffers
         R = uv.shape[0]
         self.reserve(R)
         if prediction is None:
@@ -442,6 +532,7 @@ class FusedTrainer:
         if self.proposal:
             self.prop_node_desc = torch.zeros((A, 6), dtype=torch.float32, device=self.dev)
             self.prop_struct.node_desc = self.prop_node_desc.data_ptr()
+        self._drain_prefetch()
         self.ws, self.ws_rays, self._graphs = None, 0, {}
         if hasattr(self, "_graph_rays"):
             del self._graph_rays
@@ -504,6 +595,7 @@ class FusedTrainer:
         this trainer's (a checkpoint taken after restructure()), the trainer
         first moves to the saved structure; then every value is copied into the
         trainer's buffers, whose device addresses the step descriptors hold."""
+        self._drain_prefetch()  # the restored cameras may move the next rays
         if int(sd["seed"]) != self.seed:
             raise ValueError("state was saved by a trainer with another seed")
         if "tree_max_depth" not in sd or "tree_active_node_ids" not in sd:

@@ -950,6 +950,52 @@ def test_host_batches_are_staged_like_device_batches(neat, case):
         b.step(host[0][0].double(), host[0][1], host[0][2])
 
 
+@pytest.mark.parametrize("proposal", [False, True])
+def test_look_ahead_segment_lists_take_the_same_steps(neat, case, proposal):
+    """step(..., next=b) builds batch b's segment lists on a side stream
+    under the step's Adam update (neat_train_step_segments, behind the step's
+    phase [4], or [5] on a proposal TRAIN step) and the call that takes b
+    skips building them (neat_train_step_prebuilt).  Six steps on different
+    batches queued without a synchronisation (with the proposal: TRAIN steps
+    1 and 5, SAMPLE steps in between), against the same steps without
+    look-ahead: the same counters every step, the same losses (the forward is
+    deterministic) and the same parameters up to the grid-gradient atomics'
+    order; pinned host batches the same way (staged one step ahead)."""
+    from neat_b200.trainer import FusedTrainer
+    def make():
+        return FusedTrainer(case.tree, _camera(case), case.C, case.G, case.M, lr_grid=1e-2, lr_decoder=5e-5, seed=7,
+                            grid=torch.from_numpy(case.grid), decoder=torch.from_numpy(case.dec),
+                            proposal=proposal, proposal_every=4)
+    n = case.R // 6
+    cols = (case.uv, case.img, case.target)
+    parts = [tuple(_dev(x[k * n:(k + 1) * n]) for x in cols) for k in range(6)]
+    host = [tuple(torch.from_numpy(np.ascontiguousarray(x[k * n:(k + 1) * n])).pin_memory() for x in cols)
+            for k in range(6)]
+    a = make()
+    la, ca = [], []
+    for p in parts:
+        la.append(a.step(*p).clone())
+        ca.append(a.counters.clone())
+    rel = 1e-4 if proposal else 1e-5
+    def moved(x, y):
+        return float(((x - y).abs() > 1e-6).float().mean())
+    for batches in (parts, host):
+        b = make()
+        lb, cb = [], []
+        for k in range(6):
+            lb.append(b.step(*batches[k], next=batches[k + 1] if k + 1 < 6 else None).clone())
+            cb.append(b.counters.clone())
+            assert (b._pf is not None) == (k + 1 < 6)
+        torch.cuda.synchronize()
+        a.check_status()
+        b.check_status()
+        for k in range(6):
+            assert torch.equal(cb[k], ca[k]), (k, cb[k].tolist(), ca[k].tolist())
+            assert float(lb[k]) == pytest.approx(float(la[k]), rel=rel)
+        assert moved(b.decoder, a.decoder) < 1e-2
+        assert moved(b.grid, a.grid) < 1e-3
+
+
 def test_checkpoint_after_restructure_restores_the_saved_tree(neat, case):
     """A checkpoint taken after restructure() holds the new active-node set; a
     trainer built on the original tree moves to that set before copying the

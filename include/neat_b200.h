@@ -418,8 +418,12 @@ int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, co
 /* neat_train_step_segments runs phase [1] of a step (rays, hit lists,      */
 /* node-major segments, sample offsets, tile map) for `batch` into          */
 /* `workspace` (neat_train_step_workspace_bytes bytes) and `counters` /     */
-/* `status` (as neat_step_out).  neat_train_step_prebuilt is               */
-/* neat_train_step for that batch without phase [1]: same arguments, with  */
+/* `status` (as neat_step_out); with a learned proposal in SAMPLE mode      */
+/* (`proposal`, as the step will pass it in its state) also the segments'   */
+/* placement CDF, which depends on the proposal's parameters and node       */
+/* descriptors (final once the TRAIN step that updates them has ended).     */
+/* neat_train_step_prebuilt is neat_train_step for that batch without       */
+/* phase [1] (nor, in SAMPLE mode, the CDF): same arguments, with           */
 /* out->counters = the counters neat_train_step_segments filled.            */
 /* A step reads the segment buffers up to its phase [4] (backward done),    */
 /* or up to [5] when it trains the learned proposal: queue                  */
@@ -427,8 +431,9 @@ int neat_train_step(const neat_step_desc* desc, const neat_step_state* state, co
 /* the running step (its counters must be another array than the running   */
 /* step's), and the prebuilt step behind the segments' completion.         */
 /* ----------------------------------------------------------------------- */
-int neat_train_step_segments(const neat_step_desc* desc, const neat_step_batch* batch, int64_t* counters,
-                             int* status, void* workspace, size_t workspace_bytes, neat_stream_t stream);
+int neat_train_step_segments(const neat_step_desc* desc, const neat_proposal* proposal, const neat_step_batch* batch,
+                             int64_t* counters, int* status, void* workspace, size_t workspace_bytes,
+                             neat_stream_t stream);
 int neat_train_step_prebuilt(const neat_step_desc* desc, const neat_step_state* state, const neat_step_batch* batch,
                              uint64_t seed, int step, const neat_step_out* out, void* workspace,
                              size_t workspace_bytes, neat_stream_t stream);

@@ -132,8 +132,8 @@ _SIGS = {
     "neat_train_step_prebuilt": (c_int, [ctypes.POINTER(StepDesc), ctypes.POINTER(StepState),
                                          ctypes.POINTER(StepBatch), c_uint64, c_int, ctypes.POINTER(StepOut), c_void_p,
                                          c_size_t, c_void_p]),
-    "neat_train_step_segments": (c_int, [ctypes.POINTER(StepDesc), ctypes.POINTER(StepBatch), c_void_p, c_void_p,
-                                         c_void_p, c_size_t, c_void_p]),
+    "neat_train_step_segments": (c_int, [ctypes.POINTER(StepDesc), c_void_p, ctypes.POINTER(StepBatch), c_void_p,
+                                         c_void_p, c_void_p, c_size_t, c_void_p]),
     "neat_project": (c_int, [ctypes.POINTER(StepDesc), c_void_p, c_void_p, c_void_p, ctypes.POINTER(StepBatch),
                              ctypes.POINTER(ProjectOut), c_void_p, c_size_t, c_void_p]),
     "neat_proposal_params": (c_int64, []),

@@ -995,7 +995,8 @@ static int train_step(const neat_step_desc* d, const neat_step_state* s, const n
     }
     if (pmode == NEAT_PROPOSAL_SAMPLE)
     {
-        ok         = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;
+        // (prebuilt: neat_train_step_segments has placed the CDF with the lists)
+        if (!prebuilt) ok = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;
         ta.seg_cdf = w.seg_cdf;
     }
     else if (pmode == NEAT_PROPOSAL_TRAIN)
@@ -1072,16 +1073,24 @@ extern "C" int neat_train_step_prebuilt(const neat_step_desc* d, const neat_step
     return train_step(d, s, b, seed, step, out, workspace, workspace_bytes, stream, true);
 }
 
-extern "C" int neat_train_step_segments(const neat_step_desc* d, const neat_step_batch* b, int64_t* counters,
-                                        int* status, void* workspace, size_t workspace_bytes, neat_stream_t stream)
+extern "C" int neat_train_step_segments(const neat_step_desc* d, const neat_proposal* proposal,
+                                        const neat_step_batch* b, int64_t* counters, int* status, void* workspace,
+                                        size_t workspace_bytes, neat_stream_t stream)
 {
     if (!d || !b || !counters || !status || !workspace) return NEAT_ERR_BAD_INPUT;
     const int chk = check_desc(d, b);
     if (chk != NEAT_OK) return chk;
+    int pmode = NEAT_PROPOSAL_OFF;
+    if (!proposal_mode(d, proposal, pmode)) return NEAT_ERR_BAD_INPUT;
     StepLayout L;
     if (!step_layout(d, b->num_rays, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
     const StepBufs w = step_bufs(L, workspace);
-    const bool ok    = build_segments(d, b, L, w, counters, status, (cudaStream_t)stream);
+    cudaStream_t st  = (cudaStream_t)stream;
+    bool ok          = build_segments(d, b, L, w, counters, status, st);
+    // a SAMPLE step's placement CDF depends on the segments and on the proposal's
+    // parameters and node descriptors, which only a TRAIN step's end changes
+    if (pmode == NEAT_PROPOSAL_SAMPLE)
+        ok = ok && launch_proposal_cdf(w.segs, counters, proposal, w.seg_cdf, st) == cudaSuccess;
     return ok && cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 

@@ -333,9 +333,14 @@ class FusedTrainer:
         desc = self.desc if (not self.proposal or train) else self.desc_budget
         ci = self._ci ^ 1
         batch = _lib.StepBatch(uv=uv.data_ptr(), image_id=image_id.data_ptr(), target=target.data_ptr(), num_rays=R)
-        rc = self.lib.neat_train_step_segments(ctypes.byref(desc), ctypes.byref(batch), self._cnt[ci].data_ptr(),
-                                               self.status.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
-                                               ps.cuda_stream)
+        prop = None
+        if self.proposal:
+            # the next step's mode; the running step read the struct when it was queued
+            self.prop_struct.mode = _lib.NEAT_PROPOSAL_TRAIN if train else _lib.NEAT_PROPOSAL_SAMPLE
+            prop = ctypes.addressof(self.prop_struct)
+        rc = self.lib.neat_train_step_segments(ctypes.byref(desc), prop, ctypes.byref(batch),
+                                               self._cnt[ci].data_ptr(), self.status.data_ptr(), self.ws.data_ptr(),
+                                               self.ws.numel(), ps.cuda_stream)
         _lib.check(rc, "neat_train_step_segments")
         done = torch.cuda.Event()
         done.record(ps)

@@ -125,15 +125,27 @@ __global__ void k_proposal_cdf(const SegRec* __restrict__ segs, const int64_t* c
     for (int i = threadIdx.x; i < PropOff::total; i += blockDim.x) P[i] = params[i];
     __syncthreads();
     const int64_t n = counters[0];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    // two segments a thread (i and i + stride) per iteration, packed f32x2
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride)
     {
-        float f[PIN], p[PBIN], c[PBIN];
-        proposal_features(segs[i], node_desc, f);
-        proposal_forward(P, f, mix, p, nullptr);
-        proposal_cdf(p, c);
+        const int64_t i1 = i + stride;
+        const bool two   = i1 < n;
+        float f0[PIN], f1[PIN], p0[PBIN], p1[PBIN], c[PBIN];
+        proposal_features(segs[i], node_desc, f0);
+        proposal_features(segs[two ? i1 : i], node_desc, f1);
+        proposal_forward2(P, f0, f1, mix, p0, p1);
+        proposal_cdf(p0, c);
         float4* dst = reinterpret_cast<float4*>(seg_cdf + 8 * i);
         dst[0]      = make_float4(c[0], c[1], c[2], c[3]);
         dst[1]      = make_float4(c[4], c[5], c[6], c[7]);
+        if (two)
+        {
+            proposal_cdf(p1, c);
+            dst    = reinterpret_cast<float4*>(seg_cdf + 8 * i1);
+            dst[0] = make_float4(c[0], c[1], c[2], c[3]);
+            dst[1] = make_float4(c[4], c[5], c[6], c[7]);
+        }
     }
 }
 

@@ -57,6 +57,9 @@ def test_library_host_calls_without_gpu():
     assert lib.neat_make_rays(None, None, None, -1, 16, 16, None, None, None, None, None, None) == \
         _lib.NEAT_ERR_BAD_INPUT
     assert lib.neat_tree_prepare(None, None, None, 4, 9, None, None, None) == _lib.NEAT_ERR_BAD_INPUT
+    # the look-ahead entries refuse missing arguments the same way
+    assert lib.neat_train_step_segments(None, None, None, None, None, None, 0, None) == _lib.NEAT_ERR_BAD_INPUT
+    assert lib.neat_train_step_prebuilt(None, None, None, 0, 1, None, None, 0, None) == _lib.NEAT_ERR_BAD_INPUT
 
 
 def test_no_cpu_fallback_when_library_missing(monkeypatch):

@@ -225,8 +225,11 @@ class FusedTrainer:
         on a side stream while this step's Adam update runs
         (neat_train_step_segments, queued behind the step's phase [4], or [5]
         on a proposal TRAIN step), and that call skips building them
-        (neat_train_step_prebuilt).  Ignored while poses or intrinsics are
-        optimised (the pose update after the step moves the next rays)."""
+        (neat_train_step_prebuilt).  The following call is recognised by its
+        tensors, so their contents must stay as passed until it runs (a loop
+        that refills one buffer in place passes next=None).  Ignored while
+        poses or intrinsics are optimised (the pose update after the step moves
+        the next rays)."""
         cur = torch.cuda.current_stream(self.dev)
         pf, self._pf = self._pf, None
         staged = None

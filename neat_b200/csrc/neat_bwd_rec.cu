@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                 for (int i = 0; i < 8; ++i)
                 {
                     const float2 z  = make_float2(__uint_as_float(z1r[j][2 * i]), __uint_as_float(z1r[j][2 * i + 1]));
-                    const float2 sg = make_float2(sigmoidf_(z.x), sigmoidf_(z.y));
+                    const float2 sg = sigmoid2<PREC>(z);
                     const float2 u  = __ffma2_rn(z, __ffma2_rn(sg, neg1x2(), one2()), one2());
                     const float2 dd = __fmul2_rn(sg, u);
                     d1[2 * i]       = dd.x;
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(BR_THREADS, 1) k_bwd_rec(StepTcArgs a)
                         const float2 w3 = *reinterpret_cast<const float2*>(sw3 + col);
                         const float2 zz = __fadd2_rn(
                             make_float2(__uint_as_float(z2r[j][2 * i]), __uint_as_float(z2r[j][2 * i + 1])), b2);
-                        const float2 sg = make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y));
+                        const float2 sg = sigmoid2<PREC>(zz);
                         const float2 h2 = __fmul2_rn(zz, sg);
                         yp2             = __ffma2_rn(h2, w3, yp2);
                         h2k[8 * j + i]  = h2;

@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     for (int i = 0; i < 8; ++i)
                     {
                         const float2 zz = make_float2(z[2 * i], z[2 * i + 1]);
-                        hz[i]           = __fmul2_rn(zz, make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y)));
+                        hz[i]           = __fmul2_rn(zz, sigmoid2<PREC>(zz));
                     }
 #pragma unroll
                     for (int p = 0; p < P::PIECES; ++p)
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 else
                 {
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+                    for (int i = 0; i < 16; ++i) z[i] = silu1<PREC>(z[i]);
                     store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
                     store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
                 }
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         const int col   = c0 + 16 * j + 2 * i;
                         const float2 zz = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]),
                                                      *reinterpret_cast<const float2*>(sb2 + col));
-                        const float2 h2 = __fmul2_rn(zz, make_float2(sigmoidf_(zz.x), sigmoidf_(zz.y)));
+                        const float2 h2 = __fmul2_rn(zz, sigmoid2<PREC>(zz));
                         yp2             = __ffma2_rn(h2, *reinterpret_cast<const float2*>(sw3 + col), yp2);
                     }
                 }
@@ -887,7 +887,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                     {
-                        const float sg = sigmoidf_(z[i]);
+                        const float sg = sigmoid1<PREC>(z[i]);
                         d1[i]          = sg * (1.0f + z[i] * (1.0f - sg));
                         z[i]           = z[i] * sg;
                     }
@@ -896,7 +896,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 else
                 {
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) z[i] = siluf_(z[i]);
+                    for (int i = 0; i < 16; ++i) z[i] = silu1<PREC>(z[i]);
                 }
                 store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j), z);
                 store_chunk<PREC>(pHB, K::HB_PC, HB::off(s, c0 + 16 * j + 8), z + 8);
@@ -973,7 +973,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         {
                             const int col  = c0 + 16 * j + i;
                             const float zz = z[i] + sb2[col];
-                            const float sg = sigmoidf_(zz);
+                            const float sg = sigmoid1<PREC>(zz);
                             z[i]           = zz * sg;
                             yp             = fmaf(z[i], sw3[col], yp);
                             g[i]           = sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
@@ -985,7 +985,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     {
 #pragma unroll
                         for (int i = 0; i < 16; ++i)
-                            yp = fmaf(siluf_(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
+                            yp = fmaf(silu1<PREC>(z[i] + sb2[c0 + 16 * j + i]), sw3[c0 + 16 * j + i], yp);
                     }
                 }
                 if constexpr (CACHE) tmem_wait_st();
@@ -1064,7 +1064,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         {
                             const int col   = c0 + 16 * j + i;
                             const float zz  = z[i] + sb2[col];
-                            const float sg  = sigmoidf_(zz);
+                            const float sg  = sigmoid1<PREC>(zz);
                             d[i]            = dy * sw3[col] * (sg * (1.0f + zz * (1.0f - sg)));
                             dw3[16 * j + i] = fmaf(zz * sg, dy, dw3[16 * j + i]);
                         }
@@ -1138,7 +1138,7 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                         tmem_ld16(tD2 + lane + c0 + 16 * j, g);
                         tmem_ld16(tD1 + lane + c0 + 16 * j, z);
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) g[i] *= silu_grad(z[i]);
+                        for (int i = 0; i < 16; ++i) g[i] *= silu_grad1<PREC>(z[i]);
                     }
 #pragma unroll
                     for (int i = 0; i < 16; i += P::E)

@@ -372,6 +372,51 @@ __device__ __forceinline__ float2 one2() { return make_float2(1.0f, 1.0f); }
 // a - b (exact when the difference is representable, as a bf16 remainder is)
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, neg1x2(), a); }
 
+// sigma(z) of a pair of pre-activations for precision PREC.  BF16X3 keeps
+// 1 / (1 + 2^(-z log2 e)) (ex2 + rcp, FP32-level).  BF16, whose GEMM operands
+// carry 8 significant bits, uses sigma(z) = 1/2 + tanh(z/2) / 2 with one
+// tanh.approx.f32 a value (relative error of tanh below 2^-10.9, so sigma is
+// within 2^-11.9 absolute): one SFU op a value instead of two.  h = z sigma(z)
+// then stays within |z| 2^-11.9, below the BF16 rounding of h (|h| 2^-9) for
+// z > -2 and small against the layer's other activations below it.
+template <int PREC>
+__device__ __forceinline__ float2 sigmoid2(float2 z)
+{
+    if constexpr (PREC == BF16)
+    {
+        const float2 hz = __fmul2_rn(z, make_float2(0.5f, 0.5f));
+        float2 th;
+        asm("tanh.approx.f32 %0, %1;" : "=f"(th.x) : "f"(hz.x));
+        asm("tanh.approx.f32 %0, %1;" : "=f"(th.y) : "f"(hz.y));
+        return __ffma2_rn(th, make_float2(0.5f, 0.5f), make_float2(0.5f, 0.5f));
+    }
+    else
+        return make_float2(sigmoidf_(z.x), sigmoidf_(z.y));
+}
+template <int PREC>
+__device__ __forceinline__ float sigmoid1(float z)
+{
+    if constexpr (PREC == BF16)
+    {
+        float th;
+        asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(0.5f * z));
+        return fmaf(0.5f, th, 0.5f);
+    }
+    else
+        return sigmoidf_(z);
+}
+template <int PREC>
+__device__ __forceinline__ float silu1(float z)
+{
+    return z * sigmoid1<PREC>(z);
+}
+template <int PREC>
+__device__ __forceinline__ float silu_grad1(float z)
+{
+    const float sg = sigmoid1<PREC>(z);
+    return sg * (1.0f + z * (1.0f - sg));
+}
+
 // One BF16 piece of a pair: the packed bits, and the pair minus the piece
 // (exact: the remainder of a bf16 rounding).
 __device__ __forceinline__ uint32_t piece2(float2& r)

@@ -480,15 +480,34 @@ __global__ void k_tonemap_param_loss(neat_tonemap T)
     *T.param_loss = l;
 }
 
-__global__ void k_dec_reduce_adam(const float* __restrict__ part, int nparts, int P, float* __restrict__ grad,
-                                  float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float b1,
-                                  float b2, float eps, const StepScalars* __restrict__ sc)
+// Decoder gradient: the sum of the CTA partials (rows of part), then Adam.  A
+// block takes 32 parameters; its warp g sums rows g, g + 8, g + 16, .. (each
+// warp reads 128 contiguous bytes of a row), and the 8 warp sums are added in
+// warp order: a fixed order, so the gradient is reproducible, and ~150
+// blocks instead of one thread a parameter walking all rows.
+constexpr int DEC_RED_GROUPS = 8;
+
+__global__ void __launch_bounds__(32 * DEC_RED_GROUPS)
+    k_dec_reduce_adam(const float* __restrict__ part, int nparts, int P, float* __restrict__ grad,
+                      float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float b1, float b2,
+                      float eps, const StepScalars* __restrict__ sc)
 {
+    __shared__ float red[DEC_RED_GROUPS][33];
+    const int lx = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int i  = blockIdx.x * 32 + lx;
+    float s      = 0.0f;
+    if (i < P)
+    {
+#pragma unroll 4
+        for (int b = g; b < nparts; b += DEC_RED_GROUPS) s += part[(int64_t)b * P + i];
+    }
+    red[g][lx] = s;
+    __syncthreads();
+    if (g != 0 || i >= P) return;
     const float step_size = sc->dec_step_size, sqrt_bc2 = sc->sqrt_bc2;
-    const int i           = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    float gsum = 0.0f;
-    for (int b = 0; b < nparts; ++b) gsum += part[(int64_t)b * P + i];
+    float gsum = red[0][lx];
+#pragma unroll
+    for (int k = 1; k < DEC_RED_GROUPS; ++k) gsum += red[k][lx];
     grad[i] = gsum;
     float pi = p[i], mi = m[i], vi = v[i];
     adam_update(pi, gsum, mi, vi, b1, b2, eps, step_size, sqrt_bc2);
@@ -1034,7 +1053,7 @@ static int train_step(const neat_step_desc* d, const neat_step_state* s, const n
     phase(4);
 
     const int P = (int)decoder_params(d->C);
-    k_dec_reduce_adam<<<(P + 255) / 256, 256, 0, st>>>(w.dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
+    k_dec_reduce_adam<<<(P + 31) / 32, 32 * DEC_RED_GROUPS, 0, st>>>(w.dec_part, L.bwd_grid, P, s->decoder_grad, s->decoder,
                                                         s->decoder_m, s->decoder_v, d->beta1, d->beta2, d->eps,
                                                         w.scal);
     const int64_t ngrid = (int64_t)A * d->G * d->G * d->G * d->C;

@@ -52,9 +52,9 @@ STEP_LAUNCHES = 23
 TRAFFIC_BYTES_PER_SAMPLE = {
     # BF16x3 at the full-size workload itself (2^18 rays, 11.64 M samples): 886.6 + 176.5 MB
     ("full", "bf16x3"): (1063.1e6 / 11.6376e6, "ncu capture of a full-size launch (2^18 rays), per sample"),
-    # BF16, same scene at 2^16 rays (2.908 M samples): 344.3 + 119.7 MB -- an upper bound at
+    # BF16, same scene at 2^16 rays (2.908 M samples): 344.3 + 120.8 MB -- an upper bound at
     # larger batches, which reuse more of the grid gradient in L2
-    ("full", "bf16"): (464.0e6 / 2.908e6, "ncu capture at 2^16 rays scaled by samples (upper bound)")}
+    ("full", "bf16"): (465.1e6 / 2.908e6, "ncu capture at 2^16 rays scaled by samples (upper bound)")}
 KERNEL_NAME = {"simt": "k_step_tiles<C=%d, backward> (FP32 SIMT)",
                "bf16x3": "k_bwd_rec<C=%d, BF16x3> (backward from the forward's records, MMA warp)",
                "bf16": "k_bwd_rec<C=%d, BF16> (backward from the forward's records, MMA warp)"}

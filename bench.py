@@ -304,15 +304,24 @@ def decoder_path(name):
             "bf16": _lib.NEAT_DECODER_TC_BF16}[name]
 
 
+# the count head's tolerance: a segment gets ceil(exp(v) / eps) samples (at most
+# the budget, at least 2), v its predicted log(length x density variation); the
+# midpoint rule then misses about eps / 2 of its integral at density jumps,
+# below the projections' Poisson noise at I0 = 1e4 (about 0.01)
+COUNT_EPS = 0.05
+
+
 def make_trainer(cfg, tree, cam, dev, decoder, proposal, seed):
     """FusedTrainer of a workload: decoder path by name; with the learned
-    proposal the BF16 grid copy, the workload's sample budget and a 50-step
-    proposal cycle (one uniform TRAIN step, then SAMPLE steps)."""
+    proposal the BF16 grid copy, the workload's sample budget, the count head's
+    sample counts and a 50-step proposal cycle (one uniform TRAIN step, then
+    SAMPLE steps)."""
     from neat_b200.trainer import FusedTrainer
     kw = dict(decoder_path=decoder_path(decoder), device=dev)
     if proposal:
         kw.update(proposal=True, proposal_budget=cfg.get("proposal_budget", 12), proposal_every=50,
-                  grid_bf16=decoder == "bf16")
+                  grid_bf16=decoder == "bf16", proposal_count_eps=cfg.get("count_eps", COUNT_EPS),
+                  proposal_count_min=2)
     elif decoder == "bf16":
         kw.update(grid_bf16=True)
     tr = FusedTrainer(tree, cam, cfg["C"], cfg["G"], cfg["M"], lr_grid=1e-2, lr_decoder=5e-5, seed=seed, **kw)
@@ -355,10 +364,11 @@ def time_steps(tr, batches, phase_events=True):
 def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
     """rays/s of the plain FP32 SIMT step, the BF16 step (BF16 grid copy and
     decoder operands, FP32 accumulation) and the BF16 step with the learned
-    proposal (12 samples per segment; one full 50-step cycle, its uniform
-    TRAIN step included), CUDA events around each timed loop; the BF16 +
-    proposal step against both FP32 steps (ref_rays_per_s: the FP32-accurate
-    tensor-core step of the main line)."""
+    proposal (budget 12 samples per segment, fewer where the count head
+    predicts little variation; one full 50-step cycle, its uniform TRAIN step
+    included, after two cycles that train the proposal), CUDA events around
+    each timed loop; the BF16 + proposal step against both FP32 steps
+    (ref_rays_per_s: the FP32-accurate tensor-core step of the main line)."""
     R = cfg["R"]
     gen = torch.Generator(device=dev)
     gen.manual_seed(4242)
@@ -367,8 +377,8 @@ def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
     for name, dec, prop in (("fp32_simt", "simt", False), ("bf16", "bf16", False), ("bf16_proposal12", "bf16", True)):
         tr = make_trainer(cfg, tree, cam, dev, dec, prop, cfg["seed"])
         k = steps if prop else 10
-        for i in range(3 if not prop else 0):
-            tr.step(*batches[i])
+        for i in range(3 if not prop else 2 * steps):
+            tr.step(*batches[i % steps])
         ms, phase_ms, counts = time_steps(tr, batches[:k])
         out[name] = {"rays_per_s": R * k / (ms / 1000.0), "ms_per_step": ms / k, "steps": k,
                      "samples_per_step": float(counts[:, 1].double().mean()), "phase_ms": phase_ms}
@@ -384,16 +394,19 @@ def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
 def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
     """Time to the plain method's volume PSNR.  The plain method (FP32-accurate
     decoder, uniform 32 samples) trains `steps` steps; its final volume PSNR is
-    the target.  Then BF16 + learned proposal (12 samples per segment) trains
-    until it reaches the target within 0.1 dB (at most `steps` steps), and so
-    does BF16 with 12 uniform samples per segment (the same budget without the
-    network: the proposal's ablation).  All runs see the same batches from the
-    same initial state and are evaluated
-    every `every` steps; each run's time to the target - 0.1 dB is the
-    CUDA-event time of its training steps up to the first evaluation at or
-    above it (evaluations excluded).  Volume PSNR = 10 log10(peak^2 / MSE) over
-    the vol_n^3 voxel-corner lattice (UniformSampledVolume) against the f64
-    phantom density, peak = the phantom's maximum, MSE in f64."""
+    the target.  Then BF16 + learned proposal (budget 12 samples per segment,
+    fewer where the count head predicts little variation) trains until it
+    reaches the target within 0.1 dB (at most `steps` steps), and so do two
+    ablations of the learned part, BF16 with uniform samples and no network:
+    12 per segment (the same budget) and the uniform budget whose samples per
+    step come closest to the proposal run's mean (the same number of samples,
+    spread evenly).  All runs see the same batches from the same initial state
+    and are evaluated every `every` steps; each run's time to the target -
+    0.1 dB is the CUDA-event time of its training steps up to the first
+    evaluation at or above it (evaluations excluded).  Volume PSNR =
+    10 log10(peak^2 / MSE) over the vol_n^3 voxel-corner lattice
+    (UniformSampledVolume) against the f64 phantom density, peak = the
+    phantom's maximum, MSE in f64."""
     gt = scene.density_volume(vol_n)
     peak2 = float(gt.max()) ** 2
     R = cfg["R"]
@@ -404,44 +417,65 @@ def volume_psnr_race(cfg, scene, tree, cam, dev, steps, every=100, vol_n=256):
         return 10.0 * np.log10(peak2 / mse)
 
     res = {}
-    target = None
-    # the third run is the ablation of the learned part: the same BF16 step and
-    # the same 12-sample budget per segment, placed uniformly (no network)
-    for name, dec, prop, M in (("plain_fp32", "bf16x3", False, cfg["M"]), ("bf16_proposal12", "bf16", True, cfg["M"]),
-                               ("bf16_uniform12", "bf16", False, 12)):
+    target = [None]
+
+    def run(name, dec, prop, M):
         tr = make_trainer(dict(cfg, M=M), tree, cam, dev, dec, prop, cfg["seed"])
         gen = torch.Generator(device=dev)
         gen.manual_seed(777)
-        ms, curve, k = 0.0, [], 0
+        ms, curve, k, samples = 0.0, [], 0, 0.0
         while k < steps:
             n = min(every, steps - k)
             bs = [scene.sample_batch(R, gen) for _ in range(n)]
-            t, _, _ = time_steps(tr, bs, phase_events=False)
+            t, _, cnt = time_steps(tr, bs, phase_events=False)
             k += n
             ms += t
+            samples += float(cnt[:, 1].double().sum())
             p = vpsnr(tr)
             curve.append([k, round(ms, 1), round(p, 3)])
-            if target is not None and p >= target - 0.1:
+            if target[0] is not None and p >= target[0] - 0.1:
                 break
-        res[name] = {"steps": k, "train_ms": ms, "ms_per_step": ms / k, "volume_psnr_db": curve[-1][2],
-                     "curve": curve}
-        if target is None:
-            target = curve[-1][2]
+        res[name] = {"steps": k, "train_ms": ms, "ms_per_step": ms / k, "samples_per_step": samples / k,
+                     "samples_per_segment_budget": M if not prop else cfg.get("proposal_budget", 12),
+                     "volume_psnr_db": curve[-1][2], "curve": curve}
+        if target[0] is None:
+            target[0] = curve[-1][2]
         del tr
         torch.cuda.empty_cache()
-    for name in ("plain_fp32", "bf16_proposal12", "bf16_uniform12"):
-        hit = [c for c in res[name]["curve"] if c[2] >= target - 0.1]
+
+    run("plain_fp32", "bf16x3", False, cfg["M"])
+    run("bf16_proposal12", "bf16", True, cfg["M"])
+    run("bf16_uniform12", "bf16", False, 12)
+    # the uniform budget with the proposal run's samples per step: one step's
+    # sample count per candidate budget (the counts depend on the rays only)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(777)
+    b = scene.sample_batch(R, gen)
+    best = None
+    for M in range(1, 13):
+        tr = make_trainer(dict(cfg, M=M), tree, cam, dev, "bf16", False, cfg["seed"])
+        tr.step(*b)
+        n = float(tr.counters[1].item())
+        del tr
+        if best is None or abs(n - res["bf16_proposal12"]["samples_per_step"]) < best[1]:
+            best = (M, abs(n - res["bf16_proposal12"]["samples_per_step"]))
+    torch.cuda.empty_cache()
+    run("bf16_uniform_matched", "bf16", False, best[0])
+    tgt = target[0]
+    for name in ("plain_fp32", "bf16_proposal12", "bf16_uniform12", "bf16_uniform_matched"):
+        hit = [c for c in res[name]["curve"] if c[2] >= tgt - 0.1]
         res[name]["ms_to_target"] = hit[0][1] if hit else None
         res[name]["steps_to_target"] = hit[0][0] if hit else None
     a, b = res["plain_fp32"]["ms_to_target"], res["bf16_proposal12"]["ms_to_target"]
-    res["target_db"] = target - 0.1
-    res["plain_final_db"] = target
+    res["target_db"] = tgt - 0.1
+    res["plain_final_db"] = tgt
     res["speedup_to_target"] = (a / b) if (a and b) else None
-    u = res["bf16_uniform12"]["ms_to_target"]
-    res["proposal_vs_uniform12_to_target"] = (u / b) if (u and b) else None
+    for name in ("bf16_uniform12", "bf16_uniform_matched"):
+        u = res[name]["ms_to_target"]
+        res["proposal_vs_" + name[5:] + "_to_target"] = (u / b) if (u and b) else None
     res["definition"] = ("target = plain method's final volume PSNR - 0.1 dB; volume PSNR = 10 log10(peak^2 / MSE), "
                          "%d^3 voxel-corner lattice vs the phantom density, f64; time = CUDA events around the "
-                         "training steps" % vol_n)
+                         "training steps; proposal_vs_X = X's time to the target / the proposal's" % vol_n)
     return res
 
 
@@ -541,9 +575,9 @@ def reference_gpu_igs(cfg, scene, tree, cam, dev, reps=5):
 
 def large_workload(dev, steps=50, warmup=3):
     """The large porous configuration, BF16 + learned proposal: rays/s over one
-    full 50-step proposal cycle (its uniform 32-sample TRAIN step included),
-    device-resident batches, CUDA events; per-phase times and samples per
-    step."""
+    full 50-step proposal cycle (its uniform 32-sample TRAIN step included)
+    after two cycles that train the proposal, device-resident batches, CUDA
+    events; per-phase times and samples per step."""
     cfg = dict(WORKLOADS["large"])
     scene, tree, cam = build_workload(cfg, dev)
     tr = make_trainer(cfg, tree, cam, dev, "bf16", True, cfg["seed"])
@@ -553,13 +587,13 @@ def large_workload(dev, steps=50, warmup=3):
     batches = [scene.sample_batch(R, gen) for _ in range(warmup + steps)]
     for i in range(warmup):  # the warm-up includes the first TRAIN step; the timed cycle has its own
         tr.step(*batches[i])
-    while (tr.step_id % 50) != 0:  # start the timed region at a cycle boundary
-        tr.step(*batches[0])
+    while tr.step_id < 100 or (tr.step_id % 50) != 0:  # two cycles; the timed region starts at a boundary
+        tr.step(*batches[tr.step_id % warmup])
     ms, phase_ms, counts = time_steps(tr, batches[warmup:])
     S = counts[:, 1].double()
     out = {"workload": cfg["desc"], "rays_per_s": R * steps / (ms / 1000.0), "ms_per_step": ms / steps,
            "steps": steps, "timed": "one 50-step proposal cycle: 1 uniform TRAIN step (32 samples per segment) + "
-                                    "49 SAMPLE steps (12 per segment)",
+                                    "49 SAMPLE steps (at most 12 per segment: the count head's counts)",
            "samples_per_step_mean": float(S.mean()), "samples_train_step": float(S.max()),
            "samples_sample_step": float(S.min()), "active_nodes": tree.NumActiveNodes(),
            "node_depths": {int(k): int(v) for k, v in zip(*np.unique(tree.node_depth[tree.active_node_ids],

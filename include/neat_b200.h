@@ -265,8 +265,18 @@ typedef struct
 /* target is |m_b - m_b-1| + |m_b+1 - m_b| of the binned masses m, each     */
 /* segment weighted by its total variation (the midpoint rule is exact on  */
 /* constant and linear stretches; its error sits at changes).               */
+/* A linear count head on the last hidden layer and the inputs,            */
+/* v = bv + Wv . h2 + Uv . f, predicts log(a + 1e-4) of the segment, a =    */
+/* (tmax - tmin) sum_j |rho_j - rho_j-1| over the densities of its TRAIN-  */
+/* call samples (the midpoint rule with n samples misses about a / (2 n) of */
+/* the integral at density jumps).  TRAIN calls train it on the squared     */
+/* error over every segment (its gradient stops at h2; it steps at 10x lr); */
+/* with count_eps > 0, SAMPLE calls give a segment                          */
+/* n = min(n_ref, max(count_min, ceil(exp(v) / count_eps))) samples, n_ref  */
+/* the reference's count at the budget: flat and empty segments get fewer. */
 /* params: neat_proposal_params() floats,                                   */
-/*   W1 [32][16] | b1 [32] | W2 [32][32] | b2 [32] | W3 [8][32] | b3 [8].    */
+/*   W1 [32][16] | b1 [32] | W2 [32][32] | b2 [32] | W3 [8][32] | b3 [8]    */
+/*   | Wv [32] | Uv [16] | bv.                                              */
 /* ----------------------------------------------------------------------- */
 #define NEAT_PROPOSAL_IN 16
 #define NEAT_PROPOSAL_HIDDEN 32
@@ -284,12 +294,15 @@ typedef struct
     float* v;          /* Adam second moment */
     float* grad;       /* out: gradient of the last training iteration */
     int* step_counter; /* device int: proposal Adam steps taken (advanced on the device) */
-    float* loss;       /* optional device f32[2]: mass-weighted mean cross-entropy of the last
-                        * iteration and of its targets' entropy (their difference: the KL) */
+    float* loss;       /* optional device f32[3]: mass-weighted mean cross-entropy of the last
+                        * iteration and of its targets' entropy (their difference: the KL),
+                        * and the count head's mean squared error / 2 */
     float lr, beta1, beta2, eps;
     float mix;         /* uniform share of the sample density, e.g. 0.1 */
     int iters;         /* Adam iterations per TRAIN call */
     float* node_desc;  /* [num_active][6] node descriptors, written by TRAIN calls */
+    float count_eps;   /* > 0: SAMPLE calls take the count head's sample counts (above); 0: n_ref */
+    int count_min;     /* fewest samples a segment gets under count_eps (>= 1 when count_eps > 0) */
 } neat_proposal;
 
 /* ----------------------------------------------------------------------- */

@@ -54,7 +54,8 @@ NEAT_PROPOSAL_IN, NEAT_PROPOSAL_HIDDEN, NEAT_PROPOSAL_BINS = 16, 32, 8
 class Proposal(ctypes.Structure):
     _fields_ = [("mode", c_int), ("params", c_void_p), ("m", c_void_p), ("v", c_void_p), ("grad", c_void_p),
                 ("step_counter", c_void_p), ("loss", c_void_p), ("lr", c_float), ("beta1", c_float),
-                ("beta2", c_float), ("eps", c_float), ("mix", c_float), ("iters", c_int), ("node_desc", c_void_p)]
+                ("beta2", c_float), ("eps", c_float), ("mix", c_float), ("iters", c_int), ("node_desc", c_void_p),
+                ("count_eps", c_float), ("count_min", c_int)]
 
 
 NEAT_RESPONSE_PARAMS = 25

@@ -67,6 +67,8 @@ struct StepTileArgs
     const int* step_dev;  // when set, the step number is read here (device-side step counter)
     const float* seg_cdf;  // proposal CDF per node-major segment [8] (null: uniform stratified)
     float* seg_hist;       // per ray-major segment [8]: contribution mass per sub-interval (null: off)
+    float* seg_dens;       // per node-major sample: its density (null: off; samples < dens_cap only)
+    int64_t dens_cap;
     float* seg_pgrad;      // per node-major segment [6]: sums of dL/d(ix,iy,iz) and t times it (null: off)
     // per-sample records the forward writes for the backward (null: off): SoA
     // [8 + C][rec_cap], fields lu, lv, lw, weight, t (f32), ray, row, seg (i32),
@@ -96,9 +98,11 @@ cudaError_t launch_pose_grad(const SegRec* segs, const int64_t* counters, const 
                              cudaStream_t st);
 
 // Learned proposal (neat_proposal.cu).
-// CDF of every node-major segment (counters[0] of them) from the proposal MLP.
-cudaError_t launch_proposal_cdf(const SegRec* segs, const int64_t* counters, const neat_proposal* pr, float* seg_cdf,
-                                cudaStream_t st);
+// CDF of every node-major segment (counters[0] of them) from the proposal MLP
+// and, when pr->count_eps > 0, its sample count from the count head (into the
+// segment record and seg_n, before the sample offsets are scanned).
+cudaError_t launch_proposal_cdf(SegRec* segs, int* seg_n, const int64_t* counters, const neat_proposal* pr,
+                                float* seg_cdf, cudaStream_t st);
 // Node descriptors from the current grid (channel-last) and decoder.
 cudaError_t launch_node_desc(const float* grid, int64_t A, int C, int G, const float* decoder, float beta,
                              float* node_desc, cudaStream_t st);
@@ -106,7 +110,13 @@ cudaError_t launch_node_desc(const float* grid, int64_t A, int C, int G, const f
 int proposal_grad_blocks();
 size_t proposal_part_floats();  // workspace floats of the training partials
 cudaError_t launch_proposal_train(const SegRec* segs, const int64_t* counters, const float* seg_hist,
-                                  const neat_proposal* pr, float* part, int iters, cudaStream_t st);
+                                  const float* seg_tv, const neat_proposal* pr, float* part, int iters,
+                                  cudaStream_t st);
+// Per segment of a uniformly sampled TRAIN step: (tmax - tmin) times the total
+// variation of its samples' densities (seg_dens, node-major samples) into
+// seg_tv[rm]; -1 for a segment whose samples lie past dens_cap.
+cudaError_t launch_seg_variation(const SegRec* segs, const int* samp_off, const int64_t* counters,
+                                 const float* seg_dens, int64_t dens_cap, float* seg_tv, cudaStream_t st);
 
 // tcgen05 tile kernels (neat_tc.cu); prec 0 = BF16 operands, 1 = three-piece BF16 split.
 int tc_backward_grid(int C, int prec);

@@ -117,9 +117,22 @@ cudaError_t launch_node_desc(const float* grid, int64_t A, int C, int G, const f
     return cudaGetLastError();
 }
 
-__global__ void k_proposal_cdf(const SegRec* __restrict__ segs, const int64_t* counters,
+// The count head's sample count for a segment: its record's n (and the step
+// between uniform samples, kept consistent) and its seg_n entry.
+__device__ __forceinline__ void set_count(SegRec& r, int& sn, float v, float eps, int nmin)
+{
+    const int n = proposal_count(v, r.n, eps, nmin);
+    r.n         = n;
+    r.step      = __fdiv_rn(__fsub_rn(r.tmax, r.tmin), (float)n);
+    sn          = n;
+}
+
+// Per node-major segment: the proposal's CDF bin ends and, when
+// count_eps > 0, the segment's sample count from the count head (written to
+// the segment record and to seg_n, ahead of the sample-offset scan).
+__global__ void k_proposal_cdf(SegRec* __restrict__ segs, int* __restrict__ seg_n, const int64_t* counters,
                                const float* __restrict__ params, const float* __restrict__ node_desc, float mix,
-                               float* __restrict__ seg_cdf)
+                               float count_eps, int count_min, float* __restrict__ seg_cdf)
 {
     __shared__ float P[PropOff::total];
     for (int i = threadIdx.x; i < PropOff::total; i += blockDim.x) P[i] = params[i];
@@ -131,28 +144,31 @@ __global__ void k_proposal_cdf(const SegRec* __restrict__ segs, const int64_t* c
     {
         const int64_t i1 = i + stride;
         const bool two   = i1 < n;
-        float f0[PIN], f1[PIN], p0[PBIN], p1[PBIN], c[PBIN];
+        float f0[PIN], f1[PIN], p0[PBIN], p1[PBIN], c[PBIN], v0, v1;
         proposal_features(segs[i], node_desc, f0);
         proposal_features(segs[two ? i1 : i], node_desc, f1);
-        proposal_forward2(P, f0, f1, mix, p0, p1);
+        proposal_forward2(P, f0, f1, mix, p0, p1, v0, v1);
         proposal_cdf(p0, c);
         float4* dst = reinterpret_cast<float4*>(seg_cdf + 8 * i);
         dst[0]      = make_float4(c[0], c[1], c[2], c[3]);
         dst[1]      = make_float4(c[4], c[5], c[6], c[7]);
+        if (count_eps > 0.0f) set_count(segs[i], seg_n[i], v0, count_eps, count_min);
         if (two)
         {
             proposal_cdf(p1, c);
             dst    = reinterpret_cast<float4*>(seg_cdf + 8 * i1);
             dst[0] = make_float4(c[0], c[1], c[2], c[3]);
             dst[1] = make_float4(c[4], c[5], c[6], c[7]);
+            if (count_eps > 0.0f) set_count(segs[i1], seg_n[i1], v1, count_eps, count_min);
         }
     }
 }
 
-cudaError_t launch_proposal_cdf(const SegRec* segs, const int64_t* counters, const neat_proposal* pr, float* seg_cdf,
-                                cudaStream_t st)
+cudaError_t launch_proposal_cdf(SegRec* segs, int* seg_n, const int64_t* counters, const neat_proposal* pr,
+                                float* seg_cdf, cudaStream_t st)
 {
-    k_proposal_cdf<<<sm_count() * 4, 128, 0, st>>>(segs, counters, pr->params, pr->node_desc, pr->mix, seg_cdf);
+    k_proposal_cdf<<<sm_count() * 4, 128, 0, st>>>(segs, seg_n, counters, pr->params, pr->node_desc, pr->mix,
+                                                    pr->count_eps, pr->count_min, seg_cdf);
     return cudaGetLastError();
 }
 
@@ -162,7 +178,13 @@ constexpr int SF        = PIN + 1;   // padded row strides of the per-warp stagi
 constexpr int SH        = PH + 1;
 constexpr int SB        = PBIN + 1;
 constexpr int PT_STAGE  = 32 * (SF + 4 * SH + SB);  // floats staged per warp
-constexpr int PT_PARTS  = PropOff::total + 3;       // gradient, loss sum, count, target entropy sum
+// gradient, then: cross-entropy sum, total variation weight, target entropy sum,
+// count-head squared error sum, count-head segments
+constexpr int PT_PARTS  = PropOff::total + 5;
+// the count head learns at this multiple of the proposal's learning rate (a
+// linear regression on the trunk's features, it has to follow the trunk and
+// the method's changing density within a few TRAIN steps)
+constexpr float HEAD_LR_SCALE = 10.0f;
 
 int proposal_grad_blocks() { return sm_count() * 2; }
 
@@ -171,9 +193,13 @@ int proposal_grad_blocks() { return sm_count() * 2; }
 // variation, so empty or flat space does not drown the segments that decide
 // the quadrature error): part[block][0 .. total) gradient sums, [total]
 // weighted cross-entropy sum, [total + 1] total weight, [total + 2] weighted
-// sum of the targets' entropies (cross-entropy - entropy = KL to the targets).
+// sum of the targets' entropies (cross-entropy - entropy = KL to the targets),
+// [total + 3] the count head's sum of (v - y)^2 / 2 over the segments, y =
+// log(a + 1e-4) with a from k_seg_variation, and [total + 4] their number.
+// The count head's gradient (rows VW .. total) stops at the trunk's features.
 __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __restrict__ segs, const int64_t* counters,
                                                                const float* __restrict__ seg_hist,
+                                                               const float* __restrict__ seg_tv,
                                                                const float* __restrict__ params,
                                                                const float* __restrict__ node_desc, float mix, int it,
                                                                float* __restrict__ part)
@@ -198,7 +224,8 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
 
     // accumulators owned by this lane (hidden unit j = lane)
     float gW1[PIN - 1] = {}, gb1 = 0.0f, gW2[PH] = {}, gb2 = 0.0f, gW3[PBIN] = {}, gb3 = 0.0f;
-    float lsum = 0.0f, cnt = 0.0f, hsum = 0.0f;
+    float gWv = 0.0f, gUv = 0.0f, gbv = 0.0f;  // count head: Wv[lane], Uv[lane], bv (lane 0)
+    float lsum = 0.0f, cnt = 0.0f, hsum = 0.0f, vsum = 0.0f, vcnt = 0.0f;
 
     const int64_t n      = counters[0];
     const int64_t stride = n > PT_MAXSEG ? (n + PT_MAXSEG - 1) / PT_MAXSEG : 1;
@@ -208,8 +235,8 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
     for (int64_t base = ((int64_t)blockIdx.x * PT_WARPS + w) * 32; base < nsub; base += nwarps * 32)
     {
         const int64_t k = base + lane;
-        float f[PIN], q[PBIN], mass = 0.0f;
-        bool use = false;
+        float f[PIN], q[PBIN], mass = 0.0f, vy = 0.0f;
+        bool use = false, valid = false;
 #pragma unroll
         for (int i = 0; i < PIN; ++i) f[i] = 0.0f;
 #pragma unroll
@@ -236,10 +263,13 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
                 v[b - 1] += dm;
                 tv += dm;
             }
-            use = tv > 1e-20f;
+            use            = tv > 1e-20f;
+            const float sv = seg_tv[r.rm];  // the count head's target: log(a + 1e-4)
+            valid          = sv >= 0.0f;
+            vy             = logf(sv + 1e-4f);
+            proposal_features(r, node_desc, f);
             if (use)
             {
-                proposal_features(r, node_desc, f);
                 const float inv = 0.5f / tv;
 #pragma unroll
                 for (int b = 0; b < PBIN; ++b) q[b] = v[b] * inv;
@@ -271,6 +301,21 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
             const float sg = prop_sigmoid(z);
             mh2[kk]        = z * sg;
             md2[kk]        = sg * (1.0f + z * (1.0f - sg));
+        }
+        // count head on the trunk's h2 and the inputs: v, and dv = v - y
+        {
+            float vh = P[PropOff::VB];
+#pragma unroll
+            for (int i = 0; i < PIN; ++i) vh = fmaf(P[PropOff::VU + i], f[i], vh);
+#pragma unroll 4
+            for (int kk = 0; kk < PH; ++kk) vh = fmaf(P[PropOff::VW + kk], mh2[kk], vh);
+            const float dv = valid ? vh - vy : 0.0f;
+            if (valid)
+            {
+                vsum = fmaf(0.5f * dv, dv, vsum);
+                vcnt += 1.0f;
+            }
+            sdz3[lane * SB + PBIN] = dv;
         }
         float sm[PBIN], mxz = -3.0e38f;
 #pragma unroll
@@ -352,6 +397,10 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
 #pragma unroll
             for (int b = 0; b < PBIN; ++b) gW3[b] = fmaf(sdz3[s2 * SB + b], hh, gW3[b]);
             if (lane < PBIN) gb3 += sdz3[s2 * SB + lane];
+            const float dv = sdz3[s2 * SB + PBIN];
+            gWv            = fmaf(dv, hh, gWv);
+            if (lane < PIN) gUv = fmaf(dv, sf[s2 * SF + lane], gUv);
+            gbv += dv;
         }
         __syncwarp();
     }
@@ -370,19 +419,26 @@ __global__ void __launch_bounds__(32 * PT_WARPS) k_prop_grad(const SegRec* __res
 #pragma unroll
     for (int b = 0; b < PBIN; ++b) rw[PropOff::W3 + b * PH + lane] = gW3[b];
     if (lane < PBIN) rw[PropOff::b3 + lane] = gb3;
-    float ls = lsum, cn = cnt, hs = hsum;
+    rw[PropOff::VW + lane] = gWv;
+    if (lane < PIN) rw[PropOff::VU + lane] = gUv;
+    if (lane == 0) rw[PropOff::VB] = gbv;
+    float ls = lsum, cn = cnt, hs = hsum, vs = vsum, vc = vcnt;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
     {
         ls += __shfl_xor_sync(0xffffffffu, ls, o);
         cn += __shfl_xor_sync(0xffffffffu, cn, o);
         hs += __shfl_xor_sync(0xffffffffu, hs, o);
+        vs += __shfl_xor_sync(0xffffffffu, vs, o);
+        vc += __shfl_xor_sync(0xffffffffu, vc, o);
     }
     if (lane == 0)
     {
         rw[PropOff::total]     = ls;
         rw[PropOff::total + 1] = cn;
         rw[PropOff::total + 2] = hs;
+        rw[PropOff::total + 3] = vs;
+        rw[PropOff::total + 4] = vc;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < PT_PARTS; i += blockDim.x)
@@ -405,65 +461,110 @@ __global__ void k_prop_begin(int* counter, float lr, float b1, float b2, float* 
     scal[1]      = (float)sqrt(bc2);
 }
 
-// Reduce the block partials, normalise by the number of segments used, Adam.
-// A block takes 32 parameters (one per lane, so each partial row is read
-// coalesced); its 8 warps split the partial rows (warp w: rows w, w + 8, ..)
-// and their sums are added in warp order: a fixed association, the same
-// every call.  Every block forms the segment count the same way.
+// Reduce the block partials, normalise, Adam.  The trunk and placement head
+// are normalised by the total variation weight, the count head by its number
+// of segments (and steps HEAD_LR_SCALE times as far).  A block takes 32
+// parameters (one per lane, so each partial row is read coalesced); its 8
+// warps split the partial rows (warp w: rows w, w + 8, ..) and their sums are
+// added in warp order: a fixed association, the same every call.  Every block
+// forms the normalisers the same way.
 constexpr int PA_WARPS = 8;
 __global__ void __launch_bounds__(32 * PA_WARPS)
     k_prop_adam(const float* __restrict__ part, int nblocks, const float* __restrict__ scal, neat_proposal pr)
 {
-    __shared__ float red[PA_WARPS][35];  // 32 parameter sums, count, loss sum, target-entropy sum
+    constexpr int NS = 5;                 // cross-entropy, weight, target entropy, head error, head count
+    __shared__ float red[PA_WARPS][32 + NS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int i    = blockIdx.x * 32 + lane;
-    float g = 0.0f, cnt = 0.0f, ls = 0.0f, hs = 0.0f;
+    float g = 0.0f, x[NS] = {};
     for (int b = w; b < nblocks; b += PA_WARPS)
     {
         const float* pb = part + (int64_t)b * PT_PARTS;
         if (i < PropOff::total) g += pb[i];
         if (lane == 0)
         {
-            ls += pb[PropOff::total];
-            cnt += pb[PropOff::total + 1];
-            hs += pb[PropOff::total + 2];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) x[q] += pb[PropOff::total + q];
         }
     }
     red[w][lane] = g;
     if (lane == 0)
     {
-        red[w][32] = cnt;
-        red[w][33] = ls;
-        red[w][34] = hs;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) red[w][32 + q] = x[q];
     }
     __syncthreads();
     if (w != 0 || i >= PropOff::total) return;
-    g = cnt = ls = hs = 0.0f;
+    g = 0.0f;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) x[q] = 0.0f;
 #pragma unroll
     for (int k = 0; k < PA_WARPS; ++k)
     {
         g += red[k][lane];
-        cnt += red[k][32];
-        ls += red[k][33];
-        hs += red[k][34];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) x[q] += red[k][32 + q];
     }
-    g          = cnt > 0.0f ? g / cnt : 0.0f;
-    pr.grad[i] = g;
+    const float ls = x[0], cnt = x[1], hs = x[2], vs = x[3], vc = x[4];
+    const bool head = i >= PropOff::VW;
+    const float nrm = head ? vc : cnt;
+    g               = nrm > 0.0f ? g / nrm : 0.0f;
+    pr.grad[i]      = g;
     if (i == 0 && pr.loss)
     {
         pr.loss[0] = cnt > 0.0f ? ls / cnt : 0.0f;
         pr.loss[1] = cnt > 0.0f ? hs / cnt : 0.0f;
+        pr.loss[2] = vc > 0.0f ? vs / vc : 0.0f;
     }
     float m = pr.m[i], v = pr.v[i];
     m       = fmaf(1.0f - pr.beta1, g, m * pr.beta1);
     v       = fmaf((1.0f - pr.beta2) * g, g, v * pr.beta2);
     pr.m[i] = m;
     pr.v[i] = v;
-    pr.params[i] = fmaf(-scal[0], m / (sqrtf(v) / scal[1] + pr.eps), pr.params[i]);
+    const float lr = head ? HEAD_LR_SCALE * scal[0] : scal[0];
+    pr.params[i]   = fmaf(-lr, m / (sqrtf(v) / scal[1] + pr.eps), pr.params[i]);
+}
+
+// One thread a node-major segment: a = (tmax - tmin) sum_j |rho_j - rho_j-1|
+// over its consecutive samples.  The midpoint rule with n samples misses
+// about a / (2 n) of the segment's integral at density jumps, so a is what
+// the count head predicts (as log(a + 1e-4)).
+__global__ void k_seg_variation(const SegRec* __restrict__ segs, const int* __restrict__ samp_off,
+                                const int64_t* counters, const float* __restrict__ seg_dens, int64_t dens_cap,
+                                float* __restrict__ seg_tv)
+{
+    const int64_t n = counters[0];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        const SegRec& r = segs[i];
+        const int64_t o = samp_off[i];
+        float tv        = -1.0f;
+        if (o + r.n <= dens_cap)
+        {
+            tv          = 0.0f;
+            float prev  = seg_dens[o];
+            for (int j = 1; j < r.n; ++j)
+            {
+                const float x = seg_dens[o + j];
+                tv += fabsf(x - prev);
+                prev = x;
+            }
+            tv = (r.tmax - r.tmin) * tv;
+        }
+        seg_tv[r.rm] = tv;
+    }
+}
+
+cudaError_t launch_seg_variation(const SegRec* segs, const int* samp_off, const int64_t* counters,
+                                 const float* seg_dens, int64_t dens_cap, float* seg_tv, cudaStream_t st)
+{
+    k_seg_variation<<<sm_count() * 8, 128, 0, st>>>(segs, samp_off, counters, seg_dens, dens_cap, seg_tv);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_proposal_train(const SegRec* segs, const int64_t* counters, const float* seg_hist,
-                                  const neat_proposal* pr, float* part, int iters, cudaStream_t st)
+                                  const float* seg_tv, const neat_proposal* pr, float* part, int iters,
+                                  cudaStream_t st)
 {
     const int nb      = proposal_grad_blocks();
     static_assert(PT_STAGE >= PT_PARTS, "reduction area must fit the staging area of a warp");
@@ -477,8 +578,8 @@ cudaError_t launch_proposal_train(const SegRec* segs, const int64_t* counters, c
     float* scal = part + (size_t)nb * PT_PARTS;
     for (int it = 0; it < iters; ++it)
     {
-        k_prop_grad<<<nb, 32 * PT_WARPS, smem, st>>>(segs, counters, seg_hist, pr->params, pr->node_desc, pr->mix,
-                                                     it, part);
+        k_prop_grad<<<nb, 32 * PT_WARPS, smem, st>>>(segs, counters, seg_hist, seg_tv, pr->params, pr->node_desc,
+                                                     pr->mix, it, part);
         k_prop_begin<<<1, 32, 0, st>>>(pr->step_counter, pr->lr, pr->beta1, pr->beta2, scal);
         k_prop_adam<<<(PropOff::total + 31) / 32, 32 * PA_WARPS, 0, st>>>(part, nb, scal, *pr);
     }

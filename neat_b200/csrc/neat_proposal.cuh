@@ -32,8 +32,28 @@ struct PropOff
     static constexpr int b2    = W2 + PH * PH;
     static constexpr int W3    = b2 + PH;
     static constexpr int b3    = W3 + PBIN * PH;
-    static constexpr int total = b3 + PBIN;
+    // count head: v = bv + Wv . h2 + Uv . f, a prediction of log(a + 1e-4),
+    // a = (tmax - tmin) times the total variation of the density along the
+    // segment, trained by regression on the trunk's features (the trunk gets
+    // no gradient from it)
+    static constexpr int VW    = b3 + PBIN;
+    static constexpr int VU    = VW + PH;
+    static constexpr int VB    = VU + PIN;
+    static constexpr int total = VB + 1;
 };
+
+// Samples of a segment under the count head's prediction v: the midpoint
+// rule with n samples misses about a / (2 n) of the segment's integral at
+// density jumps, so n = ceil(exp(v) / eps) keeps that near eps / 2; clamped to
+// [min(nmin, n_ref), n_ref] (n_ref: the reference's count at the budget).
+// eps <= 0 keeps n_ref.
+__device__ __forceinline__ int proposal_count(float v, int n_ref, float eps, int nmin)
+{
+    if (!(eps > 0.0f)) return n_ref;
+    const float x = fminf(expf(v) / eps, (float)n_ref);  // NaN v: fminf keeps n_ref
+    const int n   = max((int)ceilf(x), min(nmin, n_ref));
+    return min(n, n_ref);
+}
 
 __device__ __forceinline__ float prop_sigmoid(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 
@@ -124,12 +144,21 @@ __device__ __forceinline__ void proposal_forward(const float* __restrict__ P, co
 // proposal_forward for two segments at once in packed f32x2 arithmetic (each
 // lane rounds as fmaf does, so each segment's result is proposal_forward's):
 // half the FMA instructions, the weight loads shared.
+// Also the count head's v of both segments (v0, v1).
 __device__ __forceinline__ void proposal_forward2(const float* __restrict__ P, const float f0[PIN],
-                                                  const float f1[PIN], float mix, float p0[PBIN], float p1[PBIN])
+                                                  const float f1[PIN], float mix, float p0[PBIN], float p1[PBIN],
+                                                  float& v0, float& v1)
 {
     float2 F[PIN];
 #pragma unroll
     for (int i = 0; i < PIN; ++i) F[i] = make_float2(f0[i], f1[i]);
+    float2 vh = make_float2(P[PropOff::VB], P[PropOff::VB]);
+#pragma unroll
+    for (int i = 0; i < PIN; ++i)
+    {
+        const float u = P[PropOff::VU + i];
+        vh            = __ffma2_rn(make_float2(u, u), F[i], vh);
+    }
     float2 h1[PH];
 #pragma unroll
     for (int j = 0; j < PH; ++j)
@@ -171,7 +200,11 @@ __device__ __forceinline__ void proposal_forward2(const float* __restrict__ P, c
             const float w = P[PropOff::W3 + b * PH + k];
             z3[b]         = __ffma2_rn(make_float2(w, w), h2, z3[b]);
         }
+        const float wv = P[PropOff::VW + k];
+        vh             = __ffma2_rn(make_float2(wv, wv), h2, vh);
     }
+    v0 = vh.x;
+    v1 = vh.y;
     float mx0 = -3.0e38f, mx1 = -3.0e38f;
 #pragma unroll
     for (int b = 0; b < PBIN; ++b)

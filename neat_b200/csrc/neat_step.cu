@@ -635,11 +635,11 @@ struct StepLayout
     {
         ORIGIN, DIRECTION, RAY_NSEG, RAY_SEG_OFF, NODE_NSEG, NODE_SEG_OFF, RAY_HITS, SEGS, SEG_N,
         SAMP_OFF, TILE_SEG, PARTIAL, DPRED, LOSS_PART, DEC_PART, SCAN_SCRATCH, SCAL, SEG_CDF, SEG_HIST,
-        PROP_PART, SEG_PGRAD, RAY_PGRAD, REC, NUM
+        SEG_DENS, SEG_TV, PROP_PART, SEG_PGRAD, RAY_PGRAD, REC, NUM
     };
     size_t off[NUM];
     size_t total;
-    int64_t tiles_cap, sample_cap, rec_cap;
+    int64_t tiles_cap, sample_cap, rec_cap, dens_cap;
     int loss_blocks, bwd_grid, cap_ray;
 };
 
@@ -657,6 +657,9 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
                                 : d->record_samples_per_ray < 0 ? 0
                                                                 : d->record_samples_per_ray;
     L.rec_cap = std::min<int64_t>(L.sample_cap, std::max<int64_t>(R, 1) * rec_per_ray);
+    // proposal TRAIN steps: the densities of up to 4 (M + 1) samples a ray (a
+    // step with more trains the count head on the segments inside that room)
+    L.dens_cap = d->proposal ? std::min<int64_t>(L.sample_cap, std::max<int64_t>(R, 1) * (M + 1) * 4) : 0;
     L.loss_blocks     = (int)((R + 255) / 256);
     size_t smem       = 0;
     L.bwd_grid        = d->decoder_path == NEAT_DECODER_SIMT_FP32
@@ -671,7 +674,8 @@ static bool step_layout(const neat_step_desc* d, int64_t R, StepLayout& L)
         (size_t)(cap + 1) * 4,
         (size_t)L.tiles_cap * 4, (size_t)cap * 8, (size_t)R * 4, (size_t)L.loss_blocks * 4,
         (size_t)L.bwd_grid * P * 4, (size_t)scan_scratch_elems(scan_max) * 4, sizeof(StepScalars),
-        d->proposal ? (size_t)cap * 8 * 4 : 0, d->proposal ? (size_t)cap * 8 * 4 : 0,
+        d->proposal ? (size_t)cap * 8 * 4 : 0, d->proposal ? (size_t)cap * 8 * 4 : 0, (size_t)L.dens_cap * 4,
+        d->proposal ? (size_t)cap * 4 : 0,
         d->proposal ? proposal_part_floats() * 4 : 0, d->pose_grad ? (size_t)cap * 6 * 4 : 0,
         d->pose_grad ? (size_t)R * 6 * 4 : 0,
         d->decoder_path != NEAT_DECODER_SIMT_FP32 ? (size_t)L.rec_cap * (8 + d->C) * 4 : 0};
@@ -758,7 +762,7 @@ struct StepBufs
     float *dpred, *loss_part, *dec_part;
     int* scratch;
     StepScalars* scal;
-    float *seg_cdf, *seg_hist, *prop_part;
+    float *seg_cdf, *seg_hist, *seg_dens, *seg_tv, *prop_part;
     float *seg_pgrad, *ray_pgrad;
     float* rec;
 };
@@ -787,6 +791,8 @@ static StepBufs step_bufs(const StepLayout& L, void* workspace)
     w.scal         = (StepScalars*)P_(StepLayout::SCAL);
     w.seg_cdf      = (float*)P_(StepLayout::SEG_CDF);
     w.seg_hist     = (float*)P_(StepLayout::SEG_HIST);
+    w.seg_dens     = (float*)P_(StepLayout::SEG_DENS);
+    w.seg_tv       = (float*)P_(StepLayout::SEG_TV);
     w.prop_part    = (float*)P_(StepLayout::PROP_PART);
     w.seg_pgrad    = (float*)P_(StepLayout::SEG_PGRAD);
     w.ray_pgrad    = (float*)P_(StepLayout::RAY_PGRAD);
@@ -814,8 +820,10 @@ static int check_desc(const neat_step_desc* d, const neat_step_batch* b)
 
 // Rays -> per-ray hit lists -> node-major segments -> sample offsets -> tile
 // map (phases 0..1 of the step).  counters[0..3] and *status are written.
+// pr != nullptr (a SAMPLE step of the learned proposal): the CDF of every
+// segment, and its sample count from the count head, before the sample offsets.
 static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, const StepLayout& L, const StepBufs& w,
-                           int64_t* cnt, int* status, cudaStream_t st)
+                           int64_t* cnt, int* status, cudaStream_t st, const neat_proposal* pr = nullptr)
 {
     const int64_t R = b->num_rays, cap = d->seg_capacity;
     const int A = d->num_active, D = d->max_depth, M = d->max_samples_per_node;
@@ -831,6 +839,7 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
     ok = ok && launch_step_place(w.ray_hits, w.ray_nseg, w.ray_seg_off, R, L.cap_ray, w.node_seg_off, w.segs,
                                  w.seg_n, cnt + 0, cap, st) == cudaSuccess;
     k_zero_partial<<<sm_count() * 4, 256, 0, st>>>(w.partial, cnt);
+    if (pr) ok = ok && launch_proposal_cdf(w.segs, w.seg_n, cnt, pr, w.seg_cdf, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.seg_n, cnt + 0, cap, w.samp_off, w.scratch, cnt + 1, st) == cudaSuccess;
     k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, status);
     k_tile_seg<<<(unsigned)std::min<int64_t>((cap + 255) / 256, (int64_t)sm_count() * 8), 256, 0, st>>>(
@@ -863,6 +872,8 @@ static StepTileArgs tile_args(const neat_step_desc* d, const StepBufs& w, const 
     ta.step_dev  = &w.scal->step;
     ta.seg_cdf   = nullptr;
     ta.seg_hist  = nullptr;
+    ta.seg_dens  = nullptr;
+    ta.dens_cap  = 0;
     ta.seg_pgrad = nullptr;
     ta.rec       = nullptr;
     ta.rec_cap   = 0;
@@ -957,7 +968,8 @@ static bool proposal_mode(const neat_step_desc* d, const neat_proposal* pr, int&
     if (!d->proposal || d->decoder_path == NEAT_DECODER_SIMT_FP32 || !pr->params || !pr->node_desc) return false;
     if (mode == NEAT_PROPOSAL_TRAIN && (!pr->m || !pr->v || !pr->grad || !pr->step_counter || pr->iters < 0))
         return false;
-    return pr->mix >= 0.0f && pr->mix <= 1.0f;
+    if (pr->count_eps > 0.0f && pr->count_min < 1) return false;
+    return pr->mix >= 0.0f && pr->mix <= 1.0f && !(pr->count_eps < 0.0f) && pr->count_eps == pr->count_eps;
 }
 
 }  // namespace neat
@@ -1002,7 +1014,7 @@ static int train_step(const neat_step_desc* d, const neat_step_state* s, const n
     phase(0);
     k_step_begin<<<1, 32, 0, st>>>(s->step_counter, step, (double)d->lr_grid, (double)d->lr_decoder,
                                    (double)d->beta1, (double)d->beta2, w.scal);
-    if (!prebuilt) ok = build_segments(d, b, L, w, cnt, out->status, st);
+    if (!prebuilt) ok = build_segments(d, b, L, w, cnt, out->status, st, pmode == NEAT_PROPOSAL_SAMPLE ? pr : nullptr);
     phase(1);
 
     StepTileArgs ta = tile_args(d, w, s->grid, s->grid_grad, s->decoder, cnt, out->status, seed, step, 1);
@@ -1012,19 +1024,19 @@ static int train_step(const neat_step_desc* d, const neat_step_state* s, const n
         ta.rec     = L.rec_cap > 0 ? w.rec : nullptr;
         ta.rec_cap = L.rec_cap;
     }
-    if (pmode == NEAT_PROPOSAL_SAMPLE)
-    {
-        // (prebuilt: neat_train_step_segments has placed the CDF with the lists)
-        if (!prebuilt) ok = ok && launch_proposal_cdf(w.segs, cnt, pr, w.seg_cdf, st) == cudaSuccess;
-        ta.seg_cdf = w.seg_cdf;
-    }
+    if (pmode == NEAT_PROPOSAL_SAMPLE) ta.seg_cdf = w.seg_cdf;  // placed with the segment lists
     else if (pmode == NEAT_PROPOSAL_TRAIN)
     {
         k_zero_per_segment<<<sm_count() * 4, 256, 0, st>>>(w.seg_hist, cnt, 8);
         ta.seg_hist = w.seg_hist;
+        ta.seg_dens = w.seg_dens;
+        ta.dens_cap = L.dens_cap;
     }
     ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
     ta.seg_hist = nullptr;
+    ta.seg_dens = nullptr;
+    if (pmode == NEAT_PROPOSAL_TRAIN)
+        ok = ok && launch_seg_variation(w.segs, w.samp_off, cnt, w.seg_dens, L.dens_cap, w.seg_tv, st) == cudaSuccess;
     phase(2);
     const float invR = (float)(1.0 / (double)R);
     ToneMap tm{};
@@ -1071,7 +1083,8 @@ static int train_step(const neat_step_desc* d, const neat_step_state* s, const n
     {
         ok = ok && launch_node_desc(s->grid, A, d->C, d->G, s->decoder, d->softplus_beta, pr->node_desc, st) ==
                        cudaSuccess;
-        ok = ok && launch_proposal_train(w.segs, cnt, w.seg_hist, pr, w.prop_part, pr->iters, st) == cudaSuccess;
+        ok = ok && launch_proposal_train(w.segs, cnt, w.seg_hist, w.seg_tv, pr, w.prop_part, pr->iters, st) ==
+                       cudaSuccess;
     }
     phase(5);
     ok = ok && cudaGetLastError() == cudaSuccess;
@@ -1105,11 +1118,10 @@ extern "C" int neat_train_step_segments(const neat_step_desc* d, const neat_prop
     if (!step_layout(d, b->num_rays, L) || workspace_bytes < L.total) return NEAT_ERR_CAPACITY;
     const StepBufs w = step_bufs(L, workspace);
     cudaStream_t st  = (cudaStream_t)stream;
-    bool ok          = build_segments(d, b, L, w, counters, status, st);
-    // a SAMPLE step's placement CDF depends on the segments and on the proposal's
-    // parameters and node descriptors, which only a TRAIN step's end changes
-    if (pmode == NEAT_PROPOSAL_SAMPLE)
-        ok = ok && launch_proposal_cdf(w.segs, counters, proposal, w.seg_cdf, st) == cudaSuccess;
+    // a SAMPLE step's placement CDF and sample counts depend on the segments and
+    // on the proposal's parameters and node descriptors, which only a TRAIN
+    // step's end changes
+    bool ok = build_segments(d, b, L, w, counters, status, st, pmode == NEAT_PROPOSAL_SAMPLE ? proposal : nullptr);
     return ok && cudaGetLastError() == cudaSuccess ? NEAT_OK : NEAT_ERR_CUDA;
 }
 
@@ -1132,13 +1144,9 @@ extern "C" int neat_project(const neat_step_desc* d, const float* grid, const fl
     const StepBufs w = step_bufs(L, workspace);
     int64_t* cnt     = out->counters;
     k_step_begin<<<1, 32, 0, st>>>(nullptr, 1, 0.0, 0.0, 0.5, 0.5, w.scal);
-    bool ok               = build_segments(d, b, L, w, cnt, out->status, st);
+    bool ok = build_segments(d, b, L, w, cnt, out->status, st, pmode == NEAT_PROPOSAL_SAMPLE ? proposal : nullptr);
     StepTileArgs ta = tile_args(d, w, grid, nullptr, decoder, cnt, out->status, 0, 1, 0);
-    if (pmode == NEAT_PROPOSAL_SAMPLE)
-    {
-        ok         = ok && launch_proposal_cdf(w.segs, cnt, proposal, w.seg_cdf, st) == cudaSuccess;
-        ta.seg_cdf = w.seg_cdf;
-    }
+    if (pmode == NEAT_PROPOSAL_SAMPLE) ta.seg_cdf = w.seg_cdf;
     ok = ok && launch_tiles_path(d, false, ta, st) == cudaSuccess;
     // the loss-partials slab holds L.loss_blocks floats; the error sums need two
     // doubles per block, which the (larger) dpred slab of R floats provides

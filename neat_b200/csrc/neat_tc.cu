@@ -736,6 +736,8 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                 const float c   = vld ? softplusf_(y, a.beta) * qd[s] : 0.0f;
                 // proposal targets: contribution mass per eighth of the segment
                 if (a.seg_hist && vld) atomicAdd(a.seg_hist + 8 * (int64_t)rm + min(7, (int)(qd[128 + s] * 8.0f)), c);
+                // .. and each sample's density (the count head's variation target)
+                if (a.seg_dens && vld && tile * 128 + s < a.dens_cap) a.seg_dens[tile * 128 + s] = softplusf_(y, a.beta);
                 double v = (double)c;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1)
@@ -1007,6 +1009,9 @@ __global__ void __launch_bounds__(TcThreads<PREC, BWD>::value, TcThreads<PREC, B
                     const float c = q.valid ? softplusf_(y, a.beta) * q.weight : 0.0f;
                     // proposal targets: contribution mass per eighth of the segment
                     if (a.seg_hist && q.valid) atomicAdd(a.seg_hist + 8 * (int64_t)q.rm + min(7, (int)(q.u * 8.0f)), c);
+                    // .. and each sample's density (the count head's variation target)
+                    if (a.seg_dens && q.valid && tile * 128 + s < a.dens_cap)
+                        a.seg_dens[tile * 128 + s] = softplusf_(y, a.beta);
                     const int seg = cur.seg;
                     double v      = (double)c;
 #pragma unroll

@@ -25,7 +25,7 @@ class FusedTrainer:
                  max_samples_per_node=32, lr_grid=1e-2, lr_decoder=5e-5, softplus_beta=2.0, seed=0, grid=None,
                  decoder=None, seg_capacity_per_ray=None, decoder_path=_lib.NEAT_DECODER_TC_BF16X3, device="cuda",
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=10,
-                 proposal_mix=0.25, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
+                 proposal_mix=0.25, proposal_count_eps=0.0, proposal_count_min=2, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
                  tonemap=None, pose_grad=False, optimize_pose=False, optimize_intrinsics=False, lr_pose=1e-3,
                  lr_intrinsics=100.0, record_samples_per_ray=0):
         self.dev = torch.device(device)
@@ -108,9 +108,11 @@ class FusedTrainer:
             self.grid_bf16 = self.grid.to(torch.bfloat16).contiguous()
             self.state.grid_bf16 = self.grid_bf16.data_ptr()
         # learned sample proposal: SAMPLE-mode steps place proposal_budget samples per
-        # node segment by the proposal's CDF; every proposal_every-th step (the first
-        # included) samples uniformly with max_samples_per_node, bins the
-        # contributions and trains the proposal on them
+        # node segment by the proposal's CDF (with proposal_count_eps > 0: fewer,
+        # down to proposal_count_min, where the count head predicts little density
+        # variation); every proposal_every-th step (the first included) samples
+        # uniformly with max_samples_per_node, bins the contributions and trains
+        # the proposal on them
         self.proposal = bool(proposal)
         self.desc.proposal = 1 if self.proposal else 0
         if self.proposal:
@@ -121,14 +123,16 @@ class FusedTrainer:
             self.prop_v = torch.zeros_like(self.prop)
             self.prop_grad = torch.zeros_like(self.prop)
             self.prop_steps = torch.zeros(1, dtype=torch.int32, device=self.dev)
-            self.prop_loss = torch.zeros(2, dtype=torch.float32, device=self.dev)  # cross-entropy, target entropy
+            # cross-entropy, target entropy, count head's mean squared error / 2
+            self.prop_loss = torch.zeros(3, dtype=torch.float32, device=self.dev)
             self.prop_node_desc = torch.zeros((A, 6), dtype=torch.float32, device=self.dev)
             self.prop_every = int(proposal_every)
             self.prop_struct = _lib.Proposal(
                 mode=_lib.NEAT_PROPOSAL_OFF, params=self.prop.data_ptr(), m=self.prop_m.data_ptr(),
                 v=self.prop_v.data_ptr(), grad=self.prop_grad.data_ptr(), step_counter=self.prop_steps.data_ptr(),
                 loss=self.prop_loss.data_ptr(), lr=float(proposal_lr), beta1=0.9, beta2=0.999, eps=1e-8,
-                mix=float(proposal_mix), iters=int(proposal_iters), node_desc=self.prop_node_desc.data_ptr())
+                mix=float(proposal_mix), iters=int(proposal_iters), node_desc=self.prop_node_desc.data_ptr(),
+                count_eps=float(proposal_count_eps), count_min=int(proposal_count_min))
             self.state.proposal = ctypes.addressof(self.prop_struct)
             self.desc_budget = _lib.StepDesc.from_buffer_copy(self.desc)
             self.desc_budget.max_samples_per_node = int(proposal_budget)

@@ -494,6 +494,8 @@ def quat_exp_mul_f64(tangent, q):
 # learned sample proposal (restatement of neat_b200/csrc/neat_proposal.cuh)
 # --------------------------------------------------------------------------
 PROP_IN, PROP_H, PROP_B = 16, 32, 8
+PROP_TRUNK = PROP_H * PROP_IN + PROP_H + PROP_H * PROP_H + PROP_H + PROP_B * PROP_H + PROP_B
+PROP_TOTAL = PROP_TRUNK + PROP_H + PROP_IN + 1  # then the count head Wv [32] | Uv [16] | bv
 JITTER_STREAM = 0x4a495454
 
 
@@ -545,15 +547,42 @@ def proposal_features(o, d, segs, pmin, pmax, node_desc, prefix):
     return f
 
 
-def proposal_probs_f64(torch, params, f, mix):
-    """Mixed bin probabilities p = (1 - mix) softmax(MLP(f)) + mix / 8, f64."""
+def _proposal_trunk_f64(torch, params, f):
     H, I, B = PROP_H, PROP_IN, PROP_B
-    W1, b1, W2, b2, W3, b3 = torch.split(params, [H * I, H, H * H, H, B * H, B])
+    W1, b1, W2, b2, W3, b3, Wv, Uv, bv = torch.split(params, [H * I, H, H * H, H, B * H, B, H, I, 1])
     x = torch.as_tensor(f, dtype=torch.float64)
     h1 = torch.nn.functional.silu(x @ W1.reshape(H, I).T + b1)
     h2 = torch.nn.functional.silu(h1 @ W2.reshape(H, H).T + b2)
-    z = h2 @ W3.reshape(B, H).T + b3
-    return (1 - mix) * torch.softmax(z, 1) + mix / B
+    return x, h2, (W3, b3, Wv, Uv, bv)
+
+
+def proposal_probs_f64(torch, params, f, mix):
+    """Mixed bin probabilities p = (1 - mix) softmax(MLP(f)) + mix / 8, f64."""
+    _, h2, (W3, b3, _, _, _) = _proposal_trunk_f64(torch, params, f)
+    z = h2 @ W3.reshape(PROP_B, PROP_H).T + b3
+    return (1 - mix) * torch.softmax(z, 1) + mix / PROP_B
+
+
+def proposal_head_f64(torch, params, f, detach_trunk=False):
+    """The count head v = bv + Wv . h2 + Uv . f (neat_proposal.cuh: PropOff::VW),
+    a prediction of log(a + 1e-4), f64; detach_trunk: no gradient into h2."""
+    x, h2, (_, _, Wv, Uv, bv) = _proposal_trunk_f64(torch, params, f)
+    if detach_trunk:
+        h2 = h2.detach()
+    return h2 @ Wv + x @ Uv + bv
+
+
+def proposal_counts(v, n_ref, eps, nmin):
+    """Samples a segment gets from the count head (neat_proposal.cuh:
+    proposal_count): min(n_ref, max(min(nmin, n_ref), ceil(exp(v) / eps))),
+    n_ref where eps <= 0; also the unrounded exp(v) / eps (for callers that
+    set aside counts within rounding of an integer)."""
+    n_ref = np.asarray(n_ref, np.int64)
+    if eps <= 0:
+        return n_ref.copy(), np.full(n_ref.shape, np.inf)
+    x = np.minimum(np.exp(np.asarray(v, np.float64)) / eps, n_ref)
+    n = np.maximum(np.ceil(x).astype(np.int64), np.minimum(nmin, n_ref))
+    return np.minimum(n, n_ref), x
 
 
 def proposal_inverse(c, u):
@@ -567,16 +596,21 @@ def proposal_inverse(c, u):
     return (b + np.clip(fr, 0.0, 1.0)) / PROP_B
 
 
-def sample_offsets(segs, jitter, seed, step):
+def sample_offsets(segs, jitter, seed, step, n_key=None):
     """Per sample of the segments (segment-major, j inside): segment index, j,
-    stratified offset a (Philox jitter stream or 0.5) and u = (j + a) / n in f32."""
+    stratified offset a (Philox jitter stream or 0.5) and u = (j + a) / n in f32.
+    The jitter is keyed on the index in the ray of the segment's first sample
+    under the counts n_key (default: the segments' own counts; the count head's
+    counts keep the keys of the reference's counts)."""
     n = segs["n"].astype(np.int64)
     sid = np.repeat(np.arange(n.shape[0]), n)
     start = np.concatenate([[0], np.cumsum(n)[:-1]])
     j = np.arange(sid.shape[0]) - start[sid]
     # index in the ray of each segment's first sample (segments are ray-major)
+    nk = n if n_key is None else np.asarray(n_key, np.int64)
+    kstart = np.concatenate([[0], np.cumsum(nk)[:-1]])
     first = np.concatenate([[0], np.cumsum(segs["ray_nseg"].astype(np.int64))[:-1]])
-    base = start - start[first[segs["ray"]]]
+    base = kstart - kstart[first[segs["ray"]]]
     if jitter:
         a = np.array([uniform(seed, int(segs["ray"][s]), int(base[s] + jj), step, JITTER_STREAM)
                       for s, jj in zip(sid, j)], np.float32)
@@ -586,11 +620,11 @@ def sample_offsets(segs, jitter, seed, step):
     return sid, j, a, u.astype(np.float32)
 
 
-def proposal_samples(o, d, segs, cdf, jitter, seed=0, step=1):
+def proposal_samples(o, d, segs, cdf, jitter, seed=0, step=1, n_key=None):
     """Samples placed by the proposal CDF (one row of bin ends per segment):
     t = tmin + (tmax - tmin) F^-1((j + a) / n), midpoint-rule weights on the
     placed positions, f64.  Returns a SampleList-like dict for image_f64."""
-    sid, j, a, u = sample_offsets(segs, jitter, seed, step)
+    sid, j, a, u = sample_offsets(segs, jitter, seed, step, n_key)
     t0 = segs["tmin"].astype(np.float64)[sid]
     t1 = segs["tmax"].astype(np.float64)[sid]
     n = segs["n"][sid]
@@ -627,6 +661,28 @@ def proposal_targets(o, d, segs, M, grid, dec, node_min, node_max, prefix, jitte
     return hist
 
 
+def proposal_count_targets(o, d, segs, M, grid, dec, node_min, node_max, prefix, jitter, seed, step, beta=2.0):
+    """The count head's target argument per segment of a uniformly sampled
+    step (neat_proposal.cu: k_seg_variation): a = (tmax - tmin) times the total
+    variation sum_j |rho_j - rho_j-1| of its samples' densities, f64."""
+    import torch
+    s = create_samples(o, d, np.nonzero(prefix >= 0)[0], node_min, node_max, M, jitter, seed, step)
+    sid, j, _, _ = sample_offsets(segs, jitter, seed, step)
+    assert sid.shape[0] == s["ray_t"].shape[0]
+    g = torch.from_numpy(s["coords"]).double()
+    nid = torch.from_numpy(s["node_id"])
+    mn = torch.from_numpy(node_min).double()[nid]
+    mx = torch.from_numpy(node_max).double()[nid]
+    row = torch.from_numpy(prefix[s["node_id"]])
+    grid_t = torch.as_tensor(np.asarray(grid, np.float64))
+    feat = _trilinear_f64(torch, grid_t, row, (g - mn) / (mx - mn) * 2 - 1)
+    dens = decoder_f64(torch, feat, torch.as_tensor(np.asarray(dec, np.float64)), grid_t.shape[1], beta).numpy()
+    step_tv = np.where(j > 0, np.abs(dens - np.concatenate([[0.0], dens[:-1]])), 0.0)
+    tv = np.zeros(segs["n"].shape[0])
+    np.add.at(tv, sid, step_tv)
+    return (segs["tmax"].astype(np.float64) - segs["tmin"].astype(np.float64)) * tv
+
+
 def proposal_variation_targets(hist):
     """Binned masses m [Nseg, 8] -> (targets v / sum v with v_b = |m_b - m_b-1|
     + |m_b+1 - m_b|, total variation sum_b |m_b - m_b-1| as the segment's weight)."""
@@ -638,10 +694,14 @@ def proposal_variation_targets(hist):
     return v / np.where(tv > 0, 2 * tv, 1.0)[:, None], tv
 
 
-def proposal_grad_f64(params, f, hist, mix):
+def proposal_grad_f64(params, f, hist, mix, a=None):
     """Cross-entropy between the variation targets of the binned masses and the
     proposal, averaged over the segments weighted by their total variation,
-    and its gradient w.r.t. the packed parameters (f64)."""
+    and its gradient w.r.t. the trunk and placement head (f64).  With the
+    count targets a (proposal_count_targets; < 0: no target), also the count
+    head's loss mean((v - log(a + 1e-4))^2) / 2 over the segments and its
+    gradient w.r.t. the count head (the trunk held fixed): (ce, gradient,
+    head loss or None)."""
     import torch
     qv, tv = proposal_variation_targets(hist)
     use = tv > 1e-20
@@ -651,7 +711,19 @@ def proposal_grad_f64(params, f, hist, mix):
     p = proposal_probs_f64(torch, P, f[use], mix)
     loss = (-(q * torch.log(p)).sum(1) * m).sum() / m.sum()
     loss.backward()
-    return float(loss.detach()), P.grad.numpy()
+    grad = P.grad.numpy().copy()
+    grad[PROP_TRUNK:] = 0.0
+    if a is None:
+        return float(loss.detach()), grad, None
+    a = np.asarray(a, np.float64)
+    ok = a >= 0
+    P2 = torch.tensor(np.asarray(params, np.float64), requires_grad=True)
+    v = proposal_head_f64(torch, P2, f[ok], detach_trunk=True)
+    y = torch.from_numpy(np.log(a[ok] + 1e-4))
+    lh = 0.5 * ((v - y) ** 2).mean()
+    lh.backward()
+    grad[PROP_TRUNK:] = P2.grad.numpy()[PROP_TRUNK:]
+    return float(loss.detach()), grad, float(lh.detach())
 
 
 # --------------------------------------------------------------------------

@@ -484,6 +484,48 @@ def test_proposal_sampling_matches_f64(neat, oracle, case, path):
     assert err < PATHS[path][1]
 
 
+@pytest.mark.parametrize("path", ["bf16x3", "bf16"])
+def test_proposal_counts_match_f64(neat, oracle, case, path):
+    """Sample counts from the count head (count_eps 0.2, count_min 2, budget
+    8) and the samples placed with them, a = 0.5: the total sample count and
+    the projection against the f64 oracle that forms the same counts from the
+    same parameters.  A segment whose exp(v) / eps lies within 1e-4 of an
+    integer may round either way in f32; rays holding one are set aside (and
+    counted)."""
+    c = case
+    eps, nmin = 0.2, 2
+    tr = _prop_trainer(c, path, proposal_budget=8, proposal_count_eps=eps, proposal_count_min=nmin)
+    params = _random_proposal(tr)
+    pred = tr.project(_dev(c.uv), _dev(c.img), use_proposal=True)
+    torch.cuda.synchronize()
+    tr.check_status()
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    segs = oracle.ray_segments(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, 8)
+    f = oracle.proposal_features(o, d, segs, T.node_position_min, T.node_position_max, tr.prop_node_desc.cpu().numpy(),
+                                 T.node_active_prefix_sum)
+    P = torch.from_numpy(params)
+    v = oracle.proposal_head_f64(torch, P, f).numpy()
+    n, x = oracle.proposal_counts(v, segs["n"], eps, nmin)
+    amb = (np.abs(x - np.round(x)) < 1e-4) & (x > nmin) & (x < segs["n"])
+    p = oracle.proposal_probs_f64(torch, P, f, tr.prop_struct.mix).numpy()
+    cdf = np.cumsum(p, 1)
+    cdf[:, -1] = 1.0
+    s = oracle.proposal_samples(o, d, dict(segs, n=n), cdf, False, n_key=segs["n"])
+    ref = oracle.image_f64(s, torch.from_numpy(c.grid.astype(np.float64)), torch.from_numpy(c.dec.astype(np.float64)),
+                           T.node_position_min, T.node_position_max, T.node_active_prefix_sum, c.R).numpy()
+    keep = np.ones(c.R, bool)
+    keep[segs["ray"][amb]] = False
+    total = int(tr.counters[1].item())
+    print(path, "count head: samples", total, "of", int(segs["n"].sum()), "at the budget; ambiguous segments",
+          int(amb.sum()), "rays kept", int(keep.sum()))
+    assert abs(total - int(n.sum())) <= int(amb.sum())
+    assert total < 0.9 * int(segs["n"].sum())  # the head cuts counts on this case
+    err = _rel2(pred.cpu().numpy()[keep], ref[keep])
+    print(path, "proposal projection with learned counts, rel err", err)
+    assert err < PATHS[path][1]
+
+
 def test_proposal_training_gradient_matches_f64(neat, oracle, case):
     """A TRAIN step: uniform sampling, contributions binned per segment,
     one proposal iteration with lr 0 -> its gradient equals the f64 oracle's
@@ -503,12 +545,19 @@ def test_proposal_training_gradient_matches_f64(neat, oracle, case):
     nd = tr.prop_node_desc.cpu().numpy()
     nd_ref = oracle.node_descriptors_f64(tr.grid_reference_layout().cpu().numpy(), tr.decoder.cpu().numpy())
     np.testing.assert_allclose(nd, nd_ref, rtol=1e-4, atol=1e-4)
+    a = oracle.proposal_count_targets(o, d, segs, c.M, c.grid, c.dec, T.node_position_min, T.node_position_max,
+                                      T.node_active_prefix_sum, True, 99, 1)
     f = oracle.proposal_features(o, d, segs, T.node_position_min, T.node_position_max, nd, T.node_active_prefix_sum)
-    loss, g = oracle.proposal_grad_f64(params, f, hist, tr.prop_struct.mix)
+    loss, g, lh = oracle.proposal_grad_f64(params, f, hist, tr.prop_struct.mix, a)
     gg = tr.prop_grad.cpu().numpy()
-    print("proposal loss", float(tr.prop_loss[0].item()), loss, "grad rel err", _rel2(gg, g))
-    assert abs(float(tr.prop_loss[0].item()) - loss) <= 1e-4 * abs(loss)
+    tl = tr.prop_loss.cpu().numpy()
+    head = slice(oracle.PROP_TRUNK, None)
+    print("proposal loss", tl[0], loss, "grad rel err", _rel2(gg, g), "| count head loss", tl[2], lh,
+          "grad rel err", _rel2(gg[head], g[head]))
+    assert abs(float(tl[0]) - loss) <= 1e-4 * abs(loss)
+    assert abs(float(tl[2]) - lh) <= 1e-4 * abs(lh)
     assert _rel2(gg, g) < 1e-4
+    assert _rel2(gg[head], g[head]) < 1e-4
     np.testing.assert_array_equal(tr.prop.cpu().numpy(), params.astype(np.float32))  # lr 0
 
 
@@ -545,7 +594,7 @@ def test_proposal_gain_over_uniform(neat, oracle, case):
     torch.cuda.synchronize()
     tr.check_status()
     assert torch.equal(params, tr.prop)
-    ce, h = tr.prop_loss.cpu().numpy()
+    ce, h, _ = tr.prop_loss.cpu().numpy()
     uv, im = _dev(c.uv), _dev(c.img)
     p_prop = tr.project(uv, im, use_proposal=True).cpu().numpy().astype(np.float64)
     p_unif = tr.project(uv, im, samples_per_node=8).cpu().numpy().astype(np.float64)

@@ -354,17 +354,34 @@ def test_proposal_gradient_matches_finite_differences(oracle):
     training kernel is checked against) matches central differences."""
     import torch
     rng = np.random.default_rng(4)
-    P = rng.normal(0, 0.3, 1864)
+    P = rng.normal(0, 0.3, oracle.PROP_TOTAL)
     f = rng.uniform(-1, 1, (40, 16)).astype(np.float32)
     f[:, 13:] = 0
     hist = rng.uniform(0, 1, (40, 8)) * (rng.uniform(0, 1, (40, 1)) > 0.2)
-    loss, g = oracle.proposal_grad_f64(P, f, hist, 0.1)
-    for k in rng.choice(1864, 25, replace=False):
+    a = rng.uniform(0, 0.3, 40) * (rng.uniform(0, 1, 40) > 0.2)
+    a[3] = -1.0  # a segment without a count target
+    loss, g, lh = oracle.proposal_grad_f64(P, f, hist, 0.1, a)
+    trunk = rng.choice(oracle.PROP_TRUNK, 20, replace=False)
+    head = oracle.PROP_TRUNK + rng.choice(oracle.PROP_TOTAL - oracle.PROP_TRUNK, 10, replace=False)
+    for k in np.concatenate([trunk, head]):
         e = np.zeros_like(P)
         e[k] = 1e-6
-        lp, _ = oracle.proposal_grad_f64(P + e, f, hist, 0.1)
-        lm, _ = oracle.proposal_grad_f64(P - e, f, hist, 0.1)
-        assert abs((lp - lm) / 2e-6 - g[k]) <= 1e-6 + 1e-5 * abs(g[k])
+        lp, _, hp = oracle.proposal_grad_f64(P + e, f, hist, 0.1, a)
+        lm, _, hm = oracle.proposal_grad_f64(P - e, f, hist, 0.1, a)
+        fd = (lp - lm) / 2e-6 if k < oracle.PROP_TRUNK else (hp - hm) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(g[k])
+
+
+def test_proposal_counts_rule(oracle):
+    """The count head's rule: n_ref where eps <= 0; else
+    min(n_ref, max(min(nmin, n_ref), ceil(exp(v) / eps)))."""
+    v = np.log(np.array([0.05, 0.25, 0.31, 10.0, 1e-9, 0.2]))
+    n_ref = np.array([12, 12, 12, 12, 12, 1])
+    n, x = oracle.proposal_counts(v, n_ref, 0.1, 2)
+    np.testing.assert_array_equal(n, [2, 3, 4, 12, 2, 1])
+    np.testing.assert_allclose(x[:3], [0.5, 2.5, 3.1])
+    n0, _ = oracle.proposal_counts(v, n_ref, 0.0, 2)
+    np.testing.assert_array_equal(n0, n_ref)
 
 
 def test_pose_gradients_match_finite_differences(oracle):

@@ -309,6 +309,10 @@ def decoder_path(name):
 # midpoint rule then misses about eps / 2 of its integral at density jumps,
 # below the projections' Poisson noise at I0 = 1e4 (about 0.01)
 COUNT_EPS = 0.05
+# proposal lines are timed over one 50-step cycle after this many: the count
+# head's sample counts settle within about 1000 steps (3.4 M samples a step
+# over the first 100 steps of the race, 2.3 M from step 1000 on)
+PROPOSAL_WARM_CYCLES = 20
 
 
 def make_trainer(cfg, tree, cam, dev, decoder, proposal, seed):
@@ -366,7 +370,9 @@ def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
     decoder operands, FP32 accumulation) and the BF16 step with the learned
     proposal (budget 12 samples per segment, fewer where the count head
     predicts little variation; one full 50-step cycle, its uniform TRAIN step
-    included, after two cycles that train the proposal), CUDA events around
+    included, after 20 cycles that train the proposal and its count head to
+    their steady state; the race below covers training from the start), CUDA
+    events around
     each timed loop; the BF16 + proposal step against both FP32 steps
     (ref_rays_per_s: the FP32-accurate tensor-core step of the main line)."""
     R = cfg["R"]
@@ -377,7 +383,7 @@ def step_variants(cfg, scene, tree, cam, dev, ref_rays_per_s, steps=50):
     for name, dec, prop in (("fp32_simt", "simt", False), ("bf16", "bf16", False), ("bf16_proposal12", "bf16", True)):
         tr = make_trainer(cfg, tree, cam, dev, dec, prop, cfg["seed"])
         k = steps if prop else 10
-        for i in range(3 if not prop else 2 * steps):
+        for i in range(3 if not prop else PROPOSAL_WARM_CYCLES * steps):
             tr.step(*batches[i % steps])
         ms, phase_ms, counts = time_steps(tr, batches[:k])
         out[name] = {"rays_per_s": R * k / (ms / 1000.0), "ms_per_step": ms / k, "steps": k,
@@ -576,8 +582,8 @@ def reference_gpu_igs(cfg, scene, tree, cam, dev, reps=5):
 def large_workload(dev, steps=50, warmup=3):
     """The large porous configuration, BF16 + learned proposal: rays/s over one
     full 50-step proposal cycle (its uniform 32-sample TRAIN step included)
-    after two cycles that train the proposal, device-resident batches, CUDA
-    events; per-phase times and samples per step."""
+    after 20 cycles that train the proposal and its count head, device-resident
+    batches, CUDA events; per-phase times and samples per step."""
     cfg = dict(WORKLOADS["large"])
     scene, tree, cam = build_workload(cfg, dev)
     tr = make_trainer(cfg, tree, cam, dev, "bf16", True, cfg["seed"])
@@ -587,8 +593,8 @@ def large_workload(dev, steps=50, warmup=3):
     batches = [scene.sample_batch(R, gen) for _ in range(warmup + steps)]
     for i in range(warmup):  # the warm-up includes the first TRAIN step; the timed cycle has its own
         tr.step(*batches[i])
-    while tr.step_id < 100 or (tr.step_id % 50) != 0:  # two cycles; the timed region starts at a boundary
-        tr.step(*batches[tr.step_id % warmup])
+    while tr.step_id < 50 * PROPOSAL_WARM_CYCLES or (tr.step_id % 50) != 0:  # the timed region starts at a boundary
+        tr.step(*batches[tr.step_id % len(batches)])
     ms, phase_ms, counts = time_steps(tr, batches[warmup:])
     S = counts[:, 1].double()
     out = {"workload": cfg["desc"], "rays_per_s": R * steps / (ms / 1000.0), "ms_per_step": ms / steps,

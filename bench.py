@@ -69,12 +69,12 @@ def step_launches(decoder, C, proposal, train):
     """Kernels one neat_train_step launches: STEP_LAUNCHES, plus the records
     backward (three pieces at C = 4, 8; BF16 at C = 4, 8, 16; the plain
     backward kernel then returns at once); with the learned proposal a SAMPLE step adds the CDF
-    kernel and a TRAIN step the histogram zeroing, the node descriptors and 3
-    kernels per proposal iteration."""
+    kernel and a TRAIN step the histogram zeroing, the segments' density
+    variation, the node descriptors and 3 kernels per proposal iteration."""
     records = (decoder == "bf16x3" and C in (4, 8)) or (decoder == "bf16" and C in (4, 8, 16))
     n = STEP_LAUNCHES + (1 if records else 0)
     if proposal:
-        n += (2 + 3 * PROPOSAL_ITERS) if train else 1
+        n += (3 + 3 * PROPOSAL_ITERS) if train else 1
     return n
 
 
@@ -620,6 +620,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="neat", choices=["neat", "reference"])
     ap.add_argument("--workload", default="full", choices=list(WORKLOADS))
+    ap.add_argument("--proposal", action="store_true",
+                    help="main line with the learned proposal (BF16 decoder unless --decoder; on by itself for "
+                         "the large workload), timed from a cycle boundary after %d proposal cycles"
+                         % PROPOSAL_WARM_CYCLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-psnr", action="store_true", help="skip the small workload's time-to-PSNR leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / BF16 / BF16+proposal step variants")
@@ -644,8 +648,8 @@ def main():
     if args.rays:
         cfg["R"] = args.rays
     large = args.workload == "large"
-    decoder = args.decoder or ("bf16" if large else "bf16x3")
-    proposal = large
+    proposal = large or args.proposal
+    decoder = args.decoder or ("bf16" if proposal else "bf16x3")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -705,6 +709,10 @@ def main():
     # does not build the first timed batch's lists, which stay inside the timed region.
     for i in range(W):
         tr.step(*batches[i], next=batches[i + 1] if PREFETCH and i + 1 < W else None)
+    # with the proposal: train it and its count head to their steady state, and
+    # start the timed region at a cycle boundary (a uniform TRAIN step first)
+    while proposal and (tr.step_id < 50 * PROPOSAL_WARM_CYCLES or tr.step_id % 50 != 0):
+        tr.step(*batches[tr.step_id % W])
     torch.cuda.synchronize()
     tr.check_status()
 
@@ -794,8 +802,7 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    launches = sum(step_launches(decoder, cfg["C"], proposal, proposal and (i - 1) % 50 == 0)
-                   for i in range(W + 1, W + K + 1))
+    launches = sum(step_launches(decoder, cfg["C"], proposal, proposal and i % 50 == 0) for i in range(K))
     traffic_key = (args.workload, decoder)
     line = {
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": K, "warmup": W,
@@ -803,9 +810,11 @@ def main():
         "dtype": "bf16" if decoder == "bf16" else "f32",
         "data": "synthetic",
         "config": {"workload": cfg["desc"], "decoder": DECODER_DESC[decoder],
-                   "proposal": ("learned, %d samples per segment, 50-step cycle; %d of the timed steps are "
-                                "uniform TRAIN steps" % (cfg.get("proposal_budget", 12),
-                                                         sum((i - 1) % 50 == 0 for i in range(W + 1, W + K + 1))))
+                   "proposal": ("learned, budget %d samples per segment, the count head's counts (count_eps %g), "
+                                "50-step cycle, timed after %d cycles from a cycle boundary; %d of the timed steps "
+                                "are uniform TRAIN steps"
+                                % (cfg.get("proposal_budget", 12), cfg.get("count_eps", COUNT_EPS),
+                                   PROPOSAL_WARM_CYCLES, sum(i % 50 == 0 for i in range(K))))
                    if proposal else None,
                    "rays_per_step": R, "samples_per_step": S, "segments_per_step": counters[0],
                    "active_nodes": n_active, "parallelism": f"replicas x{world}",

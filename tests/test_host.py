@@ -62,6 +62,35 @@ def test_library_host_calls_without_gpu():
     assert lib.neat_train_step_prebuilt(None, None, None, 0, 1, None, None, 0, None) == _lib.NEAT_ERR_BAD_INPUT
 
 
+def test_proposal_count_arguments_checked_before_any_launch():
+    """A SAMPLE-mode proposal with the count head on needs count_min >= 1 and a
+    finite, non-negative count_eps: otherwise the call is refused on the host
+    (bad input); valid ones get as far as the workspace size check (a zero-byte
+    workspace: capacity), before any launch."""
+    import ctypes
+    import math
+    from neat_b200 import _lib
+    lib = _lib.load()
+    d = _lib.StepDesc(tree_table=16, num_active=8, max_depth=2, node_min=16, node_max=16, w=64, h=64,
+                      intrinsics=16, rotation=16, translation=16, C=8, G=9, softplus_beta=2.0,
+                      max_samples_per_node=8, seg_capacity=4096, decoder_path=_lib.NEAT_DECODER_TC_BF16, proposal=1)
+    b = _lib.StepBatch(uv=16, image_id=16, target=16, num_rays=512)
+    cnt = (ctypes.c_int64 * 4)()
+    status = ctypes.c_int(0)
+
+    def call(eps, nmin):
+        pr = _lib.Proposal(mode=_lib.NEAT_PROPOSAL_SAMPLE, params=16, node_desc=16, mix=0.25, count_eps=eps,
+                           count_min=nmin)
+        return lib.neat_train_step_segments(ctypes.byref(d), ctypes.byref(pr), ctypes.byref(b), ctypes.addressof(cnt),
+                                            ctypes.addressof(status), 16, 0, None)
+
+    assert call(0.05, 0) == _lib.NEAT_ERR_BAD_INPUT
+    assert call(-0.1, 2) == _lib.NEAT_ERR_BAD_INPUT
+    assert call(math.nan, 2) == _lib.NEAT_ERR_BAD_INPUT
+    assert call(0.05, 2) == _lib.NEAT_ERR_CAPACITY
+    assert call(0.0, 0) == _lib.NEAT_ERR_CAPACITY  # counts off: count_min unused
+
+
 def test_no_cpu_fallback_when_library_missing(monkeypatch):
     from neat_b200 import _lib
     monkeypatch.setattr(_lib, "_lib", None)

@@ -815,10 +815,11 @@ def main():
         "data": "synthetic",
         "config": {"workload": cfg["desc"], "decoder": DECODER_DESC[decoder],
                    "proposal": ("learned, budget %d samples per segment, the count head's counts (count_eps %g), "
-                                "50-step cycle, timed after %d cycles from a cycle boundary; %d of the timed steps "
-                                "are uniform TRAIN steps"
+                                "uniform share %g, 50-step cycle, timed after %d cycles from a cycle boundary; %d of "
+                                "the timed steps are uniform TRAIN steps"
                                 % (cfg.get("proposal_budget", 12), cfg.get("count_eps", COUNT_EPS),
-                                   PROPOSAL_WARM_CYCLES, sum(i % 50 == 0 for i in range(K))))
+                                   cfg.get("proposal_mix", PROPOSAL_MIX), PROPOSAL_WARM_CYCLES,
+                                   sum(i % 50 == 0 for i in range(K))))
                    if proposal else None,
                    "rays_per_step": R, "samples_per_step": S, "segments_per_step": counters[0],
                    "active_nodes": n_active, "parallelism": f"replicas x{world}",

@@ -228,6 +228,15 @@ typedef struct
      * per ray (0: 4 (max_samples_per_node + 1); negative: no records).  A
      * step with more samples than the room recomputes them in the backward. */
     int record_samples_per_ray;
+    /* Optional (may be NULL): for a tree of max_depth <= 5 whose active nodes
+     * are disjoint, the global id of the active node holding each finest cell,
+     * or -1: int32 [2^D][2^D][2^D] (z, y, x), device memory.  At
+     * max_depth 5 the step then finds each ray's hits by a 3-D DDA over these
+     * cells (a thread a ray; below depth 5 the walk is faster and stays), the
+     * same hits and intervals, each node's slab test unchanged (an entry
+     * that is no node of the tree raises NEAT_ERR_BAD_INPUT in the status
+     * word and counts as -1); NULL keeps the level-by-level octree walk. */
+    const int32_t* cell_node;
 } neat_step_desc;
 
 /* Decoder paths of the fused step.

@@ -43,7 +43,7 @@ class StepDesc(ctypes.Structure):
         ("C", c_int), ("G", c_int), ("softplus_beta", c_float), ("max_samples_per_node", c_int),
         ("lr_grid", c_float), ("lr_decoder", c_float), ("beta1", c_float), ("beta2", c_float), ("eps", c_float),
         ("seg_capacity", c_int64), ("decoder_path", c_int), ("proposal", c_int), ("pose_grad", c_int),
-        ("record_samples_per_ray", c_int),
+        ("record_samples_per_ray", c_int), ("cell_node", c_void_p),
     ]
 
 

@@ -147,15 +147,19 @@ __device__ __forceinline__ void make_ray(float u, float v, int w, int h, const d
 // because near only grows and far only shrinks.  Returns hit, tmin, tmax
 // (float, as the reference's tuple).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, int P, int D, const float o[3],
-                                          const float d[3], float& tmin, float& tmax)
+// The slab test of the box with plane indices k[0..5] (x0, x1, y0, y1, z0, z1);
+// Tf(a, k) gives the slab parameter (plane_k - o_a) / d_a of axis a (read
+// only where d_a != 0).
+template <class TF>
+__device__ __forceinline__ bool slab_test_k(const uint8_t* k, TF&& Tf, int D, const float o[3], const float d[3],
+                                            float& tmin, float& tmax)
 {
     float tn = -INFINITY, tf = INFINITY;
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-        int k0 = e.k[2 * a], k1 = e.k[2 * a + 1];
+        int k0 = k[2 * a], k1 = k[2 * a + 1];
         if (d[a] == 0.0f)
         {
             float mn = plane_coord(k0, D), mx = plane_coord(k1, D);
@@ -163,7 +167,7 @@ __device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, in
         }
         else
         {
-            float T1 = T[a * P + k0], T2 = T[a * P + k1];
+            float T1 = Tf(a, k0), T2 = Tf(a, k1);
             if (T1 > T2)
             {
                 float tmp = T1;
@@ -180,6 +184,21 @@ __device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, in
     tmin           = ok ? tn : 0.0f;
     tmax           = ok ? fminf(tf, 43637576.0f) : 0.0f;
     return ok;
+}
+
+// The slab test of a node with the slab parameters of every plane in T
+// ([3][P], P = 2^D + 1).
+__device__ __forceinline__ bool slab_test(const NodeEntry& e, const float* T, int P, int D, const float o[3],
+                                          const float d[3], float& tmin, float& tmax)
+{
+    return slab_test_k(
+        e.k, [&](int a, int k) { return T[a * P + k]; }, D, o, d, tmin, tmax);
+}
+
+// The slab parameter of plane k of axis a: the value a [3][P] table holds.
+__device__ __forceinline__ float plane_t(int k, int D, float oa, float da)
+{
+    return __fdiv_rn(__fsub_rn(plane_coord(k, D), oa), da);
 }
 
 // Stratified sample position j of a segment, HyperTree.cu:341-358, rounded as

@@ -30,7 +30,8 @@ static_assert(sizeof(SegRec) == 80, "SegRec must be 80 bytes");
 cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R, int w, int h, const double* intr,
                              const double* rot, const double* trans, const void* table, int D, int M, int cap_ray,
                              float* origin, float* direction, SegRec* ray_hits, int* ray_nseg, int* node_nseg,
-                             int64_t* counters, int* status, cudaStream_t st);
+                             int64_t* counters, int* status, cudaStream_t st,
+                             const int32_t* cell_node = nullptr);
 
 // Pass 2: place the per-ray lists into node-major buckets.
 cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,

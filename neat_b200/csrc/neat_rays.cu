@@ -71,7 +71,7 @@ __device__ int warp_traverse_hits(const NodeEntry* __restrict__ tab, int D, int 
     {
         const int ax = i / P, k = i - ax * P;
         const float dv = d[ax];
-        ws.T[i]        = (dv != 0.0f) ? __fdiv_rn(__fsub_rn(plane_coord(k, D), o[ax]), dv) : 0.0f;
+        ws.T[i]        = (dv != 0.0f) ? plane_t(k, D, o[ax], dv) : 0.0f;
     }
     __syncwarp();
     int count = 0, fsz = 0, cur = 0;
@@ -539,14 +539,198 @@ __global__ void __launch_bounds__(PLACE_T)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Hits by a 3-D DDA over the finest cells (a tree of depth <= 5 whose active
+// nodes are disjoint; cell_node maps each finest cell to its active node, or
+// -1).  One thread per ray steps from cell to cell along the line inside the
+// root box, in the order of the plane crossings (the slab parameters of the
+// table the walk uses: plane_t); when the cell's node changes, the node's own
+// slab test (slab_test_k, unchanged) gives its interval and the 1e-5 rule
+// decides.  A node whose interval has positive length holds cells of
+// positive length along the ray, so the DDA visits it; cells crossed at one
+// point only (the ray through an edge or a corner) are stepped over, and a
+// node touched only there fails the 1e-5 rule anyway.  Boxes are convex and
+// disjoint, so each hit is visited once and in increasing tmin: the canonical
+// (tmin, node id) order, with the same records as k_step_rays.
+// ---------------------------------------------------------------------------
+// The step uses it at depth 5, where it is faster than the walk (segment build
+// 0.83 -> 0.75 ms at 2^19 rays); at depth 4 the walk is (0.36 against 0.37 ms).
+constexpr int DDA_THREADS = 128;
+
+__global__ void __launch_bounds__(DDA_THREADS)
+    k_step_rays_dda(int64_t R, const NodeEntry* __restrict__ table, const int32_t* __restrict__ cell_node, int D,
+                    int M, int cap_ray, const float* __restrict__ origin, const float* __restrict__ direction,
+                    SegRec* __restrict__ ray_hits, int* __restrict__ ray_nseg, int* __restrict__ node_nseg,
+                    int64_t* counters, int* status)
+{
+    const int64_t r = (int64_t)blockIdx.x * DDA_THREADS + threadIdx.x;
+    if (r >= R) return;
+    float o[3], d[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        o[c] = origin[3 * r + c];
+        d[c] = direction[3 * r + c];
+    }
+    const int N       = 1 << D;
+    const int n_nodes = (int)tree_nodes(D);
+    auto Tf           = [&](int a, int k) { return plane_t(k, D, o[a], d[a]); };
+    bool bad          = false;
+    SegRec* out = ray_hits + r * (int64_t)cap_ray;
+    int k = 0, prefix = 0;
+    bool over = false;
+    // the segment of node `node` (visited in tmin order), if it is a hit
+    auto emit = [&](int node) {
+        const NodeEntry e = table[node];
+        float t0, t1;
+        const bool h   = slab_test_k(e.k, Tf, D, o, d, t0, t1);
+        const float dt = __fsub_rn(t1, t0);
+        if (!(h && e.active && !(dt <= 1e-5f))) return;  // (double)dt < 1e-5
+        const int n = iceil_pos(__fmul_rn(__fdiv_rn(dt, e.diag), (float)M));
+        if (k < cap_ray)
+        {
+            SegRec sg;
+            sg.ray        = (int32_t)r;
+            sg.local_base = prefix;
+            sg.tmin       = t0;
+            sg.tmax       = t1;
+            sg.n          = n;
+            sg.row        = e.local;
+            sg.rm         = atomicAdd(&node_nseg[e.local], 1);
+            sg.step       = __fdiv_rn(dt, (float)n);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                sg.o[c]  = o[c];
+                sg.d[c]  = d[c];
+                sg.mn[c] = plane_coord(e.k[2 * c], D);
+                sg.mx[c] = plane_coord(e.k[2 * c + 1], D);
+            }
+            out[k] = sg;
+        }
+        else
+            over = true;
+        prefix += n;
+        ++k;
+    };
+    const uint8_t root[6] = {0, (uint8_t)N, 0, (uint8_t)N, 0, (uint8_t)N};
+    float ta, tb;
+    if (slab_test_k(root, Tf, D, o, d, ta, tb))
+    {
+        // the cell holding the line just after ta on each axis, and the slab
+        // parameter where the line leaves it along that axis
+        int ci[3];
+        float nx[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+        {
+            if (d[a] == 0.0f)
+            {
+                int lo = 0, hi = N;  // plane_coord(lo) <= o < plane_coord(hi)
+                while (hi - lo > 1)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (plane_coord(mid, D) <= o[a])
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                ci[a] = lo;
+                nx[a] = INFINITY;
+            }
+            else if (d[a] > 0.0f)
+            {
+                int lo = 0, hi = N;  // the last plane k < N with T(k) <= ta (T increases with k)
+                while (hi - lo > 1)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (Tf(a, mid) <= ta)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                ci[a] = lo;
+                nx[a] = Tf(a, lo + 1);
+            }
+            else
+            {
+                int lo = 0, hi = N;  // the first plane k > 0 with T(k) <= ta (T decreases with k)
+                while (hi - lo > 1)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (Tf(a, mid) <= ta)
+                        hi = mid;
+                    else
+                        lo = mid;
+                }
+                ci[a] = hi - 1;
+                nx[a] = Tf(a, hi - 1);
+            }
+        }
+        int cur = -1;
+        for (int steps = 0; steps < 3 * N + 3; ++steps)
+        {
+            int node = __ldg(cell_node + ((int64_t)ci[2] * N + ci[1]) * N + ci[0]);
+            if (node < -1 || node >= n_nodes)
+            {
+                bad  = true;  // not a node of this tree: the map does not belong to it
+                node = -1;
+            }
+            if (node != cur)
+            {
+                if (cur >= 0) emit(cur);
+                cur = node;
+            }
+            const float tn = fminf(nx[0], fminf(nx[1], nx[2]));
+            if (!(tn < tb)) break;
+            bool out_of_box = false;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+            {
+                if (nx[a] == tn)
+                {
+                    if (d[a] > 0.0f)
+                    {
+                        ++ci[a];
+                        out_of_box = out_of_box || ci[a] >= N;
+                        if (ci[a] < N) nx[a] = Tf(a, ci[a] + 1);
+                    }
+                    else
+                    {
+                        --ci[a];
+                        out_of_box = out_of_box || ci[a] < 0;
+                        if (ci[a] >= 0) nx[a] = Tf(a, ci[a]);
+                    }
+                }
+            }
+            if (out_of_box) break;
+        }
+        if (cur >= 0) emit(cur);
+    }
+    if (over) raise_status(status, NEAT_ERR_CAPACITY);
+    if (bad) raise_status(status, NEAT_ERR_BAD_INPUT);
+    if (k > NEAT_MAX_HITS_PER_RAY) raise_status(status, NEAT_ERR_TOO_MANY_HITS);
+    k = min(k, cap_ray);
+    ray_nseg[r] = k;
+    if ((unsigned long long)k > *(volatile unsigned long long*)&counters[2])
+        atomicMax((unsigned long long*)&counters[2], (unsigned long long)k);
+}
+
 cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R, int w, int h, const double* intr,
                              const double* rot, const double* trans, const void* table, int D, int M, int cap_ray,
                              float* origin, float* direction, SegRec* ray_hits, int* ray_nseg, int* node_nseg,
-                             int64_t* counters, int* status, cudaStream_t st)
+                             int64_t* counters, int* status, cudaStream_t st, const int32_t* cell_node)
 {
     if (R <= 0) return cudaSuccess;
     k_make_rays<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(uv, image_id, nullptr, R, w, h, intr, rot, trans, origin,
                                                             direction);
+    if (cell_node && D == 5)
+    {
+        k_step_rays_dda<<<(unsigned)((R + DDA_THREADS - 1) / DDA_THREADS), DDA_THREADS, 0, st>>>(
+            R, (const NodeEntry*)table, cell_node, D, M, cap_ray, origin, direction, ray_hits, ray_nseg, node_nseg,
+            counters, status);
+        return cudaGetLastError();
+    }
     const unsigned grid = (unsigned)((R + RAY_WARPS - 1) / RAY_WARPS);
     const NodeEntry* tab = (const NodeEntry*)table;
     if (cap_ray <= WarpHitsStep::kHits && D <= WarpHitsStep::kDepth)

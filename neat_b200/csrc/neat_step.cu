@@ -832,7 +832,7 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
     ok      = ok && cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st) == cudaSuccess;
     ok = ok && launch_step_rays(b->uv, b->image_id, R, d->w, d->h, d->intrinsics, d->rotation, d->translation,
                                 d->tree_table, D, M, L.cap_ray, w.origin, w.direction, w.ray_hits, w.ray_nseg,
-                                w.node_nseg, cnt, status, st) == cudaSuccess;
+                                w.node_nseg, cnt, status, st, d->cell_node) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.ray_nseg, nullptr, R, w.ray_seg_off, w.scratch, cnt + 0, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.node_nseg, nullptr, A, w.node_seg_off, w.scratch, nullptr, st) == cudaSuccess;
     k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, status);

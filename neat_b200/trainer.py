@@ -27,7 +27,7 @@ class FusedTrainer:
                  proposal=False, proposal_budget=12, proposal_every=50, proposal_lr=1e-2, proposal_iters=10,
                  proposal_mix=0.25, proposal_count_eps=0.0, proposal_count_min=2, grid_bf16=False, loss_tv=0.0, loss_edge=0.0, edge_epsilon=0.001,
                  tonemap=None, pose_grad=False, optimize_pose=False, optimize_intrinsics=False, lr_pose=1e-3,
-                 lr_intrinsics=100.0, record_samples_per_ray=0):
+                 lr_intrinsics=100.0, record_samples_per_ray=0, cell_map=True):
         self.dev = torch.device(device)
         self.tree, self.camera = tree, camera
         self.C, self.G, self.M = int(num_features), int(grid_size), int(max_samples_per_node)
@@ -70,6 +70,10 @@ class FusedTrainer:
             max_samples_per_node=self.M, lr_grid=float(lr_grid), lr_decoder=float(lr_decoder), beta1=0.9,
             beta2=0.999, eps=1e-8, seg_capacity=0, decoder_path=int(decoder_path),
             record_samples_per_ray=int(record_samples_per_ray))
+        # hits by a DDA over the finest cells when the tree allows (depth <= 5,
+        # disjoint active nodes); cell_map=False keeps the level-by-level walk
+        self.cell_map = bool(cell_map)
+        self.desc.cell_node = self._cell_node_ptr(self.tables)
         # step number kept on the device: a captured graph of the step advances it on replay
         self.step_counter = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.state = _lib.StepState(
@@ -158,6 +162,10 @@ class FusedTrainer:
             if self.proposal:
                 self.desc_budget.pose_grad = 1
             self.state.pose = ctypes.addressof(self.pose)
+
+    def _cell_node_ptr(self, tables):
+        cells = tables.get("cell_node")
+        return cells.data_ptr() if (self.cell_map and cells is not None) else None
 
     def _stream(self):
         return torch.cuda.current_stream(self.dev).cuda_stream
@@ -536,6 +544,7 @@ class FusedTrainer:
         for desc in [self.desc] + ([self.desc_budget] if self.proposal else []):
             desc.tree_table = new_tables["table"].data_ptr()
             desc.num_active = A
+            desc.cell_node = self._cell_node_ptr(new_tables)
         self.state.grid, self.state.grid_m = grid.data_ptr(), self.grid_m.data_ptr()
         self.state.grid_v, self.state.grid_grad = self.grid_v.data_ptr(), self.grid_grad.data_ptr()
         if self.grid_bf16 is not None:

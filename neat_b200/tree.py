@@ -133,8 +133,29 @@ class HyperTreeBase:
                 if st:
                     raise _lib.NeatError(st, "neat_tree_prepare")
                 t["table"] = table
+                cells = self.cell_node_map()
+                t["cell_node"] = torch.from_numpy(cells).to(device) if cells is not None else None
             self._dev[key] = t
         return self._dev[key]
+
+    def cell_node_map(self):
+        """For a tree of max_depth <= 5 whose active nodes are disjoint: the
+        global id of the active node holding each finest cell, or -1, int32
+        [2^D][2^D][2^D] (z, y, x) -- the cell map of the step's DDA hit search.
+        None for deeper trees, or when an active node lies inside another."""
+        D = self.max_depth
+        if D > 5:
+            return None
+        N = 1 << D
+        cells = np.full((N, N, N), -1, np.int32)
+        for nid in self.active_node_ids:
+            lo = np.rint((self.node_position_min[nid].astype(np.float64) + 1.0) * (N / 2)).astype(np.int64)
+            hi = np.rint((self.node_position_max[nid].astype(np.float64) + 1.0) * (N / 2)).astype(np.int64)
+            box = cells[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+            if (box != -1).any():
+                return None
+            box[...] = nid
+        return cells
 
     # --- adaptive structure (stands in for the reference's MIP optimizer) ---
     def RefineByVariance(self, density_fn, target_active, samples_per_axis=6, start_depth=1):

@@ -182,6 +182,36 @@ def test_workload_proposal_sampling(neat, oracle, request, which, path, counts):
     assert err < P.PATHS[path][1]
 
 
+@pytest.mark.parametrize("path", ["bf16x3", "bf16"])
+def test_large_workload_dda_hits_equal_the_octree_walk(neat, large_case, path):
+    """At depth 5 the step finds each ray's hits by a DDA over the finest cells
+    (the trainer's default); with the cell map off it walks the octree level by
+    level.  On the large workload slice both give the same counters
+    (segments, samples, largest hit count) and the same projection up to the
+    rounding of a segment's two tile partials (the order of segments inside a
+    node bucket comes from atomics, so where a tile boundary cuts a segment
+    varies from call to call), with jitter (the step) and without (project)."""
+    c = large_case
+    a = P._trainer(c, path)
+    b = P._trainer(c, path, cell_map=False)
+    assert a.desc.cell_node and not b.desc.cell_node
+    uv, img, tgt = P._dev(c.uv), P._dev(c.img), P._dev(c.target)
+    out = []
+    for tr in (a, b):
+        pred = torch.zeros(c.R, device="cuda")
+        loss = tr.step(uv, img, tgt, prediction=pred)
+        proj = tr.project(uv, img)
+        torch.cuda.synchronize()
+        tr.check_status()
+        out.append((tr.counters.cpu().numpy().copy(), float(loss.item()), pred.cpu().numpy(), proj.cpu().numpy()))
+    print(path, "DDA", out[0][0][:3], "walk", out[1][0][:3])
+    np.testing.assert_array_equal(out[0][0][:3], out[1][0][:3])
+    assert abs(out[0][1] - out[1][1]) <= 1e-6 * abs(out[1][1])
+    tol = 3e-7 if path == "bf16x3" else 1e-3
+    np.testing.assert_allclose(out[0][2], out[1][2], rtol=tol, atol=0)
+    np.testing.assert_allclose(out[0][3], out[1][3], rtol=tol, atol=0)
+
+
 # ---------------------------------------------------------------- gradient check
 @pytest.mark.parametrize("path,bar", [("bf16x3", 1e-4), ("bf16", 5e-2)])
 def test_large_workload_finite_differences(neat, oracle, large_case, path, bar):

@@ -116,6 +116,33 @@ def test_tree_tables_match_oracle(oracle, depth):
     assert np.all(pre[T.node_depth != depth] == -1)
 
 
+def test_cell_node_map(oracle):
+    """The finest-cell map of the step's DDA hit search: every finest cell
+    holds the active node whose box contains its centre (or -1); a tree with an
+    active node inside another, or deeper than 5, has none."""
+    from neat_b200 import scene as SC
+    from neat_b200.tree import HyperTreeBase
+    objs = SC.ellipsoid_phantom(8, 10, seed=3)
+    T = HyperTreeBase(3, 4)
+    T.RefineByVariance(lambda p: oracle.phantom_density(objs, p), 200, samples_per_axis=3)
+    act = T.active_node_ids
+    keep = act[np.random.default_rng(1).random(act.shape[0]) < 0.7]  # holes: cells of no active node
+    T.SetActiveNodes(keep)
+    cells = T.cell_node_map()
+    N = 16
+    c = (np.arange(N) + 0.5) / N * 2 - 1
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    p = np.stack([x, y, z], -1).reshape(-1, 3)
+    mn, mx = T.node_position_min[keep], T.node_position_max[keep]
+    inside = np.all((p[:, None] >= mn[None]) & (p[:, None] < mx[None]), axis=2)
+    want = np.where(inside.any(1), keep[inside.argmax(1)], -1)
+    np.testing.assert_array_equal(cells.reshape(-1), want)
+    nested = np.concatenate([keep[:5], [int(T.node_parent[keep[0]])]])
+    T.SetActiveNodes(np.unique(nested))
+    assert T.cell_node_map() is None
+    assert HyperTreeBase(3, 6).cell_node_map() is None
+
+
 def test_refine_by_variance_partitions_the_cube(oracle):
     from neat_b200 import scene as SC
     from neat_b200.tree import HyperTreeBase

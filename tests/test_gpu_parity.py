@@ -610,6 +610,57 @@ def test_proposal_gain_over_uniform(neat, oracle, case):
     assert ce < np.log(8) - 0.02
 
 
+def test_count_head_gain_over_uniform(neat, oracle, case):
+    """What the count head gains, and what not: after online training on the
+    scene (budget 8, count_eps 0.05, count_min 2) its per-segment counts place
+    far fewer samples than the budget on every segment.  Against a dense f64
+    evaluation, their projection error is on a par with uniform sampling that
+    spreads as many samples evenly (interpolated between the uniform budgets
+    around that total): on this scene the learned counts save samples against
+    a fixed budget, they do not beat an even spread of the same number (within
+    15 % either way in repeated runs, better at the most aggressive tolerances
+    and worse at mild ones; the check allows 25 %)."""
+    c = case
+    tr = _prop_trainer(c, "bf16x3", proposal_budget=8, proposal_every=20, proposal_iters=50, proposal_lr=1e-2,
+                       proposal_mix=0.25, proposal_count_eps=0.05, proposal_count_min=2)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(4)
+    proj = _dev(c.proj.astype(np.float32))
+    for _ in range(600):
+        img = torch.randint(0, c.n_img, (4096,), generator=gen, device="cuda")
+        x = torch.randint(0, c.w, (4096,), generator=gen, device="cuda")
+        y = torch.randint(0, c.h, (4096,), generator=gen, device="cuda")
+        uv = torch.stack([x.float() / (c.w - 1), y.float() / (c.h - 1)], 1).contiguous()
+        tr.step(uv, img.to(torch.int32).contiguous(), proj[img, y, x].contiguous())
+    torch.cuda.synchronize()
+    tr.check_status()
+    uv, im = _dev(c.uv), _dev(c.img)
+    T = c.tree
+    o, d = oracle.make_rays(c.uv, c.img, c.w, c.h, c.intr, c.rot, c.trans)
+    dense = oracle.create_samples(o, d, T.active_node_ids, T.node_position_min, T.node_position_max, 256, False)
+    ref = oracle.image_f64(dense, torch.from_numpy(tr.grid_reference_layout().cpu().numpy().astype(np.float64)),
+                           torch.from_numpy(tr.decoder.cpu().numpy().astype(np.float64)), T.node_position_min,
+                           T.node_position_max, T.node_active_prefix_sum, c.R).numpy()
+
+    def run(**kw):
+        p = tr.project(uv, im, **kw).cpu().numpy().astype(np.float64)
+        torch.cuda.synchronize()
+        return np.abs(p - ref).mean(), int(tr.counters[1].item())
+
+    e_cnt, n_cnt = run(use_proposal=True)
+    eps = tr.prop_struct.count_eps
+    tr.prop_struct.count_eps = 0.0
+    e_full, n_full = run(use_proposal=True)
+    tr.prop_struct.count_eps = eps
+    uni = {m: run(samples_per_node=m) for m in range(1, 9)}
+    e_uni = float(np.interp(n_cnt, [v[1] for v in uni.values()], [v[0] for v in uni.values()]))
+    print("count head:", n_cnt, "samples, error", e_cnt, "| budget 8 on every segment:", n_full, "samples, error",
+          e_full, "| uniform with as many samples (interpolated): error", e_uni,
+          "| uniform budgets:", {k: (v[1], float("%.3g" % v[0])) for k, v in uni.items()})
+    assert n_cnt < 0.7 * n_full
+    assert e_cnt < 1.25 * e_uni
+
+
 # ---------------------------------------------------------------- finite differences
 def test_backward_matches_central_differences(neat, oracle):
     """Config-5 style gradient check: the fused step's analytic gradients

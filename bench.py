@@ -42,10 +42,11 @@ DECODER_DESC = {"simt": "FP32 FFMA (CUDA cores)",
 CPU_PATH_DESC = ("reference CPU IGS fwd/bwd compiled from its source (oracle/_ref), OpenMP C port of the CUDA-only "
                  "ComputeRaySamples, libtorch-CPU decoder/softplus/index_add/MSE/autograd/Adam")
 PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
-# kernels one neat_train_step launches: step scalars, rays, hit lists, 3 scans
-# x 3 kernels, segment clamp, placement, partial zeroing, sample clamp, tile
-# map, forward tiles, ray loss, loss total, backward tiles, decoder Adam, grid Adam
-STEP_LAUNCHES = 23
+# kernels one neat_train_step launches: step scalars, rays, hit lists, 2 scans
+# x 3 kernels and the one-block scan of the node counts, segment clamp,
+# placement, partial zeroing, sample clamp, tile map, forward tiles, ray loss,
+# loss total, backward tiles, decoder Adam, grid Adam
+STEP_LAUNCHES = 21
 # DRAM bytes per sample of the records backward (k_bwd_rec), dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch in a single-pass ncu capture, scaled to the
 # measured launch by its samples:

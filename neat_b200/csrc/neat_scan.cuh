@@ -128,6 +128,43 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(TO* __restrict__ out,
     }
 }
 
+// One block for a short array (n <= SCAN_SINGLE): block scan of 8 elements a
+// thread, out[n] = total (and total64): one launch instead of three.
+constexpr int SCAN_SINGLE_THREADS = 1024;
+constexpr int64_t SCAN_SINGLE     = (int64_t)SCAN_SINGLE_THREADS * SCAN_ITEMS;
+
+template <typename TO>
+__global__ void __launch_bounds__(SCAN_SINGLE_THREADS) k_scan_single(const int* __restrict__ in, const int64_t* n_dev,
+                                                                     int64_t n_host, TO* __restrict__ out,
+                                                                     int64_t* total64)
+{
+    __shared__ TO warp_tot[32];
+    const int64_t n = scan_count(n_dev, n_host);  // <= SCAN_SINGLE (checked on the host)
+    TO loc[SCAN_ITEMS];
+    TO sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+    {
+        const int64_t idx = (int64_t)threadIdx.x * SCAN_ITEMS + i;
+        const TO v        = (idx < n) ? (TO)in[idx] : (TO)0;
+        loc[i]            = sum;
+        sum += v;
+    }
+    TO total;
+    const TO pre = block_exclusive_scan<TO>(sum, warp_tot, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+    {
+        const int64_t idx = (int64_t)threadIdx.x * SCAN_ITEMS + i;
+        if (idx < n) out[idx] = pre + loc[i];
+    }
+    if (threadIdx.x == 0)
+    {
+        out[n] = total;
+        if (total64) *total64 = (int64_t)total;
+    }
+}
+
 // Scratch (in elements of TO) needed for a scan of at most n_max elements.
 inline int64_t scan_scratch_elems(int64_t n_max) { return (n_max + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
@@ -137,6 +174,11 @@ template <typename TO>
 inline cudaError_t scan_exclusive(const int* in, const int64_t* n_dev, int64_t n_max, TO* out, TO* scratch,
                                   int64_t* total64, cudaStream_t st)
 {
+    if (n_max <= SCAN_SINGLE)
+    {
+        k_scan_single<TO><<<1, SCAN_SINGLE_THREADS, 0, st>>>(in, n_dev, n_max, out, total64);
+        return cudaGetLastError();
+    }
     int64_t nb = (n_max + SCAN_TILE - 1) / SCAN_TILE;
     if (nb < 1) nb = 1;
     nb = nb < (int64_t)sm_count() * 4 ? nb : (int64_t)sm_count() * 4;

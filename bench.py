@@ -43,10 +43,11 @@ CPU_PATH_DESC = ("reference CPU IGS fwd/bwd compiled from its source (oracle/_re
                  "ComputeRaySamples, libtorch-CPU decoder/softplus/index_add/MSE/autograd/Adam")
 PHASES = ["segments", "forward_tiles", "loss", "backward_tiles", "adam"]
 # kernels one neat_train_step launches: step scalars, rays, hit lists, 2 scans
-# x 3 kernels and the one-block scan of the node counts, segment clamp,
-# placement, partial zeroing, sample clamp, tile map, forward tiles, ray loss,
-# loss total, backward tiles, decoder Adam, grid Adam
-STEP_LAUNCHES = 21
+# x 3 kernels and the one-block scan of the node counts, placement (with the
+# segment capacity check and the partials' zeroing), tile map (with the
+# sample capacity check), forward tiles, ray loss, loss total, backward tiles,
+# decoder Adam, grid Adam
+STEP_LAUNCHES = 18
 # DRAM bytes per sample of the records backward (k_bwd_rec), dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch in a single-pass ncu capture, scaled to the
 # measured launch by its samples:

@@ -36,7 +36,7 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
 // Pass 2: place the per-ray lists into node-major buckets.
 cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,
                               int cap_ray, const int* node_seg_off, SegRec* segs, int* seg_n,
-                              const int64_t* nseg_eff, int64_t cap, cudaStream_t st);
+                              int64_t* counters, int64_t cap, double* partial, int* status, cudaStream_t st);
 
 int sm_count();
 

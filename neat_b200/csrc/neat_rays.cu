@@ -483,10 +483,18 @@ __device__ __forceinline__ int64_t last_le(const int* __restrict__ off, int64_t 
 __global__ void __launch_bounds__(PLACE_T)
     k_step_place(const SegRec* __restrict__ ray_hits, const int* __restrict__ ray_seg_off, int64_t R, int cap_ray,
                  const int* __restrict__ node_seg_off, SegRec* __restrict__ segs,
-                 int* __restrict__ seg_n, const int64_t* nseg_eff, int64_t cap)
+                 int* __restrict__ seg_n, int64_t* counters, int64_t cap, double* __restrict__ partial, int* status)
 {
     __shared__ int soff[PLACE_T + 1];
-    const int64_t nseg = *nseg_eff;  // 0 after a capacity overflow
+    // more segments than the capacity: nothing is placed, the step processes
+    // nothing (counters[0] = 0 for the kernels after this one)
+    const int64_t n0   = counters[0];
+    const int64_t nseg = n0 > cap ? 0 : n0;
+    if (n0 > cap && blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        raise_status(status, NEAT_ERR_CAPACITY);
+        counters[0] = 0;
+    }
     for (int64_t base = (int64_t)blockIdx.x * PLACE_T; base < nseg; base += (int64_t)gridDim.x * PLACE_T)
     {
         // ray_seg_off[lo] <= base < ray_seg_off[hi] (ray_seg_off[R] = total > base);
@@ -507,6 +515,7 @@ __global__ void __launch_bounds__(PLACE_T)
         const int64_t rm = base + threadIdx.x;
         if (rm < nseg)
         {
+            partial[rm] = 0.0;  // the segment's projection partial, summed by the forward tiles
             int64_t ray;
             if (rm < soff[PLACE_T])
             {
@@ -747,7 +756,7 @@ cudaError_t launch_step_rays(const float* uv, const int32_t* image_id, int64_t R
 
 cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const int* ray_seg_off, int64_t R,
                               int cap_ray, const int* node_seg_off, SegRec* segs, int* seg_n,
-                              const int64_t* nseg_eff, int64_t cap, cudaStream_t st)
+                              int64_t* counters, int64_t cap, double* partial, int* status, cudaStream_t st)
 {
     if (R <= 0) return cudaSuccess;
     (void)ray_nseg;
@@ -755,7 +764,7 @@ cudaError_t launch_step_place(const SegRec* ray_hits, const int* ray_nseg, const
     const unsigned nb =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((est + PLACE_T - 1) / PLACE_T, (int64_t)sm_count() * 16));
     k_step_place<<<nb, PLACE_T, 0, st>>>(ray_hits, ray_seg_off, R, cap_ray, node_seg_off, segs, seg_n,
-                                         nseg_eff, cap);
+                                         counters, cap, partial, status);
     return cudaGetLastError();
 }
 

@@ -161,33 +161,6 @@ __global__ void __launch_bounds__(TN, 1) k_step_tiles(StepTileArgs a)
     if constexpr (BWD) dec_grad_flush<C>(g, a.dec_part + (int64_t)blockIdx.x * DecOff<C>::total, false, sm.ypart);
 }
 
-__global__ void k_clamp_segments(int64_t* counters, int64_t cap, int* status)
-{
-    if (counters[0] > cap)
-    {
-        raise_status(status, NEAT_ERR_CAPACITY);
-        counters[0] = 0;
-    }
-}
-
-__global__ void k_clamp_samples(int64_t* counters, int64_t sample_cap, int* status)
-{
-    if (counters[1] > sample_cap)
-    {
-        raise_status(status, NEAT_ERR_CAPACITY);
-        counters[1] = 0;
-    }
-    counters[3] = (counters[1] + TT - 1) / TT;
-}
-
-// Zero the per-segment partials of this step's segments (counters[0] of them).
-__global__ void k_zero_partial(double* __restrict__ partial, const int64_t* counters)
-{
-    const int64_t n = counters[0];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        partial[i] = 0.0;
-}
-
 // Zero n = counters[0] * per floats.
 __global__ void k_zero_per_segment(float* __restrict__ p, const int64_t* counters, int per)
 {
@@ -196,11 +169,24 @@ __global__ void k_zero_per_segment(float* __restrict__ p, const int64_t* counter
         p[i] = 0.0f;
 }
 
-__global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, const int64_t* counters,
-                           int* __restrict__ tile_seg, int64_t tiles_cap)
+// Also the samples' capacity check: more samples than sample_cap and the step
+// processes nothing (counters[1] = 0); counters[3] = the step's tiles.
+__global__ void k_tile_seg(const int* __restrict__ samp_off, const int* __restrict__ seg_n, int64_t* counters,
+                           int* __restrict__ tile_seg, int64_t tiles_cap, int64_t sample_cap, int* status)
 {
     const int64_t nseg = counters[0];
-    if (counters[1] == 0) return;
+    const int64_t s0   = counters[1];
+    const bool over    = s0 > sample_cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        if (over)
+        {
+            raise_status(status, NEAT_ERR_CAPACITY);
+            counters[1] = 0;
+        }
+        counters[3] = over ? 0 : (s0 + TT - 1) / TT;
+    }
+    if (over || s0 == 0) return;
     // grid-stride over the step's segments (the grid is sized for the SMs, not
     // for the segment capacity, most of which a step leaves unused)
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += (int64_t)gridDim.x * blockDim.x)
@@ -835,15 +821,12 @@ static bool build_segments(const neat_step_desc* d, const neat_step_batch* b, co
                                 w.node_nseg, cnt, status, st, d->cell_node) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.ray_nseg, nullptr, R, w.ray_seg_off, w.scratch, cnt + 0, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.node_nseg, nullptr, A, w.node_seg_off, w.scratch, nullptr, st) == cudaSuccess;
-    k_clamp_segments<<<1, 1, 0, st>>>(cnt, cap, status);
     ok = ok && launch_step_place(w.ray_hits, w.ray_nseg, w.ray_seg_off, R, L.cap_ray, w.node_seg_off, w.segs,
-                                 w.seg_n, cnt + 0, cap, st) == cudaSuccess;
-    k_zero_partial<<<sm_count() * 4, 256, 0, st>>>(w.partial, cnt);
+                                 w.seg_n, cnt, cap, w.partial, status, st) == cudaSuccess;
     if (pr) ok = ok && launch_proposal_cdf(w.segs, w.seg_n, cnt, pr, w.seg_cdf, st) == cudaSuccess;
     ok = ok && scan_exclusive<int>(w.seg_n, cnt + 0, cap, w.samp_off, w.scratch, cnt + 1, st) == cudaSuccess;
-    k_clamp_samples<<<1, 1, 0, st>>>(cnt, L.sample_cap, status);
     k_tile_seg<<<(unsigned)std::min<int64_t>((cap + 255) / 256, (int64_t)sm_count() * 8), 256, 0, st>>>(
-        w.samp_off, w.seg_n, cnt, w.tile_seg, L.tiles_cap);
+        w.samp_off, w.seg_n, cnt, w.tile_seg, L.tiles_cap, L.sample_cap, status);
     return ok;
 }
 
